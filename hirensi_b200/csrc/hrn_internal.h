@@ -1,0 +1,148 @@
+// hrn_internal.h -- context layout and helpers shared by the CUDA sources of
+// libhirensi_b200.so.  Not part of the public C ABI (include/hirensi_b200.h).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/hirensi_b200.h"
+
+namespace hrn {
+
+// Owning device buffer (cudaMalloc / cudaFree).
+struct DevBuf {
+    void *p = nullptr;
+    size_t bytes = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf &) = delete;
+    DevBuf &operator=(const DevBuf &) = delete;
+    ~DevBuf() { release(); }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+    }
+    cudaError_t alloc(size_t n) {
+        if (n == bytes && p) return cudaSuccess;
+        release();
+        if (n == 0) return cudaSuccess;
+        cudaError_t e = cudaMalloc(&p, n);
+        if (e == cudaSuccess) bytes = n;
+        else p = nullptr;
+        return e;
+    }
+    template <typename T> T *as() const { return static_cast<T *>(p); }
+};
+
+constexpr int kTagBits = 30;
+constexpr uint32_t kColMask = (1u << kTagBits) - 1u;
+
+}  // namespace hrn
+
+struct hrn_ctx {
+    int device = 0;
+    int precision = HRN_FP64;
+    std::string err;
+    cudaStream_t own_stream = nullptr;
+    cudaStream_t stream = nullptr;
+
+    // ---- operator: one CSR per row holding the C, K and G entries in that order;
+    // the top 2 bits of each column index name the matrix (0 = C, 1 = K, 2 = G).
+    int neq = 0;
+    int64_t nnz = 0;
+    int64_t nnz_w[3] = {0, 0, 0};
+    bool have_operator = false;    // values present
+    bool have_pattern = false;
+    std::vector<int32_t> h_rowptr;            // host copy of the combined pattern
+    std::vector<uint32_t> h_colx;
+    hrn::DevBuf d_rowptr, d_colx, d_rowidx;   // forward pattern (+ row of each entry)
+    hrn::DevBuf d_rowptrT, d_colxT, d_permT;  // transposed pattern, perm into forward entries
+    hrn::DevBuf d_raw;                        // unscaled values (FP64)
+    hrn::DevBuf d_fwd, d_adj;                 // scaled forward values, transposed adjoint values (T)
+    hrn::DevBuf d_diag_m, d_im;               // FP64 mass diagonal and its reciprocal
+
+    // ---- mesh (device assembly and gradient)
+    bool have_mesh = false;
+    int nj = 0, nel = 0, nel_rd = 0;
+    std::vector<double> h_xyz, h_rho, h_pml;
+    std::vector<int32_t> h_inod, h_mtel, h_id;
+    hrn::DevBuf d_xyz, d_inod, d_id, d_rho, d_pml;
+    hrn::DevBuf d_rd_elems;       // [nel_rd] element ids of the regular domain
+    hrn::DevBuf d_rd_geom;        // [nel_rd][27][10] DJI (9) and w*detJ per GLL point (FP64)
+    hrn::DevBuf d_rd_store;       // [nel_rd][27] history node index (store index / 3)
+    bool have_rd_store = false;
+    // device assembly
+    hrn::DevBuf d_asm_geom;       // [nel][27][10] for all elements
+    hrn::DevBuf d_el_color_list;  // elements sorted by colour
+    std::vector<int> color_off;   // [ncolor + 1]
+    hrn::DevBuf d_lam, d_mu;      // nodal material (FP64)
+    hrn::DevBuf d_touched;        // pattern discovery flags
+    hrn::DevBuf d_asm_err;        // device error flag of the assembly kernels
+
+    // ---- history
+    int nstore = 0;
+    std::vector<int32_t> h_store_eq;
+    hrn::DevBuf d_store_eq, d_store_pos;      // [nstore], [neq] (-1 = not stored)
+
+    // ---- shots
+    int nshot = 0, nstep = 0;
+    double dt = 0.0;
+    int nslot_f = 0;
+    hrn::DevBuf d_slot_f;         // [neq] forward source slot of each row (-1 none)
+    hrn::DevBuf d_fslot_eq;       // [nslot_f] equation of each source slot
+    hrn::DevBuf d_fsrc_b;         // [nslot_f][S] unscaled B values (FP64)
+    hrn::DevBuf d_ftab;           // [S][nstep+1][3] TIME_FUNCTION samples (FP64)
+    hrn::DevBuf d_srcv_f;         // [nstep+1][4][nslot_f][S] stage source values (T)
+    std::vector<int32_t> h_src_eq;
+    std::vector<double> h_src_b, h_ftab;
+
+    // ---- receivers
+    int nrec3 = 0, nslot_a = 0;
+    std::vector<int32_t> h_eqdis, h_eqdis_map;
+    hrn::DevBuf d_slot_a;         // [neq] receiver slot of each row (-1 none)
+    hrn::DevBuf d_aslot_ptr, d_aslot_q, d_aslot_eq;   // receiver lists per slot (CSR) and slot equation
+    hrn::DevBuf d_eqdis_map;
+    hrn::DevBuf d_srcv_a;         // [4][nslot_a][S]
+    hrn::DevBuf d_dis;            // [nshot][nrec3][nstep+1] FP64
+    hrn::DevBuf d_mis_terms;      // [nshot][nstep+1] FP64
+    hrn::DevBuf d_cost;           // [1 + nshot] FP64
+
+    // ---- state and histories
+    hrn::DevBuf d_X;              // [2][3][neq][S]
+    hrn::DevBuf d_KB;             // [3][neq][S]
+    hrn::DevBuf d_hist;           // [nstep+1][nstore][S]
+    hrn::DevBuf d_phist;          // adjoint history (optional)
+    bool have_forward = false;
+    bool have_phist = false;
+    hrn::DevBuf d_g;              // [2][nj] FP64 gradient accumulators (lambda, mu)
+
+    // ---- timing
+    bool timing = false;
+    double last_total_ms = 0.0, last_stage_ms = 0.0;
+    int64_t last_stage_launches = 0;
+    std::vector<cudaEvent_t> ev_pool;
+
+    size_t elem_bytes() const { return precision == HRN_FP64 ? 8 : 4; }
+};
+
+// Kernel launchers implemented in the .cu files.
+namespace hrn {
+int launch_scale_operator(hrn_ctx *c);
+int run_forward(hrn_ctx *c);
+int run_adjoint_gradient(hrn_ctx *c, int lambda_2mu, int keep_p);
+int run_misfit(hrn_ctx *c, double *cost);
+int build_rd_geometry(hrn_ctx *c);
+int assemble_device(hrn_ctx *c, bool discover_pattern);
+int finalize_pattern_from_keys(hrn_ctx *c, const std::vector<uint64_t> &keys);
+int set_error(hrn_ctx *c, int code, const std::string &msg);
+int cuda_error(hrn_ctx *c, cudaError_t e, const char *what);
+}  // namespace hrn
+
+#define HRN_CUDA(ctx, call)                                           \
+    do {                                                              \
+        cudaError_t _e = (call);                                      \
+        if (_e != cudaSuccess) return hrn::cuda_error((ctx), _e, #call); \
+    } while (0)

@@ -1,0 +1,854 @@
+// hrn_step.cu -- fused RK4 stage kernels of the explicit forward and adjoint
+// time loops, the adjoint source, the fused zero-lag gradient and the misfit.
+//
+// One RK4 step of S4/Solver_PETSc_Explicit.F90:983-1046 (forward) or
+// :1269-1364 (adjoint) is four launches of rk4_stage<STAGE>.  Stage s computes
+//     kb_s = src_s + C^ km_s + K^ kt_s + G^ h_s
+// over one combined CSR (C, K and G entries of a row back to back, matrix id in
+// the top bits of the column index).  The stage inputs km_s, kt_s, h_s are not
+// stored: every gathered column value is rebuilt from x1, x2, x3 and the earlier
+// kb vectors with the same fused multiply-adds the row owner uses, e.g.
+//     km_3 = c*kb_2 + x3,   kt_3 = c*km_2 + x2,   h_3 = c*kt_2 + x1   (c = dt/2).
+// The fourth stage applies x <- x + dt/6 (k1 + 2 k2 + 2 k3 + k4) for its own
+// rows and writes the new state into the other half of a ping-pong buffer.
+// All S shots of a batch share each matrix entry (vectors are [row][shot]).
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+#include "hrn_internal.h"
+
+namespace hrn {
+
+// ----------------------------------------------------------------------------
+// small vector helpers
+
+template <typename T, int S>
+__device__ __forceinline__ void ldv(const T *__restrict__ p, T (&o)[S])
+{
+    if constexpr (sizeof(T) == 8 && S % 2 == 0) {
+#pragma unroll
+        for (int s = 0; s < S; s += 2) {
+            double2 v = __ldg(reinterpret_cast<const double2 *>(p) + s / 2);
+            o[s] = v.x;
+            o[s + 1] = v.y;
+        }
+    } else if constexpr (sizeof(T) == 4 && S % 4 == 0) {
+#pragma unroll
+        for (int s = 0; s < S; s += 4) {
+            float4 v = __ldg(reinterpret_cast<const float4 *>(p) + s / 4);
+            o[s] = v.x; o[s + 1] = v.y; o[s + 2] = v.z; o[s + 3] = v.w;
+        }
+    } else if constexpr (sizeof(T) == 4 && S % 2 == 0) {
+#pragma unroll
+        for (int s = 0; s < S; s += 2) {
+            float2 v = __ldg(reinterpret_cast<const float2 *>(p) + s / 2);
+            o[s] = v.x; o[s + 1] = v.y;
+        }
+    } else {
+#pragma unroll
+        for (int s = 0; s < S; ++s) o[s] = __ldg(p + s);
+    }
+}
+
+template <typename T, int S>
+__device__ __forceinline__ void stv(T *__restrict__ p, const T (&o)[S])
+{
+    if constexpr (sizeof(T) == 8 && S % 2 == 0) {
+#pragma unroll
+        for (int s = 0; s < S; s += 2) reinterpret_cast<double2 *>(p)[s / 2] = make_double2(o[s], o[s + 1]);
+    } else if constexpr (sizeof(T) == 4 && S % 4 == 0) {
+#pragma unroll
+        for (int s = 0; s < S; s += 4)
+            reinterpret_cast<float4 *>(p)[s / 4] = make_float4(o[s], o[s + 1], o[s + 2], o[s + 3]);
+    } else {
+#pragma unroll
+        for (int s = 0; s < S; ++s) p[s] = o[s];
+    }
+}
+
+__device__ __forceinline__ double fmaT(double a, double b, double c) { return fma(a, b, c); }
+__device__ __forceinline__ float fmaT(float a, float b, float c) { return fmaf(a, b, c); }
+
+// ----------------------------------------------------------------------------
+// stage kernel
+
+template <typename T>
+struct StageArgs {
+    int n;
+    const int32_t *__restrict__ rowptr;
+    const uint32_t *__restrict__ colx;
+    const T *__restrict__ val;
+    const T *__restrict__ x1, *__restrict__ x2, *__restrict__ x3;
+    const T *__restrict__ kb1, *__restrict__ kb2, *__restrict__ kb3;
+    T *__restrict__ kb_out;                 // stages 1-3
+    T *__restrict__ y1, *__restrict__ y2, *__restrict__ y3;   // stage 4
+    const int32_t *__restrict__ slot;       // [n] source slot or -1
+    const T *__restrict__ srcv;             // [4][nslot][S] this step
+    int nslot;
+    const int32_t *__restrict__ store_pos;  // [n] history position or -1 (stage 1)
+    T *__restrict__ hist;                   // [nstore][S] of this step, or null
+    T c, D, d6;                             // dt/2, dt, dt/6 (negated for the adjoint)
+};
+
+// Stage-input value of matrix `tag` at column j (see the file comment).
+template <typename T, int S, int STAGE>
+__device__ __forceinline__ void gather(const StageArgs<T> &a, int tag, size_t j, T (&v)[S])
+{
+    const size_t o = j * S;
+    if constexpr (STAGE == 1) {
+        const T *src = tag == 0 ? a.x3 : (tag == 1 ? a.x2 : a.x1);
+        ldv<T, S>(src + o, v);
+    } else if constexpr (STAGE == 2) {
+        T p[S], q[S];
+        if (tag == 0) { ldv<T, S>(a.kb1 + o, p); ldv<T, S>(a.x3 + o, q); }
+        else if (tag == 1) { ldv<T, S>(a.x3 + o, p); ldv<T, S>(a.x2 + o, q); }
+        else { ldv<T, S>(a.x2 + o, p); ldv<T, S>(a.x1 + o, q); }
+#pragma unroll
+        for (int s = 0; s < S; ++s) v[s] = fmaT(a.c, p[s], q[s]);
+    } else if constexpr (STAGE == 3) {
+        if (tag == 0) {
+            T p[S], q[S];
+            ldv<T, S>(a.kb2 + o, p); ldv<T, S>(a.x3 + o, q);
+#pragma unroll
+            for (int s = 0; s < S; ++s) v[s] = fmaT(a.c, p[s], q[s]);
+        } else if (tag == 1) {
+            T k1[S], x3[S], x2[S];
+            ldv<T, S>(a.kb1 + o, k1); ldv<T, S>(a.x3 + o, x3); ldv<T, S>(a.x2 + o, x2);
+#pragma unroll
+            for (int s = 0; s < S; ++s) v[s] = fmaT(a.c, fmaT(a.c, k1[s], x3[s]), x2[s]);
+        } else {
+            T x3[S], x2[S], x1[S];
+            ldv<T, S>(a.x3 + o, x3); ldv<T, S>(a.x2 + o, x2); ldv<T, S>(a.x1 + o, x1);
+#pragma unroll
+            for (int s = 0; s < S; ++s) v[s] = fmaT(a.c, fmaT(a.c, x3[s], x2[s]), x1[s]);
+        }
+    } else {
+        if (tag == 0) {
+            T p[S], q[S];
+            ldv<T, S>(a.kb3 + o, p); ldv<T, S>(a.x3 + o, q);
+#pragma unroll
+            for (int s = 0; s < S; ++s) v[s] = fmaT(a.D, p[s], q[s]);
+        } else if (tag == 1) {
+            T k2[S], x3[S], x2[S];
+            ldv<T, S>(a.kb2 + o, k2); ldv<T, S>(a.x3 + o, x3); ldv<T, S>(a.x2 + o, x2);
+#pragma unroll
+            for (int s = 0; s < S; ++s) v[s] = fmaT(a.D, fmaT(a.c, k2[s], x3[s]), x2[s]);
+        } else {
+            T k1[S], x3[S], x2[S], x1[S];
+            ldv<T, S>(a.kb1 + o, k1); ldv<T, S>(a.x3 + o, x3); ldv<T, S>(a.x2 + o, x2); ldv<T, S>(a.x1 + o, x1);
+#pragma unroll
+            for (int s = 0; s < S; ++s) v[s] = fmaT(a.D, fmaT(a.c, fmaT(a.c, k1[s], x3[s]), x2[s]), x1[s]);
+        }
+    }
+}
+
+// G lanes per row; rows of a warp are independent sub-groups.
+template <typename T, int S, int STAGE, int G>
+__global__ void __launch_bounds__(256) rk4_stage(const StageArgs<T> a)
+{
+    const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+    const int row = tid / G;
+    const int lane = threadIdx.x & (G - 1);
+    if (row >= a.n) return;   // uniform over the G lanes of a row
+    const unsigned gmask = (G == 32) ? 0xffffffffu : (((1u << G) - 1u) << ((threadIdx.x & 31) & ~(G - 1)));
+
+    T acc[S];
+#pragma unroll
+    for (int s = 0; s < S; ++s) acc[s] = T(0);
+    const int k0 = __ldg(a.rowptr + row), k1 = __ldg(a.rowptr + row + 1);
+    for (int k = k0 + lane; k < k1; k += G) {
+        const uint32_t cx = __ldg(a.colx + k);
+        const T v = __ldg(a.val + k);
+        T x[S];
+        gather<T, S, STAGE>(a, int(cx >> kTagBits), size_t(cx & kColMask), x);
+#pragma unroll
+        for (int s = 0; s < S; ++s) acc[s] = fmaT(v, x[s], acc[s]);
+    }
+#pragma unroll
+    for (int off = G / 2; off > 0; off >>= 1)
+#pragma unroll
+        for (int s = 0; s < S; ++s) acc[s] += __shfl_xor_sync(gmask, acc[s], off, G);
+    if (lane != 0) return;
+
+    const size_t o = size_t(row) * S;
+    T kb[S];
+    const int sl = __ldg(a.slot + row);
+    if (sl >= 0) {
+        T sv[S];
+        ldv<T, S>(a.srcv + (size_t(STAGE - 1) * a.nslot + sl) * S, sv);
+#pragma unroll
+        for (int s = 0; s < S; ++s) kb[s] = sv[s] + acc[s];
+    } else {
+#pragma unroll
+        for (int s = 0; s < S; ++s) kb[s] = acc[s];
+    }
+    if constexpr (STAGE == 1) {
+        if (a.hist) {
+            const int p = __ldg(a.store_pos + row);
+            if (p >= 0) {
+                T x2[S];
+                ldv<T, S>(a.x2 + o, x2);
+                stv<T, S>(a.hist + size_t(p) * S, x2);
+            }
+        }
+    }
+    if constexpr (STAGE < 4) {
+        stv<T, S>(a.kb_out + o, kb);
+    } else {
+        T x1[S], x2[S], x3[S], k1[S], k2[S], k3[S], n1[S], n2[S], n3[S];
+        ldv<T, S>(a.x1 + o, x1); ldv<T, S>(a.x2 + o, x2); ldv<T, S>(a.x3 + o, x3);
+        ldv<T, S>(a.kb1 + o, k1); ldv<T, S>(a.kb2 + o, k2); ldv<T, S>(a.kb3 + o, k3);
+#pragma unroll
+        for (int s = 0; s < S; ++s) {
+            // stage inputs of this row, built exactly as gather() builds them
+            const T km2 = fmaT(a.c, k1[s], x3[s]);
+            const T km3 = fmaT(a.c, k2[s], x3[s]);
+            const T km4 = fmaT(a.D, k3[s], x3[s]);
+            const T kt2 = fmaT(a.c, x3[s], x2[s]);
+            const T kt3 = fmaT(a.c, km2, x2[s]);
+            const T kt4 = fmaT(a.D, km3, x2[s]);
+            const T ht = ((x2[s] + T(2) * kt2) + T(2) * kt3) + kt4;
+            const T hm = ((x3[s] + T(2) * km2) + T(2) * km3) + km4;
+            const T hb = ((k1[s] + T(2) * k2[s]) + T(2) * k3[s]) + kb[s];
+            n1[s] = fmaT(a.d6, ht, x1[s]);
+            n2[s] = fmaT(a.d6, hm, x2[s]);
+            n3[s] = fmaT(a.d6, hb, x3[s]);
+        }
+        stv<T, S>(a.y1 + o, n1);
+        stv<T, S>(a.y2 + o, n2);
+        stv<T, S>(a.y3 + o, n3);
+    }
+}
+
+// ----------------------------------------------------------------------------
+// operator scaling
+
+// forward: -(a_ij * iM_i)            (S4/Solver_PETSc_Explicit.F90:815-824)
+template <typename T>
+__global__ void k_scale_fwd(int64_t nnz, const int32_t *__restrict__ rowidx, const double *__restrict__ raw,
+                            const double *__restrict__ im, T *__restrict__ out)
+{
+    for (int64_t k = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; k < nnz; k += int64_t(gridDim.x) * blockDim.x)
+        out[k] = T(-__dmul_rn(raw[k], im[rowidx[k]]));
+}
+
+// adjoint, stored transposed: ((+-(a_ij iM_i)) M_i) iM_j  (:1222-1229)
+template <typename T>
+__global__ void k_scale_adj(int64_t nnz, const int64_t *__restrict__ permT, const int32_t *__restrict__ rowidx,
+                            const uint32_t *__restrict__ colx, const double *__restrict__ raw,
+                            const double *__restrict__ dm, const double *__restrict__ im, T *__restrict__ out)
+{
+    for (int64_t t = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; t < nnz; t += int64_t(gridDim.x) * blockDim.x) {
+        const int64_t k = permT[t];
+        const int i = rowidx[k];
+        const uint32_t cx = colx[k];
+        double v = -__dmul_rn(raw[k], im[i]);
+        if ((cx >> kTagBits) != 1u) v = -v;
+        v = __dmul_rn(v, dm[i]);
+        v = __dmul_rn(v, im[cx & kColMask]);
+        out[t] = T(v);
+    }
+}
+
+// ----------------------------------------------------------------------------
+// sources
+
+// Forward stage sources for every step: f(T) b^, f(T+dt/2) b^ (twice), f(T+dt) b^,
+// b^ = B * iM.  src_b [nslot][S], ftab [S][nstep+1][3] (T, T+dt, T+dt/2).
+template <typename T, int S>
+__global__ void k_src_fwd(int nstep, int nslot, const int32_t *__restrict__ slot_eq, const double *__restrict__ src_b,
+                          const double *__restrict__ ftab, const double *__restrict__ im, T *__restrict__ srcv)
+{
+    const int64_t total = int64_t(nstep + 1) * nslot * S;
+    for (int64_t t = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; t < total; t += int64_t(gridDim.x) * blockDim.x) {
+        const int s = int(t % S);
+        const int sl = int((t / S) % nslot);
+        const int n = int(t / (int64_t(S) * nslot));
+        const double bh = src_b[sl * S + s] * im[slot_eq[sl]];
+        const double *f = ftab + (size_t(s) * (nstep + 1) + n) * 3;
+        T *o = srcv + (size_t(n) * 4 * nslot) * S;
+        o[(0 * size_t(nslot) + sl) * S + s] = T(0.0 + f[0] * bh);
+        o[(1 * size_t(nslot) + sl) * S + s] = T(0.0 + f[2] * bh);
+        o[(2 * size_t(nslot) + sl) * S + s] = T(0.0 + f[2] * bh);
+        o[(3 * size_t(nslot) + sl) * S + s] = T(0.0 + f[1] * bh);
+    }
+}
+
+// Adjoint stage sources of step n (S4/Solver_PETSc_Explicit.F90:1269-1312):
+// k1 = iM r_n, k4 = iM r_{n-1}, k2 = k3 = (k1 + k4)/2 with
+// r_m = U_Store(EqDis_MAP, m) - Dis_meas(m, :) summed over duplicate equations.
+template <typename T, int S>
+__global__ void k_src_adj(int n, int nstep, int nstore, int nrec3, int nslot, const int32_t *__restrict__ ptr,
+                          const int32_t *__restrict__ qlist, const int32_t *__restrict__ slot_eq,
+                          const int32_t *__restrict__ emap, const T *__restrict__ hist,
+                          const double *__restrict__ dis, const double *__restrict__ im, T *__restrict__ srcv)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nslot * S) return;
+    const int s = t % S, sl = t / S;
+    double r1 = 0.0, r4 = 0.0;
+    for (int k = ptr[sl]; k < ptr[sl + 1]; ++k) {
+        const int q = qlist[k];
+        const size_t pos = size_t(emap[q]) * S + s;
+        const double *d = dis + (size_t(s) * nrec3 + q) * (nstep + 1);
+        r1 += double(hist[size_t(n) * nstore * S + pos]) - d[n];
+        r4 += double(hist[size_t(n - 1) * nstore * S + pos]) - d[n - 1];
+    }
+    const double m = im[slot_eq[sl]];
+    const double v1 = 0.0 + 1.0 * (r1 * m), v4 = 0.0 + 1.0 * (r4 * m);
+    const double v2 = 0.0 + (0.5 * v1 + 0.5 * v4);
+    srcv[(0 * size_t(nslot) + sl) * S + s] = T(v1);
+    srcv[(1 * size_t(nslot) + sl) * S + s] = T(v2);
+    srcv[(2 * size_t(nslot) + sl) * S + s] = T(v2);
+    srcv[(3 * size_t(nslot) + sl) * S + s] = T(v4);
+}
+
+// ----------------------------------------------------------------------------
+// zero-lag gradient (ELEMENT_g_3D, S4/Element_Matrices_3D.F90:1725-1890, and
+// Update_g, S4/Assemble_PETSc_3D.F90:556-661), one thread per GLL point.
+// With the GLL rule FN(I) at point q is the Kronecker delta, so the element
+// contribution to node I is the point scalar at q = I times w*detJ.
+
+__constant__ int c_node_at[27];   // local node at GLL point q = 9c + 3b + a
+__constant__ double c_D[3][3];    // c_D[a][b] = l_b'(xi_a)
+
+constexpr int kGradElems = 4;
+
+template <typename T, int S>
+__global__ void __launch_bounds__(128) k_gradient(int nel_rd, const int32_t *__restrict__ rd_store,
+                                                  const int32_t *__restrict__ rd_elems, const int32_t *__restrict__ inod,
+                                                  const double *__restrict__ geom, const T *__restrict__ hist_n,
+                                                  const T *__restrict__ x2, const int32_t *__restrict__ store_eq,
+                                                  double *__restrict__ g_lam, double *__restrict__ g_mu, double dt,
+                                                  int lambda_2mu)
+{
+    __shared__ T su[kGradElems][27][3][S];
+    __shared__ T sp[kGradElems][27][3][S];
+    const int le = threadIdx.x / 27, q = threadIdx.x % 27;
+    const int e = blockIdx.x * kGradElems + le;
+    const bool active = threadIdx.x < 27 * kGradElems && e < nel_rd;
+    if (active) {
+        const int sn = rd_store[size_t(e) * 27 + q];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            const int pos = 3 * sn + c;
+            const int eq = store_eq[pos];
+#pragma unroll
+            for (int s = 0; s < S; ++s) {
+                su[le][q][c][s] = hist_n[size_t(pos) * S + s];
+                sp[le][q][c][s] = x2[size_t(eq) * S + s];
+            }
+        }
+    }
+    __syncthreads();
+    if (!active) return;
+    const int aq = q % 3, bq = (q / 3) % 3, cq = q / 9;
+    const double *gm = geom + (size_t(e) * 27 + q) * 10;
+    double J[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) J[k] = gm[k];
+    const double fac0 = gm[9];
+    double tl = 0.0, tm = 0.0;
+    for (int s = 0; s < S; ++s) {
+        double du[3][3], dp[3][3];   // d(comp)/d(xi_m)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            double ux = 0, uy = 0, uz = 0, px = 0, py = 0, pz = 0;
+#pragma unroll
+            for (int t = 0; t < 3; ++t) {
+                const int nx = c_node_at[9 * cq + 3 * bq + t];
+                const int ny = c_node_at[9 * cq + 3 * t + aq];
+                const int nz = c_node_at[9 * t + 3 * bq + aq];
+                ux += c_D[aq][t] * double(su[le][nx][c][s]);
+                uy += c_D[bq][t] * double(su[le][ny][c][s]);
+                uz += c_D[cq][t] * double(su[le][nz][c][s]);
+                px += c_D[aq][t] * double(sp[le][nx][c][s]);
+                py += c_D[bq][t] * double(sp[le][ny][c][s]);
+                pz += c_D[cq][t] * double(sp[le][nz][c][s]);
+            }
+            du[c][0] = ux; du[c][1] = uy; du[c][2] = uz;
+            dp[c][0] = px; dp[c][1] = py; dp[c][2] = pz;
+        }
+        // physical gradients: d/dx_k = sum_m DJI(m,k) d/dxi_m
+        double gu[3][3], gp[3][3];
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                gu[c][k] = du[c][0] * J[0 * 3 + k] + du[c][1] * J[1 * 3 + k] + du[c][2] * J[2 * 3 + k];
+                gp[c][k] = dp[c][0] * J[0 * 3 + k] + dp[c][1] * J[1 * 3 + k] + dp[c][2] * J[2 * 3 + k];
+            }
+        const double u1x = gu[0][0], u2x = gu[1][0], u3x = gu[2][0];
+        const double u1y = gu[0][1], u2y = gu[1][1], u3y = gu[2][1];
+        const double u1z = gu[0][2], u2z = gu[1][2], u3z = gu[2][2];
+        const double p1x = gp[0][0], p2x = gp[1][0], p3x = gp[2][0];
+        const double p1y = gp[0][1], p2y = gp[1][1], p3y = gp[2][1];
+        const double p1z = gp[0][2], p2z = gp[1][2], p3z = gp[2][2];
+        const double sl = (u1x + u2y + u3z) * (p1x + p2y + p3z);
+        const double cross = (p1y + p2x) * (u1y + u2x) + (p1z + p3x) * (u1z + u3x) + (p3y + p2z) * (u3y + u2z);
+        double sm;
+        if (!lambda_2mu) sm = 2.0 * (u1x * p1x + u2y * p2y + u3z * p3z) + cross;
+        else sm = -2.0 * (p1x * (u2y + u3z) + p2y * (u1x + u3z) + p3z * (u1x + u2y)) + cross;
+        tl += (sl * fac0) * dt;
+        tm += (sm * fac0) * dt;
+    }
+    const int node = inod[size_t(rd_elems[e]) * 27 + c_node_at[q]];
+    atomicAdd(g_lam + node, tl);
+    atomicAdd(g_mu + node, tm);
+}
+
+// ----------------------------------------------------------------------------
+// misfit (Compute_Misfit, S4/Solver_PETSc_Inverse.F90:591-657)
+
+template <typename T, int S>
+__global__ void k_misfit_terms(int nstep, int nstore, int nrec3, int nslot, const int32_t *__restrict__ ptr,
+                               const int32_t *__restrict__ qlist, const int32_t *__restrict__ emap,
+                               const T *__restrict__ hist, const double *__restrict__ dis, double *__restrict__ terms)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (nstep + 1) * S) return;
+    const int s = t % S, n = t / S;
+    double d = 0.0;
+    for (int sl = 0; sl < nslot; ++sl) {
+        double r = 0.0;
+        for (int k = ptr[sl]; k < ptr[sl + 1]; ++k) {
+            const int q = qlist[k];
+            r += double(hist[(size_t(n) * nstore + emap[q]) * S + s]) - dis[(size_t(s) * nrec3 + q) * (nstep + 1) + n];
+        }
+        d += r * r;
+    }
+    terms[size_t(s) * (nstep + 1) + n] = d;
+}
+
+__global__ void k_misfit_sum(int nshot, int nstep, double dt, const double *__restrict__ terms, double *__restrict__ cost)
+{
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    double total = 0.0;
+    for (int s = 0; s < nshot; ++s) {
+        double c = 0.0;
+        for (int n = nstep; n >= 1; --n) c = c + 0.5 * terms[size_t(s) * (nstep + 1) + n] * dt;
+        cost[1 + s] = c;
+        total += c;
+    }
+    cost[0] = total;
+}
+
+// ----------------------------------------------------------------------------
+// host side
+
+static int blocks_for(int64_t work, int threads, int64_t cap = 148LL * 32)
+{
+    int64_t b = (work + threads - 1) / threads;
+    if (b < 1) b = 1;
+    if (b > cap) b = cap;
+    return int(b);
+}
+
+template <typename T>
+static int scale_operator_t(hrn_ctx *c)
+{
+    const int th = 256;
+    if (c->d_fwd.bytes != size_t(c->nnz) * sizeof(T)) HRN_CUDA(c, c->d_fwd.alloc(size_t(c->nnz) * sizeof(T)));
+    if (c->d_adj.bytes != size_t(c->nnz) * sizeof(T)) HRN_CUDA(c, c->d_adj.alloc(size_t(c->nnz) * sizeof(T)));
+    if (c->nnz == 0) return 0;
+    k_scale_fwd<T><<<blocks_for(c->nnz, th), th, 0, c->stream>>>(c->nnz, c->d_rowidx.as<int32_t>(), c->d_raw.as<double>(),
+                                                                  c->d_im.as<double>(), c->d_fwd.as<T>());
+    HRN_CUDA(c, cudaGetLastError());
+    k_scale_adj<T><<<blocks_for(c->nnz, th), th, 0, c->stream>>>(c->nnz, c->d_permT.as<int64_t>(), c->d_rowidx.as<int32_t>(),
+                                                                  c->d_colx.as<uint32_t>(), c->d_raw.as<double>(),
+                                                                  c->d_diag_m.as<double>(), c->d_im.as<double>(), c->d_adj.as<T>());
+    HRN_CUDA(c, cudaGetLastError());
+    return 0;
+}
+
+int launch_scale_operator(hrn_ctx *c)
+{
+    return c->precision == HRN_FP64 ? scale_operator_t<double>(c) : scale_operator_t<float>(c);
+}
+
+// lanes per row of the stage kernel
+constexpr int kLanes = 8;
+
+template <typename T, int S, int STAGE>
+static void launch_stage(const StageArgs<T> &a, cudaStream_t st)
+{
+    const int th = 256;
+    const int64_t threads = int64_t(a.n) * kLanes;
+    const int blocks = int((threads + th - 1) / th);
+    rk4_stage<T, S, STAGE, kLanes><<<blocks, th, 0, st>>>(a);
+}
+
+struct StageTimer {
+    hrn_ctx *c;
+    size_t used = 0;
+    explicit StageTimer(hrn_ctx *cc) : c(cc) {}
+    cudaEvent_t get()
+    {
+        if (used == c->ev_pool.size()) {
+            cudaEvent_t e;
+            cudaEventCreate(&e);
+            c->ev_pool.push_back(e);
+        }
+        return c->ev_pool[used++];
+    }
+};
+
+
+// ----------------------------------------------------------------------------
+// element geometry at the 27 GLL points: DJI (row m = xi direction, column k =
+// x direction) and w*detJ, from the Jacobian of S4/Element_Matrices_3D.F90:111-139.
+// With the GLL rule only the 3 nodes on the xi_m line through a point carry a
+// nonzero dN/dxi_m there, so DJ(i,m) is a 3-term sum; the terms are added in
+// ascending local node order (the order of MATMUL(XT, DFXI)) without fused
+// multiply-adds, so DJ, detJ and DJI equal the reference's left-to-right values.
+__constant__ double c_w[3];
+__constant__ unsigned char c_gnode[27][3][3];   // [q][m][t] local nodes on the xi_m line, ascending
+__constant__ double c_gd[27][3][3];             // matching dN/dxi_m values at q
+
+__global__ void k_geometry(int nel, const int32_t *__restrict__ elems, const int32_t *__restrict__ inod,
+                           const double *__restrict__ xyz, double *__restrict__ out, int *__restrict__ bad)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nel * 27) return;
+    const int le = t / 27, q = t % 27;
+    const int e = elems ? elems[le] : le;
+    const int aq = q % 3, bq = (q / 3) % 3, cq = q / 9;
+    const int32_t *nd = inod + size_t(e) * 27;
+    double dj[3][3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int m = 0; m < 3; ++m) {
+            double s = 0.0;
+#pragma unroll
+            for (int tt = 0; tt < 3; ++tt)
+                s = __dadd_rn(s, __dmul_rn(xyz[size_t(nd[c_gnode[q][m][tt]]) * 3 + i], c_gd[q][m][tt]));
+            dj[i][m] = s;
+        }
+#define M_(a, b) __dmul_rn(a, b)
+#define A_(a, b) __dadd_rn(a, b)
+#define S_(a, b) __dsub_rn(a, b)
+    const double detj = S_(S_(S_(A_(A_(M_(M_(dj[0][0], dj[1][1]), dj[2][2]), M_(M_(dj[1][0], dj[2][1]), dj[0][2])),
+                                     M_(M_(dj[2][0], dj[0][1]), dj[1][2])),
+                                  M_(M_(dj[0][2], dj[1][1]), dj[2][0])),
+                               M_(M_(dj[1][2], dj[2][1]), dj[0][0])),
+                            M_(M_(dj[2][2], dj[0][1]), dj[1][0]));
+    double *o = out + size_t(t) * 10;
+    if (!(detj > 0.0)) {
+        atomicExch(bad, 1);
+        for (int k = 0; k < 10; ++k) o[k] = 0.0;
+        return;
+    }
+    double ji[9];
+    ji[0] = S_(M_(dj[2][2], dj[1][1]), M_(dj[2][1], dj[1][2]));
+    ji[1] = A_(-M_(dj[2][2], dj[0][1]), M_(dj[2][1], dj[0][2]));
+    ji[2] = S_(M_(dj[1][2], dj[0][1]), M_(dj[1][1], dj[0][2]));
+    ji[3] = A_(-M_(dj[2][2], dj[1][0]), M_(dj[2][0], dj[1][2]));
+    ji[4] = S_(M_(dj[2][2], dj[0][0]), M_(dj[2][0], dj[0][2]));
+    ji[5] = A_(-M_(dj[1][2], dj[0][0]), M_(dj[1][0], dj[0][2]));
+    ji[6] = S_(M_(dj[2][1], dj[1][0]), M_(dj[2][0], dj[1][1]));
+    ji[7] = A_(-M_(dj[2][1], dj[0][0]), M_(dj[2][0], dj[0][1]));
+    ji[8] = S_(M_(dj[1][1], dj[0][0]), M_(dj[1][0], dj[0][1]));
+#pragma unroll
+    for (int k = 0; k < 9; ++k) o[k] = __ddiv_rn(ji[k], detj);
+    o[9] = M_(M_(M_(c_w[aq], c_w[bq]), c_w[cq]), detj);
+#undef M_
+#undef A_
+#undef S_
+}
+
+static int upload_tables(hrn_ctx *c)
+{
+    static const int ijk[27][3] = {{2, 0, 0}, {2, 2, 0}, {0, 2, 0}, {0, 0, 0}, {2, 0, 2}, {2, 2, 2}, {0, 2, 2}, {0, 0, 2},
+                                   {2, 1, 0}, {1, 2, 0}, {0, 1, 0}, {1, 0, 0}, {2, 0, 1}, {2, 2, 1}, {0, 2, 1}, {0, 0, 1},
+                                   {2, 1, 2}, {1, 2, 2}, {0, 1, 2}, {1, 0, 2}, {1, 1, 0}, {2, 1, 1}, {1, 2, 1}, {0, 1, 1},
+                                   {1, 0, 1}, {1, 1, 2}, {1, 1, 1}};
+    int node_at[27];
+    for (int i = 0; i < 27; ++i) node_at[9 * ijk[i][2] + 3 * ijk[i][1] + ijk[i][0]] = i;
+    // derivative of the 1D quadratic Lagrange basis l_b at GLL point xi_a
+    const double D[3][3] = {{-1.5, 2.0, -0.5}, {-0.5, 0.0, 0.5}, {0.5, -2.0, 1.5}};
+    const double w[3] = {0.33333333333333333333, 1.33333333333333333333, 0.33333333333333333333};
+    HRN_CUDA(c, cudaMemcpyToSymbol(c_node_at, node_at, sizeof(node_at)));
+    HRN_CUDA(c, cudaMemcpyToSymbol(c_D, D, sizeof(D)));
+    HRN_CUDA(c, cudaMemcpyToSymbol(c_w, w, sizeof(w)));
+    unsigned char gnode[27][3][3];
+    double gd[27][3][3];
+    for (int q = 0; q < 27; ++q) {
+        const int qi[3] = {q % 3, (q / 3) % 3, q / 9};
+        for (int m = 0; m < 3; ++m) {
+            int t = 0;
+            for (int I = 0; I < 27; ++I) {   // ascending local node order
+                bool on = true;
+                for (int k = 0; k < 3; ++k)
+                    if (k != m && ijk[I][k] != qi[k]) on = false;
+                if (!on) continue;
+                gnode[q][m][t] = (unsigned char)I;
+                gd[q][m][t] = D[qi[m]][ijk[I][m]];
+                ++t;
+            }
+        }
+    }
+    HRN_CUDA(c, cudaMemcpyToSymbol(c_gnode, gnode, sizeof(gnode)));
+    HRN_CUDA(c, cudaMemcpyToSymbol(c_gd, gd, sizeof(gd)));
+    return 0;
+}
+
+int build_rd_geometry(hrn_ctx *c)
+{
+    if (int rc = upload_tables(c)) return rc;
+    std::vector<int32_t> rd;
+    for (int e = 0; e < c->nel; ++e)
+        if (c->h_mtel[e] == 1) rd.push_back(e);
+    c->nel_rd = int(rd.size());
+    HRN_CUDA(c, c->d_rd_elems.alloc(rd.size() * 4));
+    if (!rd.empty()) HRN_CUDA(c, cudaMemcpy(c->d_rd_elems.p, rd.data(), rd.size() * 4, cudaMemcpyHostToDevice));
+    HRN_CUDA(c, c->d_rd_geom.alloc(size_t(c->nel_rd) * 27 * 10 * 8));
+    HRN_CUDA(c, c->d_asm_geom.alloc(size_t(c->nel) * 27 * 10 * 8));
+    HRN_CUDA(c, c->d_asm_err.alloc(16));
+    HRN_CUDA(c, cudaMemsetAsync(c->d_asm_err.p, 0, 16, c->stream));
+    const int th = 256;
+    if (c->nel_rd > 0)
+        k_geometry<<<(c->nel_rd * 27 + th - 1) / th, th, 0, c->stream>>>(c->nel_rd, c->d_rd_elems.as<int32_t>(), c->d_inod.as<int32_t>(),
+                                                                           c->d_xyz.as<double>(), c->d_rd_geom.as<double>(), c->d_asm_err.as<int>());
+    k_geometry<<<(c->nel * 27 + th - 1) / th, th, 0, c->stream>>>(c->nel, nullptr, c->d_inod.as<int32_t>(), c->d_xyz.as<double>(),
+                                                                   c->d_asm_geom.as<double>(), c->d_asm_err.as<int>());
+    HRN_CUDA(c, cudaGetLastError());
+    int bad = 0;
+    HRN_CUDA(c, cudaMemcpyAsync(&bad, c->d_asm_err.p, 4, cudaMemcpyDeviceToHost, c->stream));
+    HRN_CUDA(c, cudaStreamSynchronize(c->stream));
+    if (bad) return set_error(c, HRN_EMESH, "non-positive Jacobian determinant in an element");
+    c->have_rd_store = false;
+    return 0;
+}
+
+// History node index of every RD element node (nodes of RD elements are all stored).
+static int build_rd_store(hrn_ctx *c)
+{
+    if (c->have_rd_store) return 0;
+    std::vector<int32_t> inv(size_t(c->neq), -1);
+    for (int p = 0; p < c->nstore; ++p) inv[c->h_store_eq[p]] = p;
+    std::vector<int32_t> rs(size_t(c->nel_rd) * 27);
+    int k = 0;
+    for (int e = 0; e < c->nel; ++e) {
+        if (c->h_mtel[e] != 1) continue;
+        for (int i = 0; i < 27; ++i) {
+            const int node = c->h_inod[size_t(e) * 27 + i];
+            int pos[3];
+            for (int d = 0; d < 3; ++d) {
+                const int eq = c->h_id[size_t(node) * 9 + d];
+                pos[d] = eq >= 0 ? inv[eq] : -1;
+            }
+            if (pos[0] < 0 || pos[0] % 3 != 0 || pos[1] != pos[0] + 1 || pos[2] != pos[0] + 2)
+                return set_error(c, HRN_EARG, "history equations must hold the x, y, z displacement of every regular-domain node, in that order");
+            rs[size_t(k) * 27 + i] = pos[0] / 3;
+        }
+        ++k;
+    }
+    HRN_CUDA(c, c->d_rd_store.alloc(rs.size() * 4));
+    if (!rs.empty()) HRN_CUDA(c, cudaMemcpy(c->d_rd_store.p, rs.data(), rs.size() * 4, cudaMemcpyHostToDevice));
+    c->have_rd_store = true;
+    return 0;
+}
+
+// ----------------------------------------------------------------------------
+// time loops
+
+template <typename T, int S>
+static void launch_step(hrn_ctx *c, StageArgs<T> a, T *X, T *Y, StageTimer *tm)
+{
+    const size_t vn = size_t(c->neq) * S;
+    T *kb = c->d_KB.as<T>();
+    a.x1 = X; a.x2 = X + vn; a.x3 = X + 2 * vn;
+    a.kb1 = kb; a.kb2 = kb + vn; a.kb3 = kb + 2 * vn;
+    a.y1 = Y; a.y2 = Y + vn; a.y3 = Y + 2 * vn;
+    for (int st = 1; st <= 4; ++st) {
+        if (tm) cudaEventRecord(tm->get(), c->stream);
+        a.kb_out = st < 4 ? kb + size_t(st - 1) * vn : nullptr;
+        switch (st) {
+        case 1: launch_stage<T, S, 1>(a, c->stream); break;
+        case 2: launch_stage<T, S, 2>(a, c->stream); break;
+        case 3: launch_stage<T, S, 3>(a, c->stream); break;
+        default: launch_stage<T, S, 4>(a, c->stream); break;
+        }
+        if (tm) cudaEventRecord(tm->get(), c->stream);
+        a.hist = nullptr;   // history only in stage 1
+    }
+}
+
+static double sum_timer(hrn_ctx *c, const StageTimer &tm)
+{
+    double tot = 0.0;
+    for (size_t i = 0; i + 1 < tm.used; i += 2) {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, c->ev_pool[i], c->ev_pool[i + 1]);
+        tot += ms;
+    }
+    return tot;
+}
+
+template <typename T, int S>
+static int forward_t(hrn_ctx *c)
+{
+    const size_t vn = size_t(c->neq) * S;
+    T *X0 = c->d_X.as<T>(), *X1 = X0 + 3 * vn;
+    cudaEvent_t t0, t1;
+    cudaEventCreate(&t0);
+    cudaEventCreate(&t1);
+    cudaEventRecord(t0, c->stream);
+    HRN_CUDA(c, cudaMemsetAsync(X0, 0, 3 * vn * sizeof(T), c->stream));
+    if (c->nslot_f > 0) {
+        const int64_t tot = int64_t(c->nstep + 1) * c->nslot_f * S;
+        k_src_fwd<T, S><<<blocks_for(tot, 256), 256, 0, c->stream>>>(c->nstep, c->nslot_f, c->d_fslot_eq.as<int32_t>(),
+                                                                     c->d_fsrc_b.as<double>(), c->d_ftab.as<double>(),
+                                                                     c->d_im.as<double>(), c->d_srcv_f.as<T>());
+        HRN_CUDA(c, cudaGetLastError());
+    }
+    StageArgs<T> a{};
+    a.n = c->neq;
+    a.rowptr = c->d_rowptr.as<int32_t>();
+    a.colx = c->d_colx.as<uint32_t>();
+    a.val = c->d_fwd.as<T>();
+    a.slot = c->d_slot_f.as<int32_t>();
+    a.nslot = c->nslot_f;
+    a.store_pos = c->d_store_pos.as<int32_t>();
+    a.c = T(0.5 * c->dt);
+    a.D = T(c->dt);
+    a.d6 = T(c->dt / 6.0);
+    StageTimer tm(c);
+    for (int n = 0; n <= c->nstep; ++n) {
+        a.srcv = c->nslot_f ? c->d_srcv_f.as<T>() + size_t(n) * 4 * c->nslot_f * S : nullptr;
+        a.hist = c->d_hist.as<T>() + size_t(n) * c->nstore * S;
+        T *X = (n & 1) ? X1 : X0, *Y = (n & 1) ? X0 : X1;
+        launch_step<T, S>(c, a, X, Y, c->timing ? &tm : nullptr);
+    }
+    HRN_CUDA(c, cudaGetLastError());
+    cudaEventRecord(t1, c->stream);
+    HRN_CUDA(c, cudaEventSynchronize(t1));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, t0, t1);
+    cudaEventDestroy(t0);
+    cudaEventDestroy(t1);
+    c->last_total_ms = ms;
+    c->last_stage_ms = c->timing ? sum_timer(c, tm) : 0.0;
+    c->last_stage_launches = c->timing ? int64_t(tm.used / 2) : 0;
+    c->have_forward = true;
+    c->have_phist = false;
+    return 0;
+}
+
+template <typename T, int S>
+static int adjoint_t(hrn_ctx *c, int lambda_2mu, int keep_p)
+{
+    if (int rc = build_rd_store(c)) return rc;
+    const size_t vn = size_t(c->neq) * S;
+    T *X0 = c->d_X.as<T>(), *X1 = X0 + 3 * vn;
+    cudaEvent_t t0, t1;
+    cudaEventCreate(&t0);
+    cudaEventCreate(&t1);
+    cudaEventRecord(t0, c->stream);
+    HRN_CUDA(c, cudaMemsetAsync(X0, 0, 3 * vn * sizeof(T), c->stream));
+    HRN_CUDA(c, cudaMemsetAsync(c->d_g.p, 0, size_t(2) * c->nj * 8, c->stream));
+    if (keep_p) {
+        const size_t hb = size_t(c->nstep + 1) * c->nstore * S * sizeof(T);
+        HRN_CUDA(c, c->d_phist.alloc(hb));
+        HRN_CUDA(c, cudaMemsetAsync(c->d_phist.p, 0, hb, c->stream));
+    }
+    StageArgs<T> a{};
+    a.n = c->neq;
+    a.rowptr = c->d_rowptrT.as<int32_t>();
+    a.colx = c->d_colxT.as<uint32_t>();
+    a.val = c->d_adj.as<T>();
+    a.slot = c->d_slot_a.as<int32_t>();
+    a.nslot = c->nslot_a;
+    a.srcv = c->d_srcv_a.as<T>();
+    a.store_pos = c->d_store_pos.as<int32_t>();
+    a.c = T(-0.5 * c->dt);
+    a.D = T(-c->dt);
+    a.d6 = T(-c->dt / 6.0);
+    StageTimer tm(c);
+    double *gl = c->d_g.as<double>(), *gmu = gl + c->nj;
+    const int gblocks = (c->nel_rd + kGradElems - 1) / kGradElems;
+    int it = 0;
+    for (int n = c->nstep; n >= 1; --n, ++it) {
+        if (c->nslot_a > 0)
+            k_src_adj<T, S><<<(c->nslot_a * S + 127) / 128, 128, 0, c->stream>>>(
+                n, c->nstep, c->nstore, c->nrec3, c->nslot_a, c->d_aslot_ptr.as<int32_t>(), c->d_aslot_q.as<int32_t>(),
+                c->d_aslot_eq.as<int32_t>(), c->d_eqdis_map.as<int32_t>(), c->d_hist.as<T>(), c->d_dis.as<double>(),
+                c->d_im.as<double>(), c->d_srcv_a.as<T>());
+        a.hist = keep_p ? c->d_phist.as<T>() + size_t(n) * c->nstore * S : nullptr;
+        T *X = (it & 1) ? X1 : X0, *Y = (it & 1) ? X0 : X1;
+        launch_step<T, S>(c, a, X, Y, c->timing ? &tm : nullptr);
+        if (n <= c->nstep - 1 && c->nel_rd > 0)
+            k_gradient<T, S><<<gblocks, 128, 0, c->stream>>>(c->nel_rd, c->d_rd_store.as<int32_t>(), c->d_rd_elems.as<int32_t>(),
+                                                             c->d_inod.as<int32_t>(), c->d_rd_geom.as<double>(),
+                                                             c->d_hist.as<T>() + size_t(n) * c->nstore * S, X + vn,
+                                                             c->d_store_eq.as<int32_t>(), gl, gmu, c->dt, lambda_2mu);
+    }
+    HRN_CUDA(c, cudaGetLastError());
+    cudaEventRecord(t1, c->stream);
+    HRN_CUDA(c, cudaEventSynchronize(t1));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, t0, t1);
+    cudaEventDestroy(t0);
+    cudaEventDestroy(t1);
+    c->last_total_ms = ms;
+    c->last_stage_ms = c->timing ? sum_timer(c, tm) : 0.0;
+    c->last_stage_launches = c->timing ? int64_t(tm.used / 2) : 0;
+    c->have_phist = keep_p != 0;
+    return 0;
+}
+
+template <typename T, int S>
+static int misfit_t(hrn_ctx *c, double *cost)
+{
+    const int tot = (c->nstep + 1) * S;
+    k_misfit_terms<T, S><<<(tot + 127) / 128, 128, 0, c->stream>>>(c->nstep, c->nstore, c->nrec3, c->nslot_a,
+                                                                   c->d_aslot_ptr.as<int32_t>(), c->d_aslot_q.as<int32_t>(),
+                                                                   c->d_eqdis_map.as<int32_t>(), c->d_hist.as<T>(),
+                                                                   c->d_dis.as<double>(), c->d_mis_terms.as<double>());
+    k_misfit_sum<<<1, 1, 0, c->stream>>>(S, c->nstep, c->dt, c->d_mis_terms.as<double>(), c->d_cost.as<double>());
+    HRN_CUDA(c, cudaGetLastError());
+    std::vector<double> h(size_t(1 + S));
+    HRN_CUDA(c, cudaMemcpyAsync(h.data(), c->d_cost.p, h.size() * 8, cudaMemcpyDeviceToHost, c->stream));
+    HRN_CUDA(c, cudaStreamSynchronize(c->stream));
+    for (int s = 0; s < 1 + S; ++s) cost[s] = h[s];
+    return 0;
+}
+
+#define HRN_DISPATCH_S(FN, T, ...)                        \
+    switch (c->nshot) {                                   \
+    case 1: return FN<T, 1>(c, ##__VA_ARGS__);            \
+    case 2: return FN<T, 2>(c, ##__VA_ARGS__);            \
+    case 3: return FN<T, 3>(c, ##__VA_ARGS__);            \
+    case 4: return FN<T, 4>(c, ##__VA_ARGS__);            \
+    case 5: return FN<T, 5>(c, ##__VA_ARGS__);            \
+    case 6: return FN<T, 6>(c, ##__VA_ARGS__);            \
+    case 7: return FN<T, 7>(c, ##__VA_ARGS__);            \
+    case 8: return FN<T, 8>(c, ##__VA_ARGS__);            \
+    default: return set_error(c, HRN_EARG, "nshot out of range"); \
+    }
+
+int run_forward(hrn_ctx *c)
+{
+    if (c->precision == HRN_FP64) { HRN_DISPATCH_S(forward_t, double) }
+    HRN_DISPATCH_S(forward_t, float)
+}
+
+int run_adjoint_gradient(hrn_ctx *c, int lambda_2mu, int keep_p)
+{
+    if (c->precision == HRN_FP64) { HRN_DISPATCH_S(adjoint_t, double, lambda_2mu, keep_p) }
+    HRN_DISPATCH_S(adjoint_t, float, lambda_2mu, keep_p)
+}
+
+int run_misfit(hrn_ctx *c, double *cost)
+{
+    if (c->precision == HRN_FP64) { HRN_DISPATCH_S(misfit_t, double, cost) }
+    HRN_DISPATCH_S(misfit_t, float, cost)
+}
+
+}  // namespace hrn

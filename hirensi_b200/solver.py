@@ -1,0 +1,217 @@
+"""Host-side mirror of HiReNSI's explicit forward / adjoint / gradient interface.
+
+``Solver`` owns one device context of libhirensi_b200.so.  The module-level
+functions keep the names and argument meaning of the reference routines they
+replace (S4 = step_4_3D_Forward_and_Inverse):
+
+* ``EXPLICIT_RK4_PETSC_PML_3D``        S4/Solver_PETSc_Explicit.F90:660-1117
+* ``EXPLICIT_RK4_PETSC_PML_3D_Adjoint_Control_OtD``
+                                         :1125-1405 followed by :1413-1522
+* ``Compute_Misfit``                     S4/Solver_PETSc_Inverse.F90:591-657
+
+Errors raise ``HrnError`` with the library's status code, where the reference
+would STOP the process.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import capi
+from .capi import HrnError, dptr, f64, i32, iptr
+
+
+class Solver:
+    """One device context (stepping precision 'fp64' or 'fp32')."""
+
+    def __init__(self, precision: str = "fp64", device: int = 0):
+        self._L = capi.load()
+        prec = {"fp64": capi.HRN_FP64, "fp32": capi.HRN_FP32}[precision]
+        h = C.c_void_p()
+        rc = self._L.hrn_create(device, prec, C.byref(h))
+        if rc != capi.HRN_OK:
+            raise HrnError(rc, "hrn_create failed (no CUDA device?)")
+        self.h = h
+        self.precision = precision
+        self.nshot = 0
+        self.nstep = 0
+        self.nstore = 0
+        self.nrec3 = 0
+        self.nj = 0
+        self.neq = 0
+
+    # -- plumbing ---------------------------------------------------------------
+    def _check(self, rc):
+        if rc != capi.HRN_OK:
+            msg = self._L.hrn_last_error(self.h)
+            raise HrnError(rc, msg.decode() if msg else "")
+
+    def close(self):
+        if getattr(self, "h", None):
+            self._L.hrn_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_stream(self, stream_ptr: int | None):
+        self._check(self._L.hrn_set_stream(self.h, C.c_void_p(stream_ptr or 0)))
+
+    def set_timing(self, on: bool):
+        self._check(self._L.hrn_set_timing(self.h, int(bool(on))))
+
+    def last_timing(self):
+        tot, st, n = C.c_double(), C.c_double(), C.c_int64()
+        self._check(self._L.hrn_last_timing(self.h, C.byref(tot), C.byref(st), C.byref(n)))
+        return tot.value, st.value, n.value
+
+    # -- operator ---------------------------------------------------------------
+    def set_operator_csr(self, Cm, Km, Gm, diag_m):
+        """Caller-assembled C, K, G as (ia, ja, a) CSR triples and DIAG_M."""
+        arrs = []
+        for ia, ja, a in (Cm, Km, Gm):
+            arrs.append((i32(ia), i32(ja), f64(a)))
+        dm = f64(diag_m)
+        neq = dm.size
+        flat = []
+        for ia, ja, a in arrs:
+            if ia.size != neq + 1:
+                raise ValueError("row pointer length must be neq + 1")
+            flat += [iptr(ia), iptr(ja), dptr(a)]
+        self._check(self._L.hrn_set_operator_csr(self.h, neq, *flat, dptr(dm)))
+        self.neq = neq
+
+    def set_mesh(self, mesh, rho=2.0e-3):
+        """Geometry and numbering of a hirensi_b200.mesh.Mesh."""
+        rho_el = f64(np.full(mesh.nel, rho) if np.isscalar(rho) else rho)
+        self._mesh_keep = (f64(mesh.xyz), i32(mesh.inod), i32(mesh.mtel), i32(mesh.ID), rho_el, f64(mesh.pml_param))
+        xyz, inod, mtel, idm, rho_el, pml = self._mesh_keep
+        self._check(self._L.hrn_set_mesh(self.h, mesh.nj, mesh.nel, mesh.neq, dptr(xyz), iptr(inod), iptr(mtel),
+                                         iptr(idm), dptr(rho_el), dptr(pml)))
+        self.nj = mesh.nj
+        self.neq = mesh.neq
+
+    def assemble(self, lam, mu):
+        self._check(self._L.hrn_assemble(self.h, dptr(f64(lam)), dptr(f64(mu))))
+
+    def operator_csr(self, which: int):
+        nnz = C.c_int64()
+        self._check(self._L.hrn_get_operator_csr(self.h, which, None, None, None, C.byref(nnz)))
+        ia = np.zeros(self.neq + 1, np.int32)
+        ja = np.zeros(nnz.value, np.int32)
+        a = np.zeros(nnz.value)
+        self._check(self._L.hrn_get_operator_csr(self.h, which, iptr(ia), iptr(ja), dptr(a), C.byref(nnz)))
+        return ia, ja, a
+
+    def diag_m(self):
+        d = np.zeros(self.neq)
+        self._check(self._L.hrn_get_diag_m(self.h, dptr(d)))
+        return d
+
+    # -- problem ----------------------------------------------------------------
+    def set_history(self, store_eq):
+        se = i32(store_eq)
+        self._check(self._L.hrn_set_history(self.h, se.size, iptr(se)))
+        self.nstore = se.size
+
+    def set_shots(self, nstep: int, dt: float, src_eq, src_b, ftab):
+        """src_b [nsrc, nshot] unscaled force entries, ftab [nshot, nstep+1, 3]."""
+        se = i32(src_eq)
+        sb = f64(src_b)
+        ft = f64(ftab)
+        if ft.ndim == 2:
+            ft = ft[None]
+        nshot = ft.shape[0]
+        if sb.ndim == 1:
+            sb = sb[:, None]
+        if sb.shape != (se.size, nshot) or ft.shape != (nshot, nstep + 1, 3):
+            raise ValueError("src_b must be [nsrc, nshot] and ftab [nshot, nstep+1, 3]")
+        self._check(self._L.hrn_set_shots(self.h, nshot, nstep, float(dt), se.size, iptr(se) if se.size else None,
+                                          dptr(np.ascontiguousarray(sb)) if se.size else None, dptr(ft)))
+        self.nshot, self.nstep, self.dt = nshot, nstep, dt
+
+    def set_receivers(self, eqdis, eqdis_map):
+        e, m = i32(eqdis), i32(eqdis_map)
+        self._check(self._L.hrn_set_receivers(self.h, e.size, iptr(e), iptr(m)))
+        self.nrec3 = e.size
+
+    # -- time loops ---------------------------------------------------------------
+    def forward(self):
+        self._check(self._L.hrn_forward(self.h))
+
+    def history(self, shot: int = 0) -> np.ndarray:
+        u = np.zeros((self.nstep + 1, self.nstore))
+        self._check(self._L.hrn_get_history(self.h, shot, dptr(u)))
+        return u
+
+    def traces(self) -> np.ndarray:
+        t = np.zeros((self.nshot, self.nrec3, self.nstep + 1))
+        self._check(self._L.hrn_get_traces(self.h, dptr(t)))
+        return t
+
+    def _dis(self, dis_meas):
+        d = f64(dis_meas)
+        if d.ndim == 2:
+            d = d[None]
+        if d.shape != (self.nshot, self.nrec3, self.nstep + 1):
+            raise ValueError("dis_meas must be [nshot, nrec3, nstep+1]")
+        return d
+
+    def misfit(self, dis_meas) -> float:
+        d = self._dis(dis_meas)
+        out = C.c_double()
+        self._check(self._L.hrn_misfit(self.h, dptr(d), C.byref(out)))
+        return out.value
+
+    def adjoint_gradient(self, dis_meas, lambda_2mu: bool = False, keep_p: bool = False):
+        d = self._dis(dis_meas)
+        gl = np.zeros(self.nj)
+        gm = np.zeros(self.nj)
+        self._check(self._L.hrn_adjoint_gradient(self.h, dptr(d), int(lambda_2mu), int(keep_p), dptr(gl), dptr(gm)))
+        return gl, gm
+
+    def adjoint_history(self, shot: int = 0) -> np.ndarray:
+        p = np.zeros((self.nstep + 1, self.nstore))
+        self._check(self._L.hrn_get_adjoint_history(self.h, shot, dptr(p)))
+        return p
+
+
+# -- reference-named entry points ---------------------------------------------
+
+def EXPLICIT_RK4_PETSC_PML_3D(AK, DIAG_M, AC, AG, B, U_Store_Numbers_Global, NSTEP, DT, time_table,
+                              precision="fp64", solver: Solver | None = None):
+    """Forward RK4 with the assembled (unscaled) operator; returns U_Store_Mapping
+    as [NSTEP+1, NStore] (Fortran U_Store_Mapping(NStore, 0:NStep)).
+
+    ``time_table`` [NSTEP+1, 3] holds TIME_FUNCTION at T, T+DT, T+DT/2.  Unlike
+    the reference, the caller's matrices are not scaled in place.
+    """
+    s = solver or Solver(precision)
+    s.set_operator_csr(AC, AK, AG, DIAG_M)
+    s.set_history(U_Store_Numbers_Global)
+    b = f64(B)
+    nz = np.nonzero(b)[0]
+    s.set_shots(NSTEP, DT, nz, b[nz][:, None], np.asarray(time_table)[None])
+    s.forward()
+    return s.history(0)
+
+
+def Compute_Misfit(solver: Solver, Dis_meas) -> float:
+    """Sum over shots of 0.5*DT*sum_n ||U_Store(EqDis_MAP, n) - Dis_meas(n, :)||^2."""
+    return solver.misfit(Dis_meas)
+
+
+def EXPLICIT_RK4_PETSC_PML_3D_Adjoint_Control_OtD(solver: Solver, Dis_meas, lambda_2mu=False):
+    """Adjoint RK4 (OtD) with the zero-lag control accumulation fused in; returns the
+    raw (g_lambda, g_mu) the reference assembles before its sign flip."""
+    return solver.adjoint_gradient(Dis_meas, lambda_2mu=lambda_2mu)

@@ -1,0 +1,136 @@
+/*
+ * hirensi_b200.h -- C ABI of the B200 (sm_100a) implementation of HiReNSI's
+ * explicit 3D elastic forward / adjoint / gradient time loop.
+ *
+ * Plain C types only.  Every entry returns 0 on success or an HRN_E* code;
+ * hrn_last_error() gives the message.  Host arrays are read or written
+ * synchronously; the context owns all device memory.  A context is used by one
+ * host thread at a time.
+ *
+ * Array conventions (C row-major, 0-based unless stated):
+ *   CSR operators: PETSc AIJ layout (MatGetRowIJ / MatSeqAIJGetArray), 0-based,
+ *                  columns sorted within each row.
+ *   xyz[nj][3], inod[nel][27] (SHAPE_3_27 local order), id[nj][9] equation
+ *   numbers with -1 for a constrained DOF, pml_param[6][4].
+ *   u_store[nstep+1][nstore]   == Fortran U_Store_Mapping(NStore, 0:NStep)
+ *   dis_meas[nshot][nrec3][nstep+1]; per shot == Fortran Dis_meas(0:NStep, NNDH*3)
+ *
+ * Each entry names the reference routine it replaces (file:line inside the
+ * HiReNSI project, S4 = step_4_3D_Forward_and_Inverse).
+ */
+#ifndef HIRENSI_B200_H
+#define HIRENSI_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define HRN_OK 0
+#define HRN_EARG 1      /* invalid argument or size */
+#define HRN_ECUDA 2     /* CUDA runtime error */
+#define HRN_EOOM 3      /* device allocation failed */
+#define HRN_ESTATE 4    /* entry called before its prerequisites */
+#define HRN_ENAN 5      /* non-finite value detected in a reduction */
+#define HRN_EMESH 6     /* non-positive Jacobian, top PML zone or bad face load */
+
+#define HRN_FP64 0      /* stepping in FP64 */
+#define HRN_FP32 1      /* stepping in FP32, FP64 reductions */
+
+#define HRN_MAX_SHOTS 8 /* shots advanced together in one pass over the operator */
+
+typedef struct hrn_ctx hrn_ctx;
+
+/* Library version (major * 10000 + minor * 100 + patch). */
+int hrn_version(void);
+
+/* Create a context on CUDA device `device` with stepping precision HRN_FP64 or HRN_FP32. */
+int hrn_create(int device, int precision, hrn_ctx **out);
+int hrn_destroy(hrn_ctx *ctx);
+const char *hrn_last_error(const hrn_ctx *ctx);
+
+/* ---- operator ------------------------------------------------------------- */
+
+/* Drop-in for the assembled PETSc matrices AC, AK, AG and the vector DIAG_M that
+ * S4/Solve_Forward.F90:14-97 hands to EXPLICIT_RK4_PETSC_PML_3D.  Matrices are
+ * passed unscaled; the library applies -M^-1 (forward, S4/Solver_PETSc_Explicit.F90:815-824)
+ * and M (.) M^-1 (adjoint, :1222-1229) itself and never mutates caller data. */
+int hrn_set_operator_csr(hrn_ctx *ctx, int32_t neq,
+                         const int32_t *c_ia, const int32_t *c_ja, const double *c_a,
+                         const int32_t *k_ia, const int32_t *k_ja, const double *k_a,
+                         const int32_t *g_ia, const int32_t *g_ja, const double *g_a,
+                         const double *diag_m);
+
+/* Mesh for device assembly and for the gradient (the XYZ, INOD, MTEL, ID and
+ * PML_PARAM arguments of ASSEM_*_PETSC_3D and of ..._Control_OtD). */
+int hrn_set_mesh(hrn_ctx *ctx, int32_t nj, int32_t nel, int32_t neq,
+                 const double *xyz, const int32_t *inod, const int32_t *mtel,
+                 const int32_t *id, const double *rho_el, const double *pml_param);
+
+/* Device assembly of C, K, G and DIAG_M from nodal lambda, mu (host arrays [nj]):
+ * replaces ASSEM_REGULAR_DOMAIN_PETSC_3D (S4/Assemble_PETSc_3D.F90:6-184) and
+ * ASSEM_PML_PETSC_3D (:192-436).  The first call fixes the sparsity pattern
+ * (entries with a nonzero element contribution, as MAT_IGNORE_ZERO_ENTRIES). */
+int hrn_assemble(hrn_ctx *ctx, const double *lambda, const double *mu);
+
+/* Download the current operator (unscaled).  With ia/ja/a NULL only *nnz is set. */
+int hrn_get_operator_csr(hrn_ctx *ctx, int32_t which, int32_t *ia, int32_t *ja, double *a, int64_t *nnz);
+int hrn_get_diag_m(hrn_ctx *ctx, double *diag_m);
+
+/* ---- problem description --------------------------------------------------- */
+
+/* History equations U_Store_Numbers_Global (S3/PIC_Inversion_Data_Structure.F90:255-300). */
+int hrn_set_history(hrn_ctx *ctx, int32_t nstore, const int32_t *store_eq);
+
+/* Shots advanced together.  Source = nsrc entries of the unscaled force vector B
+ * per shot (src_b[nsrc][nshot], zero where a shot has no load at that equation),
+ * scaled by TIME_FUNCTION samples ftab[nshot][nstep+1][3] at T, T+dt, T+dt/2
+ * (S4/Solver_PETSc_Explicit.F90:983-995). */
+int hrn_set_shots(hrn_ctx *ctx, int32_t nshot, int32_t nstep, double dt,
+                  int32_t nsrc, const int32_t *src_eq, const double *src_b, const double *ftab);
+
+/* Receivers: EqDis (equations) and EqDis_MAP_U_Store_Numbers_Global (0-based
+ * positions in the history), S4/IO_Parallel_Inversion.F90:116-133. */
+int hrn_set_receivers(hrn_ctx *ctx, int32_t nrec3, const int32_t *eqdis, const int32_t *eqdis_map);
+
+/* ---- time loops ------------------------------------------------------------ */
+
+/* Forward RK4 for all shots, EXPLICIT_RK4_PETSC_PML_3D (S4/Solver_PETSc_Explicit.F90:660-1117).
+ * The history U_Store of every shot stays on the device. */
+int hrn_forward(hrn_ctx *ctx);
+int hrn_get_history(hrn_ctx *ctx, int32_t shot, double *u_store);
+/* Receiver traces U_Store(EqDis_MAP, 0:NStep) of every shot: traces[nshot][nrec3][nstep+1]. */
+int hrn_get_traces(hrn_ctx *ctx, double *traces);
+
+/* Compute_Misfit (S4/Solver_PETSc_Inverse.F90:591-657) summed over shots. */
+int hrn_misfit(hrn_ctx *ctx, const double *dis_meas, double *cost);
+
+/* Adjoint RK4 (OtD) with the zero-lag gradient fused into each step:
+ * EXPLICIT_RK4_PETSC_PML_3D_Adjoint_OtD (:1125-1405) followed by
+ * EXPLICIT_RK4_PETSC_PML_3D_Control_OtD (:1413-1522), summed over shots.
+ * g_lambda, g_mu [nj] receive the raw accumulated gradient (before the sign
+ * flip and mass scaling of S4/Program_Main.F90:412-455).  lambda_2mu selects
+ * ELEMENT_g_3D_v2.  keep_p stores the adjoint history for hrn_get_adjoint_history. */
+int hrn_adjoint_gradient(hrn_ctx *ctx, const double *dis_meas, int32_t lambda_2mu, int32_t keep_p,
+                         double *g_lambda, double *g_mu);
+int hrn_get_adjoint_history(hrn_ctx *ctx, int32_t shot, double *p_store);
+
+/* ---- streams and timing -------------------------------------------------------- */
+
+/* Launch all work of this context on `stream` (a cudaStream_t, NULL = the
+ * context's own stream).  The caller keeps the stream alive. */
+int hrn_set_stream(hrn_ctx *ctx, void *stream);
+
+/* With timing on, every launch of the fused RK4 stage kernel is bracketed by
+ * CUDA events on the launching stream. */
+int hrn_set_timing(hrn_ctx *ctx, int32_t enable);
+
+/* Device time of the last hrn_forward / hrn_adjoint_gradient, and (timing on)
+ * the summed duration and the number of launches of the fused stage kernel. */
+int hrn_last_timing(hrn_ctx *ctx, double *total_ms, double *stage_kernel_ms, int64_t *stage_launches);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

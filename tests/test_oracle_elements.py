@@ -1,0 +1,123 @@
+"""Structural checks of the oracle's element-level restatement (CPU)."""
+import numpy as np
+import pytest
+
+import oracle as O
+from hirensi_b200.mesh import LOCAL_IJK, box_mesh, default_pml_param
+
+G = [-1.0, 0.0, 1.0]
+
+
+def box_xt(h=(2.0, 3.0, 1.5), origin=(0.0, 0.0, -1.5), shear=0.0):
+    """Nodal coordinates XT[3][27] of a (possibly sheared) hexahedron."""
+    xt = np.zeros((3, 27))
+    for i, (a, b, c) in enumerate(LOCAL_IJK):
+        x = origin[0] + 0.5 * h[0] * a + shear * 0.5 * h[2] * c
+        y = origin[1] + 0.5 * h[1] * b
+        z = origin[2] + 0.5 * h[2] * c
+        xt[:, i] = (x, y, z)
+    return xt
+
+
+def test_gll_rule():
+    x, w = [-1.0, 0.0, 1.0], [1 / 3, 4 / 3, 1 / 3]
+    assert abs(sum(w) - 2.0) < 1e-15 and x[1] == 0.0
+
+
+@pytest.mark.parametrize("pt", [(0.1, -0.3, 0.7), (-0.9, 0.2, 0.05), (0.5, 0.5, -0.5)])
+def test_shape_partition_of_unity(pt):
+    fn, d = O.shape_3_27(*pt)
+    assert abs(fn.sum() - 1.0) < 1e-14
+    assert np.all(np.abs(d.sum(axis=0)) < 1e-14)
+    # reproduces linear and quadratic fields
+    xi = np.array([[G[a], G[b], G[c]] for a, b, c in LOCAL_IJK])
+    assert abs(fn @ xi[:, 0] - pt[0]) < 1e-14
+    assert abs(fn @ (xi[:, 1] ** 2) - pt[1] ** 2) < 1e-14
+    assert abs(d[:, 2] @ (xi[:, 2] ** 2) - 2 * pt[2]) < 1e-13
+
+
+def test_shape_kronecker_at_gll_nodes():
+    for i, (a, b, c) in enumerate(LOCAL_IJK):
+        fn, _ = O.shape_3_27(G[a], G[b], G[c])
+        e = np.zeros(27)
+        e[i] = 1.0
+        assert np.array_equal(fn, e)
+
+
+def _rigid_modes(xt):
+    modes = []
+    for d in range(3):
+        v = np.zeros((3, 27))
+        v[d] = 1.0
+        modes.append(v.reshape(-1))
+    x, y, z = xt
+    for a, b in [(0, 1), (1, 2), (0, 2)]:
+        v = np.zeros((3, 27))
+        v[a] = -xt[b]
+        v[b] = xt[a]
+        modes.append(v.reshape(-1))
+    return modes
+
+
+@pytest.mark.parametrize("shear", [0.0, 0.3])
+def test_element_k_symmetric_with_rigid_null_space(shear):
+    xt = box_xt(shear=shear)
+    lam = np.linspace(100.0, 160.0, 27)
+    mu = np.linspace(80.0, 90.0, 27)
+    ek = O.element_k(xt, lam, mu)
+    assert np.array_equal(ek, ek.T)
+    scale = np.abs(ek).max()
+    for v in _rigid_modes(xt):
+        assert np.abs(ek @ v).max() < 1e-12 * scale * np.abs(v).max()
+    # positive semi-definite with exactly 6 zero modes
+    w = np.linalg.eigvalsh(ek)
+    assert np.sum(np.abs(w) < 1e-9 * w.max()) == 6
+    assert w.min() > -1e-9 * w.max()
+
+
+def test_element_mass_is_diagonal_and_integrates_volume():
+    h = (2.0, 3.0, 1.5)
+    xt = box_xt(h=h)
+    p = default_pml_param(((-10, 10), (-10, 10), (-10, 0)), 3.0)
+    em = O.element_m(xt, 2e-3, p, 201)
+    assert np.count_nonzero(em - np.diag(np.diag(em))) == 0
+    assert abs(np.diag(em).sum() - 3 * 2e-3 * np.prod(h)) < 1e-15
+
+
+def test_pml_finder_profile_and_top_zone():
+    p = default_pml_param(((-20, 20), (-20, 20), (-20, 0)), 7.5, alpha0=5.0, beta0=400.0)
+    inner = O.pml_finder([0.0, 0.0, -5.0], p)
+    assert np.array_equal(inner[:6], [1, 1, 1, 0, 0, 0])
+    assert inner[6] == 1.0 and inner[7] == 0.0 and inner[8] == 0.0 and inner[9] == 0.0
+    x = 20.0 + 3.75   # half-way through the x+ layer
+    ab = O.pml_finder([x, 0.0, -5.0], p)
+    assert abs(ab[0] - (1 + 5.0 * 0.25)) < 1e-15 and abs(ab[3] - 400.0 * 0.25) < 1e-13
+    corner = O.pml_finder([-27.5, 27.5, -27.5], p)
+    assert np.allclose(corner[:3], 6.0) and np.allclose(corner[3:6], 400.0)
+    assert abs(corner[9] - 400.0 ** 3) < 1e-6 and np.all(corner[10:] == 0.0)
+    p_top = p.copy()
+    p_top[4, 3] = -1.0
+    with pytest.raises(ValueError):
+        O.pml_finder([0.0, 0.0, 0.0], p_top)
+
+
+def test_en_diagonal_and_ea_structural_zeros():
+    p = default_pml_param(((-2, 2), (-2, 2), (-2, 0)), 3.0)
+    xt = box_xt(h=(2.0, 2.0, 2.0), origin=(2.0, 0.0, -2.0))   # in the x+ layer
+    for f in (301, 302, 303, 304):
+        en = O.element_en(xt, p, f)
+        assert np.count_nonzero(en - np.diag(np.diag(en))) == 0
+    lam = np.full(27, 160.0)
+    mu = np.full(27, 80.0)
+    for f in range(101, 107):
+        ea = O.element_ea(xt, lam, mu, p, f)
+        assert np.all(ea[0:27, 135:162] == 0) and np.all(ea[27:54, 108:135] == 0) and np.all(ea[54:81, 81:108] == 0)
+    assert np.abs(O.element_ea(xt, lam, mu, p, 101)).max() > 0
+
+
+def test_surface_traction_integrates_face_area():
+    xt = box_xt(h=(2.0, 3.0, 1.5), origin=(0.0, 0.0, -1.5))
+    efs = O.element_fs(xt, 5)
+    assert abs(efs[54:81].sum() - 6.0) < 1e-14 and np.all(efs[:54] == 0.0)
+    with pytest.raises(ValueError):
+        O.element_fs(box_xt(origin=(0.0, 0.0, -5.0)), 5)
