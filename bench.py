@@ -1,0 +1,388 @@
+#!/usr/bin/env python
+"""Benchmark of the explicit elastic FWI gradient evaluation on B200.
+
+One step = one gradient evaluation of the plain inversion workload
+(hirensi_b200.configs.inversion_config: 16x16x8 27-node hexahedra + 3-element
+PML, 4 surface shots, 2000 RK4 steps): device assembly of C, K, G, M from the
+current model, forward RK4 of all shots with the history kept in HBM, misfit,
+adjoint RK4 with the zero-lag lambda/mu gradient fused in.  The metric is
+fwd+adj GDOF-steps/s = DOF (regular-domain displacement DOF) x (forward +
+adjoint steps) x shots / time.
+
+    python bench.py [--gpus N --steps K --warmup W] [--impl native|reference]
+
+Under torchrun each rank runs its own batch of shots (weak scaling) and the
+gradients are summed over ranks with one NCCL all-reduce per step.
+``--impl reference`` times the CPU restatement of the reference solver (the
+reference itself needs Fortran + PETSc, which this image lacks) on the host
+cores, rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "fwd+adj GDOF-steps/s and FWI time-to-misfit, plain FP64 vs batched FP32+learned"
+UNIT = "GDOF-steps/s"
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["native", "reference"], default="native")
+    ap.add_argument("--nstep", type=int, default=2000, help="time steps per shot (2000 = the configuration)")
+    ap.add_argument("--profile-case", action="store_true",
+                    help="small run for profiler captures: 40 time steps, FP64 value leg only")
+    ap.add_argument("--no-fp32", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------
+# environment helpers
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def profile_traffic(name: str):
+    """DRAM bytes per launch of a kernel from its committed ncu summary, or None."""
+    path = os.path.join(ROOT, "profiles", name)
+    try:
+        txt = open(path).read()
+    except OSError:
+        return None
+    m = re.search(r"dram_bytes_per_launch\s*=\s*([0-9.eE+]+)", txt)
+    return float(m.group(1)) if m else None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.lines = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-lms", "200", "-i", str(self.index)],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.t.join(timeout=2)
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# algorithmic bytes of one fused stage launch (per-unit figure x units)
+
+def stage_bytes(nnz_total: int, n: int, shots: int, bv: int) -> float:
+    """Average algorithmic bytes of one RK4 stage launch: every stored entry once
+    (value + 4-byte column), three row pointers, and per shot four stage vectors
+    read/written per stage plus the x1..x3 update once per step
+    (B_step / 4 of the per-step formula of the scope table)."""
+    matrix = nnz_total * (bv + 4) + 3 * 4 * (n + 1)
+    vectors = shots * (4 * n * bv + 6 * n * bv / 4.0)
+    return float(matrix + vectors)
+
+
+# ---------------------------------------------------------------------------
+# native arm
+
+def run_native(args, rank, world, local_rank):
+    import torch
+    from hirensi_b200 import build
+    from hirensi_b200.configs import RHO, inversion_config
+    from hirensi_b200.solver import Solver
+
+    build.build()
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    nstep = 40 if args.profile_case else args.nstep
+    prob = inversion_config(nstep=nstep)
+    m = prob.mesh
+    stream = torch.cuda.current_stream(dev)
+
+    def make_solver(precision):
+        s = Solver(precision, device=local_rank)
+        s.set_stream(stream.cuda_stream)
+        s.set_mesh(m, RHO)
+        s.assemble(prob.lam0, prob.mu0)
+        s.set_history(m.store_eq)
+        s.set_shots(prob.nstep, prob.dt, prob.src_eq, prob.src_b, prob.ftab)
+        s.set_receivers(prob.eqdis, prob.eqdis_map)
+        return s
+
+    # measured data: FP64 forward of the true model (set-up, untimed)
+    s64 = make_solver("fp64")
+    s64.assemble(prob.lam_true, prob.mu_true)
+    s64.forward()
+    dis = s64.traces()
+    dis_dev = torch.from_numpy(dis).to(dev)
+    lam_dev = torch.from_numpy(prob.lam0).to(dev)
+    mu_dev = torch.from_numpy(prob.mu0).to(dev)
+    g_dev = torch.zeros(2, m.nj, dtype=torch.float64, device=dev)
+    s64.set_data(device_ptr=dis_dev.data_ptr())
+    dis_pinned = torch.from_numpy(dis).pin_memory()
+    lam_h, mu_h = prob.lam0.copy(), prob.mu0.copy()
+
+    def barrier():
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+
+    def allreduce():
+        if world > 1:
+            import torch.distributed as dist
+            dist.all_reduce(g_dev)
+
+    def step_value(s):
+        s.assemble_device(lam_dev.data_ptr(), mu_dev.data_ptr())
+        s.forward()
+        s.misfit(None)
+        s.adjoint_gradient(None, to_host=False)
+        s.gradient_device(g_dev[0].data_ptr(), g_dev[1].data_ptr())
+        allreduce()
+
+    def step_e2e(s):
+        s.set_data(dis_pinned.numpy())
+        s.assemble(lam_h, mu_h)
+        s.forward()
+        s.misfit(None)
+        gl, gm = s.adjoint_gradient(None, to_host=True)
+        if world > 1:
+            g_dev[0].copy_(torch.from_numpy(gl))
+            g_dev[1].copy_(torch.from_numpy(gm))
+            allreduce()
+        return gl
+
+    def timed(fn, s, K, W, sample_clocks=False):
+        for _ in range(W):
+            fn(s)
+        torch.cuda.synchronize(dev)
+        barrier()
+        torch.cuda.synchronize(dev)
+        clk = ClockSampler(local_rank) if sample_clocks else None
+        if clk:
+            clk.start()
+        l0 = s.launch_count()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(K):
+            fn(s)
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        barrier()
+        torch.cuda.synchronize(dev)
+        ms = e0.elapsed_time(e1)
+        clocks = clk.stop() if clk else None
+        launches = s.launch_count() - l0
+        if world > 1:
+            import torch.distributed as dist
+            t = torch.tensor([ms], dtype=torch.float64, device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms, launches, clocks
+
+    K, W = args.steps, args.warmup
+    units_per_step = prob.dof * ((prob.nstep + 1) + prob.nstep) * prob.nshot * world
+
+    # value leg (inputs resident): FP64, every stage launch bracketed by events
+    def step_value_timed(s):
+        step_value(s)
+
+    for _ in range(W):
+        step_value(s64)
+    s64.set_timing(True)   # resets the per-launch accumulators: only the timed steps count
+    ms_val, launches, clocks = timed(step_value_timed, s64, K, 0, sample_clocks=True)
+    _, stage_ms, stage_n = s64.last_timing()
+    s64.set_timing(False)
+    stage_avg_ms = stage_ms / max(stage_n, 1)
+    value = units_per_step * K / (ms_val * 1e-3)
+
+    result = {"metric": METRIC, "value": value / 1e9, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
+              "ms_per_step": ms_val / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+              "dtype": "f64", "data": "synthetic (seeded layered model with a Gaussian anomaly; no dataset)"}
+    nnz = [s64.operator_csr(w)[2].size for w in range(3)]
+    result["config"] = {"workload": prob.name + f"_4shots_{prob.nstep}steps", "elements": m.nel, "nodes": m.nj,
+                        "dof": prob.dof, "equations": m.neq, "nnz_CKG": nnz, "shots_per_gpu": prob.nshot,
+                        "time_steps": prob.nstep, "dt": prob.dt,
+                        "step": "assemble + forward (history in HBM) + misfit + adjoint with fused gradient",
+                        "l2": "inputs larger than L2: FP64 operator 168 MB and 3.6 GB of histories per step"}
+    result["gpu_launches"] = int(launches)
+
+    # roofline of the dominant kernel (fused RK4 stage)
+    peak, peak_kind = measured_peaks()
+    bytes_launch = stage_bytes(sum(nnz), m.neq, prob.nshot, 8)
+    achieved = bytes_launch / (stage_avg_ms * 1e-3) / 1e9
+    traffic = profile_traffic("rk4_stage_fp64_inversion.md")
+    result["roofline"] = {"bound": "hbm", "kernel": "rk4_stage<double,4>", "achieved": achieved, "peak": peak,
+                          "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
+                          "bytes_per_launch": bytes_launch, "avg_launch_us": stage_avg_ms * 1e3,
+                          "traffic": traffic}
+    result["clocks"] = clocks
+
+    if not args.profile_case:
+        # e2e leg: host buffers through the C ABI, copies inside the timed region
+        ms_e2e, _, _ = timed(step_e2e, s64, K, min(W, 1))
+        h2d = dis.nbytes + lam_h.nbytes + mu_h.nbytes
+        d2h = 2 * m.nj * 8 + 8
+        result["e2e"] = {"value": units_per_step * K / (ms_e2e * 1e-3) / 1e9, "unit": UNIT,
+                         "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h), "ms_per_step": ms_e2e / K}
+        # FP32 stepping with FP64 reductions, same workload
+        if not args.no_fp32:
+            g64 = g_dev.clone()
+            tr64 = s64.traces()
+            s32 = make_solver("fp32")
+            s32.set_data(device_ptr=dis_dev.data_ptr())
+            ms32, _, _ = timed(step_value, s32, K, W)
+            tr32 = s32.traces()
+            g32 = g_dev.clone()
+            ms32e, _, _ = timed(step_e2e, s32, K, min(W, 1))
+
+            def rel(a, b):
+                return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+            result["fp32"] = {"value": units_per_step * K / (ms32 * 1e-3) / 1e9, "ms_per_step": ms32 / K,
+                              "e2e": {"value": units_per_step * K / (ms32e * 1e-3) / 1e9, "unit": UNIT},
+                              "seismogram_rel_l2_vs_fp64": rel(tr32, tr64),
+                              "gradient_rel_l2_vs_fp64": rel(g32.cpu().numpy(), g64.cpu().numpy())}
+            s32.close()
+        if rank == 0 and not args.no_cpu_baseline:
+            result["cpu_baseline"] = cpu_sample(prob)
+    s64.close()
+    return result
+
+
+# ---------------------------------------------------------------------------
+# CPU restatement of the reference (baseline leg and --impl reference)
+
+_CPU_SYS = {}
+
+
+def cpu_sample(prob, nsteps=100):
+    """Time the FP64 CPU restatement (OpenMP over all host cores) on a bounded
+    sample: one shot, `nsteps` forward + adjoint steps with the gradient."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    from hirensi_b200.configs import RHO
+    m = prob.mesh
+    cores = os.cpu_count() or 1
+    if "sys" not in _CPU_SYS:
+        om = O.OracleMesh(m, RHO)
+        _CPU_SYS["sys"] = (om, O.OracleSystem.assemble(om, prob.lam0, prob.mu0))
+    om, S = _CPU_SYS["sys"]
+    b = np.zeros(m.neq)
+    b[prob.src_eq[0]] = 1.0
+    ftab = prob.ftab[0][: nsteps + 1]
+    dis = np.zeros((prob.eqdis.size, nsteps + 1))
+    t0 = time.perf_counter()
+    u = S.forward(b, ftab, nsteps, prob.dt, m.store_eq, nthreads=cores)
+    p = S.adjoint(nsteps, prob.dt, m.store_eq, u, prob.eqdis, prob.eqdis_map, dis + 1e-12, nthreads=cores)
+    O.control(om, nsteps, prob.dt, m.store_eq, u, p)
+    dt = time.perf_counter() - t0
+    units = prob.dof * ((nsteps + 1) + nsteps)
+    return {"value": units / dt / 1e9, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"1 shot, {nsteps + 1} forward + {nsteps} adjoint RK4 steps with the gradient, "
+                      f"same mesh and model, {dt:.2f} s"}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return None
+    from hirensi_b200.configs import inversion_config
+    prob = inversion_config(nstep=args.nstep)
+    for _ in range(args.warmup):
+        cpu_sample(prob, nsteps=50)
+    vals = [cpu_sample(prob, nsteps=50) for _ in range(args.steps)]
+    v = float(np.median([x["value"] for x in vals]))
+    cb = dict(vals[-1])
+    cb["value"] = v
+    return {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "impl": "reference",
+            "config": {"workload": prob.name + f"_4shots_{prob.nstep}steps", "dof": prob.dof,
+                       "note": "CPU restatement of the reference solver (Fortran + PETSc not in the image); "
+                               "each step is a bounded sample: 1 shot, 51 forward + 50 adjoint steps"},
+            "cpu_baseline": cb, "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def main():
+    args = parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1 and args.impl == "native":
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    if args.impl == "reference":
+        res = run_reference(args, rank, world)
+    else:
+        res = run_native(args, rank, world, local_rank)
+    if rank == 0 and res is not None:
+        print(json.dumps(res), flush=True)
+    if world > 1 and args.impl == "native":
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -44,6 +44,10 @@ SIGNATURES = {
     "hrn_set_stream": (C.c_int, [VP, VP]),
     "hrn_set_timing": (C.c_int, [VP, C.c_int32]),
     "hrn_last_timing": (C.c_int, [VP, PD, PD, PI64]),
+    "hrn_assemble_device": (C.c_int, [VP, VP, VP]),
+    "hrn_set_data": (C.c_int, [VP, VP, C.c_int32]),
+    "hrn_get_gradient_device": (C.c_int, [VP, VP, VP]),
+    "hrn_launch_count": (C.c_int, [VP, PI64]),
 }
 
 _lib = None

@@ -385,13 +385,13 @@ static int run_kernels(hrn_ctx *c, AsmArgs A)
         A.elems = c->d_el_color_list.as<int32_t>() + c->color_off[g];
         A.nel = n;
         const bool pml = (g % 2) == 1;
-        k_asm_diag<<<(n * 27 + th - 1) / th, th, 0, c->stream>>>(A, pml ? 1 : 0);
+        k_asm_diag<<<(n * 27 + th - 1) / th, th, 0, c->stream>>>(A, pml ? 1 : 0); ++c->launches;
         if (!pml) {
             const int64_t tot = int64_t(n) * 513 * 9;
-            k_asm_rd_k<<<unsigned((tot + th - 1) / th), th, 0, c->stream>>>(A);
+            k_asm_rd_k<<<unsigned((tot + th - 1) / th), th, 0, c->stream>>>(A); ++c->launches;
         } else {
             const int64_t tot = int64_t(n) * 189 * 54;
-            k_asm_ea<<<unsigned((tot + th - 1) / th), th, 0, c->stream>>>(A);
+            k_asm_ea<<<unsigned((tot + th - 1) / th), th, 0, c->stream>>>(A); ++c->launches;
         }
         HRN_CUDA(c, cudaGetLastError());
     }
@@ -455,7 +455,7 @@ int assemble_device(hrn_ctx *c, bool discover_pattern)
     A.raw = c->d_raw.as<double>();
     A.diag_m = c->d_diag_m.as<double>();
     if (int rc = run_kernels(c, A)) return rc;
-    k_inv_mass<<<(c->neq + 255) / 256, 256, 0, c->stream>>>(c->neq, c->d_diag_m.as<double>(), c->d_im.as<double>());
+    k_inv_mass<<<(c->neq + 255) / 256, 256, 0, c->stream>>>(c->neq, c->d_diag_m.as<double>(), c->d_im.as<double>()); ++c->launches;
     HRN_CUDA(c, cudaGetLastError());
     int err = 0;
     HRN_CUDA(c, cudaMemcpyAsync(&err, c->d_asm_err.p, 4, cudaMemcpyDeviceToHost, c->stream));

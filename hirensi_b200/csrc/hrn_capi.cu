@@ -314,6 +314,10 @@ int hrn_set_timing(hrn_ctx *c, int32_t enable)
 {
     if (!c) return HRN_EARG;
     c->timing = enable != 0;
+    if (c->timing) {
+        c->acc_stage_ms = 0.0;
+        c->acc_stage_launches = 0;
+    }
     return HRN_OK;
 }
 
@@ -321,8 +325,8 @@ int hrn_last_timing(hrn_ctx *c, double *total_ms, double *stage_kernel_ms, int64
 {
     if (!c) return HRN_EARG;
     if (total_ms) *total_ms = c->last_total_ms;
-    if (stage_kernel_ms) *stage_kernel_ms = c->last_stage_ms;
-    if (stage_launches) *stage_launches = c->last_stage_launches;
+    if (stage_kernel_ms) *stage_kernel_ms = c->acc_stage_ms;
+    if (stage_launches) *stage_launches = c->acc_stage_launches;
     return HRN_OK;
 }
 
@@ -393,24 +397,36 @@ int hrn_set_mesh(hrn_ctx *c, int32_t nj, int32_t nel, int32_t neq, const double 
     return HRN_OK;
 }
 
-int hrn_assemble(hrn_ctx *c, const double *lambda, const double *mu)
+static int assemble_common(hrn_ctx *c, const double *lambda, const double *mu, bool device_src)
 {
     if (!c) return HRN_EARG;
     if (!c->have_mesh) return set_error(c, HRN_ESTATE, "no mesh: call hrn_set_mesh first");
     if (!lambda || !mu) return set_error(c, HRN_EARG, "null material");
     cudaSetDevice(c->device);
-    for (int i = 0; i < c->nj; ++i)
-        if (!std::isfinite(lambda[i]) || !std::isfinite(mu[i])) return set_error(c, HRN_ENAN, "non-finite material");
     HRN_CUDA(c, c->d_lam.alloc(size_t(c->nj) * 8));
     HRN_CUDA(c, c->d_mu.alloc(size_t(c->nj) * 8));
-    HRN_CUDA(c, cudaMemcpy(c->d_lam.p, lambda, size_t(c->nj) * 8, cudaMemcpyHostToDevice));
-    HRN_CUDA(c, cudaMemcpy(c->d_mu.p, mu, size_t(c->nj) * 8, cudaMemcpyHostToDevice));
+    if (device_src) {
+        HRN_CUDA(c, cudaMemcpyAsync(c->d_lam.p, lambda, size_t(c->nj) * 8, cudaMemcpyDeviceToDevice, c->stream));
+        HRN_CUDA(c, cudaMemcpyAsync(c->d_mu.p, mu, size_t(c->nj) * 8, cudaMemcpyDeviceToDevice, c->stream));
+    } else {
+        for (int i = 0; i < c->nj; ++i)
+            if (!std::isfinite(lambda[i]) || !std::isfinite(mu[i])) return set_error(c, HRN_ENAN, "non-finite material");
+        HRN_CUDA(c, cudaMemcpyAsync(c->d_lam.p, lambda, size_t(c->nj) * 8, cudaMemcpyHostToDevice, c->stream));
+        HRN_CUDA(c, cudaMemcpyAsync(c->d_mu.p, mu, size_t(c->nj) * 8, cudaMemcpyHostToDevice, c->stream));
+    }
     const bool first = !c->have_pattern;
     if (int rc = assemble_device(c, first)) return rc;
     c->have_operator = true;
     c->have_forward = false;
     if (first) return rebind(c);
     return HRN_OK;
+}
+
+int hrn_assemble(hrn_ctx *c, const double *lambda, const double *mu) { return assemble_common(c, lambda, mu, false); }
+
+int hrn_assemble_device(hrn_ctx *c, const double *d_lambda, const double *d_mu)
+{
+    return assemble_common(c, d_lambda, d_mu, true);
 }
 
 int hrn_get_operator_csr(hrn_ctx *c, int32_t which, int32_t *ia, int32_t *ja, double *a, int64_t *nnz)
@@ -472,6 +488,7 @@ int hrn_set_shots(hrn_ctx *c, int32_t nshot, int32_t nstep, double dt, int32_t n
     c->h_src_eq.assign(src_eq, src_eq + nsrc);
     c->h_src_b.assign(src_b, src_b + size_t(nsrc) * nshot);
     c->h_ftab.assign(ftab, ftab + size_t(nshot) * (nstep + 1) * 3);
+    c->have_data = false;
     for (double v : c->h_ftab)
         if (!std::isfinite(v)) return set_error(c, HRN_ENAN, "non-finite time function sample");
     c->have_forward = false;
@@ -561,12 +578,43 @@ int hrn_get_traces(hrn_ctx *c, double *traces)
     return HRN_OK;
 }
 
-static int upload_dis(hrn_ctx *c, const double *dis_meas)
+static int upload_dis(hrn_ctx *c, const double *dis_meas, bool device_src = false)
 {
     const size_t n = size_t(c->nshot) * c->nrec3 * (c->nstep + 1);
+    if (!dis_meas) {
+        if (n && !c->have_data) return set_error(c, HRN_ESTATE, "no measured data: pass dis_meas or call hrn_set_data");
+        return HRN_OK;
+    }
     if (n == 0) return HRN_OK;
     HRN_CUDA(c, c->d_dis.alloc(n * 8));
-    HRN_CUDA(c, cudaMemcpyAsync(c->d_dis.p, dis_meas, n * 8, cudaMemcpyHostToDevice, c->stream));
+    HRN_CUDA(c, cudaMemcpyAsync(c->d_dis.p, dis_meas, n * 8, device_src ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                                c->stream));
+    c->have_data = true;
+    return HRN_OK;
+}
+
+int hrn_set_data(hrn_ctx *c, const double *dis_meas, int32_t on_device)
+{
+    if (!c || !dis_meas) return HRN_EARG;
+    if (c->nshot == 0) return set_error(c, HRN_ESTATE, "no shots: call hrn_set_shots first");
+    cudaSetDevice(c->device);
+    return upload_dis(c, dis_meas, on_device != 0);
+}
+
+int hrn_get_gradient_device(hrn_ctx *c, double *d_g_lambda, double *d_g_mu)
+{
+    if (!c) return HRN_EARG;
+    if (!c->have_mesh || !c->d_g.p) return set_error(c, HRN_ESTATE, "no gradient");
+    if (d_g_lambda) HRN_CUDA(c, cudaMemcpyAsync(d_g_lambda, c->d_g.p, size_t(c->nj) * 8, cudaMemcpyDeviceToDevice, c->stream));
+    if (d_g_mu)
+        HRN_CUDA(c, cudaMemcpyAsync(d_g_mu, c->d_g.as<double>() + c->nj, size_t(c->nj) * 8, cudaMemcpyDeviceToDevice, c->stream));
+    return HRN_OK;
+}
+
+int hrn_launch_count(hrn_ctx *c, int64_t *n)
+{
+    if (!c || !n) return HRN_EARG;
+    *n = c->launches;
     return HRN_OK;
 }
 
@@ -574,7 +622,6 @@ int hrn_misfit(hrn_ctx *c, const double *dis_meas, double *cost)
 {
     if (!c || !cost) return HRN_EARG;
     if (!c->have_forward) return set_error(c, HRN_ESTATE, "no forward history");
-    if (c->nrec3 > 0 && !dis_meas) return set_error(c, HRN_EARG, "null measured data");
     cudaSetDevice(c->device);
     if (int rc = upload_dis(c, dis_meas)) return rc;
     std::vector<double> out(size_t(1 + c->nshot));
@@ -590,12 +637,12 @@ int hrn_adjoint_gradient(hrn_ctx *c, const double *dis_meas, int32_t lambda_2mu,
     if (!c) return HRN_EARG;
     if (int rc = check_ready(c, true)) return rc;
     if (!c->have_forward) return set_error(c, HRN_ESTATE, "no forward history: call hrn_forward first");
-    if (c->nrec3 > 0 && !dis_meas) return set_error(c, HRN_EARG, "null measured data");
     cudaSetDevice(c->device);
     if (int rc = upload_dis(c, dis_meas)) return rc;
     if (int rc = run_adjoint_gradient(c, lambda_2mu, keep_p)) return rc;
-    if (g_lambda) HRN_CUDA(c, cudaMemcpy(g_lambda, c->d_g.p, size_t(c->nj) * 8, cudaMemcpyDeviceToHost));
-    if (g_mu) HRN_CUDA(c, cudaMemcpy(g_mu, c->d_g.as<double>() + c->nj, size_t(c->nj) * 8, cudaMemcpyDeviceToHost));
+    if (g_lambda) HRN_CUDA(c, cudaMemcpyAsync(g_lambda, c->d_g.p, size_t(c->nj) * 8, cudaMemcpyDeviceToHost, c->stream));
+    if (g_mu) HRN_CUDA(c, cudaMemcpyAsync(g_mu, c->d_g.as<double>() + c->nj, size_t(c->nj) * 8, cudaMemcpyDeviceToHost, c->stream));
+    if (g_lambda || g_mu) HRN_CUDA(c, cudaStreamSynchronize(c->stream));
     return HRN_OK;
 }
 

@@ -118,11 +118,15 @@ struct hrn_ctx {
     bool have_forward = false;
     bool have_phist = false;
     hrn::DevBuf d_g;              // [2][nj] FP64 gradient accumulators (lambda, mu)
+    bool have_data = false;       // measured data resident on the device
 
     // ---- timing
+    int64_t launches = 0;          // kernels launched by this context (cumulative)
     bool timing = false;
     double last_total_ms = 0.0, last_stage_ms = 0.0;
     int64_t last_stage_launches = 0;
+    double acc_stage_ms = 0.0;      // summed since timing was last enabled
+    int64_t acc_stage_launches = 0;
     std::vector<cudaEvent_t> ev_pool;
 
     size_t elem_bytes() const { return precision == HRN_FP64 ? 8 : 4; }

@@ -457,11 +457,11 @@ static int scale_operator_t(hrn_ctx *c)
     if (c->d_adj.bytes != size_t(c->nnz) * sizeof(T)) HRN_CUDA(c, c->d_adj.alloc(size_t(c->nnz) * sizeof(T)));
     if (c->nnz == 0) return 0;
     k_scale_fwd<T><<<blocks_for(c->nnz, th), th, 0, c->stream>>>(c->nnz, c->d_rowidx.as<int32_t>(), c->d_raw.as<double>(),
-                                                                  c->d_im.as<double>(), c->d_fwd.as<T>());
+                                                                  c->d_im.as<double>(), c->d_fwd.as<T>()); ++c->launches;
     HRN_CUDA(c, cudaGetLastError());
     k_scale_adj<T><<<blocks_for(c->nnz, th), th, 0, c->stream>>>(c->nnz, c->d_permT.as<int64_t>(), c->d_rowidx.as<int32_t>(),
                                                                   c->d_colx.as<uint32_t>(), c->d_raw.as<double>(),
-                                                                  c->d_diag_m.as<double>(), c->d_im.as<double>(), c->d_adj.as<T>());
+                                                                  c->d_diag_m.as<double>(), c->d_im.as<double>(), c->d_adj.as<T>()); ++c->launches;
     HRN_CUDA(c, cudaGetLastError());
     return 0;
 }
@@ -614,9 +614,9 @@ int build_rd_geometry(hrn_ctx *c)
     const int th = 256;
     if (c->nel_rd > 0)
         k_geometry<<<(c->nel_rd * 27 + th - 1) / th, th, 0, c->stream>>>(c->nel_rd, c->d_rd_elems.as<int32_t>(), c->d_inod.as<int32_t>(),
-                                                                           c->d_xyz.as<double>(), c->d_rd_geom.as<double>(), c->d_asm_err.as<int>());
+                                                                           c->d_xyz.as<double>(), c->d_rd_geom.as<double>(), c->d_asm_err.as<int>()); ++c->launches;
     k_geometry<<<(c->nel * 27 + th - 1) / th, th, 0, c->stream>>>(c->nel, nullptr, c->d_inod.as<int32_t>(), c->d_xyz.as<double>(),
-                                                                   c->d_asm_geom.as<double>(), c->d_asm_err.as<int>());
+                                                                   c->d_asm_geom.as<double>(), c->d_asm_err.as<int>()); ++c->launches;
     HRN_CUDA(c, cudaGetLastError());
     int bad = 0;
     HRN_CUDA(c, cudaMemcpyAsync(&bad, c->d_asm_err.p, 4, cudaMemcpyDeviceToHost, c->stream));
@@ -675,6 +675,7 @@ static void launch_step(hrn_ctx *c, StageArgs<T> a, T *X, T *Y, StageTimer *tm)
         case 3: launch_stage<T, S, 3>(a, c->stream); break;
         default: launch_stage<T, S, 4>(a, c->stream); break;
         }
+        ++c->launches;
         if (tm) cudaEventRecord(tm->get(), c->stream);
         a.hist = nullptr;   // history only in stage 1
     }
@@ -705,7 +706,7 @@ static int forward_t(hrn_ctx *c)
         const int64_t tot = int64_t(c->nstep + 1) * c->nslot_f * S;
         k_src_fwd<T, S><<<blocks_for(tot, 256), 256, 0, c->stream>>>(c->nstep, c->nslot_f, c->d_fslot_eq.as<int32_t>(),
                                                                      c->d_fsrc_b.as<double>(), c->d_ftab.as<double>(),
-                                                                     c->d_im.as<double>(), c->d_srcv_f.as<T>());
+                                                                     c->d_im.as<double>(), c->d_srcv_f.as<T>()); ++c->launches;
         HRN_CUDA(c, cudaGetLastError());
     }
     StageArgs<T> a{};
@@ -736,6 +737,8 @@ static int forward_t(hrn_ctx *c)
     c->last_total_ms = ms;
     c->last_stage_ms = c->timing ? sum_timer(c, tm) : 0.0;
     c->last_stage_launches = c->timing ? int64_t(tm.used / 2) : 0;
+    c->acc_stage_ms += c->last_stage_ms;
+    c->acc_stage_launches += c->last_stage_launches;
     c->have_forward = true;
     c->have_phist = false;
     return 0;
@@ -779,7 +782,7 @@ static int adjoint_t(hrn_ctx *c, int lambda_2mu, int keep_p)
             k_src_adj<T, S><<<(c->nslot_a * S + 127) / 128, 128, 0, c->stream>>>(
                 n, c->nstep, c->nstore, c->nrec3, c->nslot_a, c->d_aslot_ptr.as<int32_t>(), c->d_aslot_q.as<int32_t>(),
                 c->d_aslot_eq.as<int32_t>(), c->d_eqdis_map.as<int32_t>(), c->d_hist.as<T>(), c->d_dis.as<double>(),
-                c->d_im.as<double>(), c->d_srcv_a.as<T>());
+                c->d_im.as<double>(), c->d_srcv_a.as<T>()); ++c->launches;
         a.hist = keep_p ? c->d_phist.as<T>() + size_t(n) * c->nstore * S : nullptr;
         T *X = (it & 1) ? X1 : X0, *Y = (it & 1) ? X0 : X1;
         launch_step<T, S>(c, a, X, Y, c->timing ? &tm : nullptr);
@@ -787,7 +790,7 @@ static int adjoint_t(hrn_ctx *c, int lambda_2mu, int keep_p)
             k_gradient<T, S><<<gblocks, 128, 0, c->stream>>>(c->nel_rd, c->d_rd_store.as<int32_t>(), c->d_rd_elems.as<int32_t>(),
                                                              c->d_inod.as<int32_t>(), c->d_rd_geom.as<double>(),
                                                              c->d_hist.as<T>() + size_t(n) * c->nstore * S, X + vn,
-                                                             c->d_store_eq.as<int32_t>(), gl, gmu, c->dt, lambda_2mu);
+                                                             c->d_store_eq.as<int32_t>(), gl, gmu, c->dt, lambda_2mu); ++c->launches;
     }
     HRN_CUDA(c, cudaGetLastError());
     cudaEventRecord(t1, c->stream);
@@ -799,6 +802,8 @@ static int adjoint_t(hrn_ctx *c, int lambda_2mu, int keep_p)
     c->last_total_ms = ms;
     c->last_stage_ms = c->timing ? sum_timer(c, tm) : 0.0;
     c->last_stage_launches = c->timing ? int64_t(tm.used / 2) : 0;
+    c->acc_stage_ms += c->last_stage_ms;
+    c->acc_stage_launches += c->last_stage_launches;
     c->have_phist = keep_p != 0;
     return 0;
 }
@@ -810,8 +815,8 @@ static int misfit_t(hrn_ctx *c, double *cost)
     k_misfit_terms<T, S><<<(tot + 127) / 128, 128, 0, c->stream>>>(c->nstep, c->nstore, c->nrec3, c->nslot_a,
                                                                    c->d_aslot_ptr.as<int32_t>(), c->d_aslot_q.as<int32_t>(),
                                                                    c->d_eqdis_map.as<int32_t>(), c->d_hist.as<T>(),
-                                                                   c->d_dis.as<double>(), c->d_mis_terms.as<double>());
-    k_misfit_sum<<<1, 1, 0, c->stream>>>(S, c->nstep, c->dt, c->d_mis_terms.as<double>(), c->d_cost.as<double>());
+                                                                   c->d_dis.as<double>(), c->d_mis_terms.as<double>()); ++c->launches;
+    k_misfit_sum<<<1, 1, 0, c->stream>>>(S, c->nstep, c->dt, c->d_mis_terms.as<double>(), c->d_cost.as<double>()); ++c->launches;
     HRN_CUDA(c, cudaGetLastError());
     std::vector<double> h(size_t(1 + S));
     HRN_CUDA(c, cudaMemcpyAsync(h.data(), c->d_cost.p, h.size() * 8, cudaMemcpyDeviceToHost, c->stream));

@@ -104,6 +104,10 @@ class Solver:
     def assemble(self, lam, mu):
         self._check(self._L.hrn_assemble(self.h, dptr(f64(lam)), dptr(f64(mu))))
 
+    def assemble_device(self, lam_ptr: int, mu_ptr: int):
+        """Assemble from device-resident nodal lambda, mu (raw device pointers, FP64 [nj])."""
+        self._check(self._L.hrn_assemble_device(self.h, C.c_void_p(lam_ptr), C.c_void_p(mu_ptr)))
+
     def operator_csr(self, which: int):
         nnz = C.c_int64()
         self._check(self._L.hrn_get_operator_csr(self.h, which, None, None, None, C.byref(nnz)))
@@ -145,6 +149,19 @@ class Solver:
         self._check(self._L.hrn_set_receivers(self.h, e.size, iptr(e), iptr(m)))
         self.nrec3 = e.size
 
+    def set_data(self, dis_meas=None, device_ptr: int | None = None):
+        """Keep the measured data [nshot, nrec3, nstep+1] on the device (host array or device pointer)."""
+        if device_ptr is not None:
+            self._check(self._L.hrn_set_data(self.h, C.c_void_p(device_ptr), 1))
+        else:
+            d = self._dis(dis_meas)
+            self._check(self._L.hrn_set_data(self.h, d.ctypes.data_as(C.c_void_p), 0))
+
+    def launch_count(self) -> int:
+        n = C.c_int64()
+        self._check(self._L.hrn_launch_count(self.h, C.byref(n)))
+        return n.value
+
     # -- time loops ---------------------------------------------------------------
     def forward(self):
         self._check(self._L.hrn_forward(self.h))
@@ -167,18 +184,29 @@ class Solver:
             raise ValueError("dis_meas must be [nshot, nrec3, nstep+1]")
         return d
 
-    def misfit(self, dis_meas) -> float:
-        d = self._dis(dis_meas)
+    def misfit(self, dis_meas=None) -> float:
+        """Misfit against dis_meas, or against the resident data when dis_meas is None."""
         out = C.c_double()
-        self._check(self._L.hrn_misfit(self.h, dptr(d), C.byref(out)))
+        if dis_meas is None:
+            self._check(self._L.hrn_misfit(self.h, None, C.byref(out)))
+        else:
+            d = self._dis(dis_meas)
+            self._check(self._L.hrn_misfit(self.h, dptr(d), C.byref(out)))
         return out.value
 
-    def adjoint_gradient(self, dis_meas, lambda_2mu: bool = False, keep_p: bool = False):
-        d = self._dis(dis_meas)
-        gl = np.zeros(self.nj)
-        gm = np.zeros(self.nj)
-        self._check(self._L.hrn_adjoint_gradient(self.h, dptr(d), int(lambda_2mu), int(keep_p), dptr(gl), dptr(gm)))
-        return gl, gm
+    def adjoint_gradient(self, dis_meas=None, lambda_2mu: bool = False, keep_p: bool = False, to_host: bool = True):
+        """Raw gradient (g_lambda, g_mu) on the host, or None when to_host is False
+        (then fetch it with gradient_device)."""
+        d = None if dis_meas is None else self._dis(dis_meas)
+        gl = np.zeros(self.nj) if to_host else None
+        gm = np.zeros(self.nj) if to_host else None
+        self._check(self._L.hrn_adjoint_gradient(self.h, dptr(d) if d is not None else None, int(lambda_2mu), int(keep_p),
+                                                 dptr(gl) if to_host else None, dptr(gm) if to_host else None))
+        return (gl, gm) if to_host else None
+
+    def gradient_device(self, lam_ptr: int, mu_ptr: int):
+        """Copy the accumulated gradient into device buffers (raw pointers, FP64 [nj])."""
+        self._check(self._L.hrn_get_gradient_device(self.h, C.c_void_p(lam_ptr), C.c_void_p(mu_ptr)))
 
     def adjoint_history(self, shot: int = 0) -> np.ndarray:
         p = np.zeros((self.nstep + 1, self.nstore))

@@ -74,6 +74,9 @@ int hrn_set_mesh(hrn_ctx *ctx, int32_t nj, int32_t nel, int32_t neq,
  * (entries with a nonzero element contribution, as MAT_IGNORE_ZERO_ENTRIES). */
 int hrn_assemble(hrn_ctx *ctx, const double *lambda, const double *mu);
 
+/* hrn_assemble with lambda, mu already on the device (device pointers [nj]). */
+int hrn_assemble_device(hrn_ctx *ctx, const double *d_lambda, const double *d_mu);
+
 /* Download the current operator (unscaled).  With ia/ja/a NULL only *nnz is set. */
 int hrn_get_operator_csr(hrn_ctx *ctx, int32_t which, int32_t *ia, int32_t *ja, double *a, int64_t *nnz);
 int hrn_get_diag_m(hrn_ctx *ctx, double *diag_m);
@@ -94,6 +97,12 @@ int hrn_set_shots(hrn_ctx *ctx, int32_t nshot, int32_t nstep, double dt,
  * positions in the history), S4/IO_Parallel_Inversion.F90:116-133. */
 int hrn_set_receivers(hrn_ctx *ctx, int32_t nrec3, const int32_t *eqdis, const int32_t *eqdis_map);
 
+/* Measured data Dis_meas of every shot, kept on the device for hrn_misfit and
+ * hrn_adjoint_gradient called with dis_meas = NULL (on_device: dis_meas is a
+ * device pointer).  Replaces the measured-data read of
+ * Input_Inv_Measured_Data (S4/PTC_Input.F90:961-1046). */
+int hrn_set_data(hrn_ctx *ctx, const double *dis_meas, int32_t on_device);
+
 /* ---- time loops ------------------------------------------------------------ */
 
 /* Forward RK4 for all shots, EXPLICIT_RK4_PETSC_PML_3D (S4/Solver_PETSc_Explicit.F90:660-1117).
@@ -103,7 +112,8 @@ int hrn_get_history(hrn_ctx *ctx, int32_t shot, double *u_store);
 /* Receiver traces U_Store(EqDis_MAP, 0:NStep) of every shot: traces[nshot][nrec3][nstep+1]. */
 int hrn_get_traces(hrn_ctx *ctx, double *traces);
 
-/* Compute_Misfit (S4/Solver_PETSc_Inverse.F90:591-657) summed over shots. */
+/* Compute_Misfit (S4/Solver_PETSc_Inverse.F90:591-657) summed over shots;
+ * dis_meas NULL uses the data of hrn_set_data. */
 int hrn_misfit(hrn_ctx *ctx, const double *dis_meas, double *cost);
 
 /* Adjoint RK4 (OtD) with the zero-lag gradient fused into each step:
@@ -111,10 +121,14 @@ int hrn_misfit(hrn_ctx *ctx, const double *dis_meas, double *cost);
  * EXPLICIT_RK4_PETSC_PML_3D_Control_OtD (:1413-1522), summed over shots.
  * g_lambda, g_mu [nj] receive the raw accumulated gradient (before the sign
  * flip and mass scaling of S4/Program_Main.F90:412-455).  lambda_2mu selects
- * ELEMENT_g_3D_v2.  keep_p stores the adjoint history for hrn_get_adjoint_history. */
+ * ELEMENT_g_3D_v2.  keep_p stores the adjoint history for hrn_get_adjoint_history.
+ * dis_meas NULL uses the data of hrn_set_data; g_lambda / g_mu NULL leave the
+ * gradient on the device (hrn_get_gradient_device). */
 int hrn_adjoint_gradient(hrn_ctx *ctx, const double *dis_meas, int32_t lambda_2mu, int32_t keep_p,
                          double *g_lambda, double *g_mu);
 int hrn_get_adjoint_history(hrn_ctx *ctx, int32_t shot, double *p_store);
+/* Copy the accumulated gradient to device buffers [nj] (either may be NULL). */
+int hrn_get_gradient_device(hrn_ctx *ctx, double *d_g_lambda, double *d_g_mu);
 
 /* ---- streams and timing -------------------------------------------------------- */
 
@@ -126,9 +140,13 @@ int hrn_set_stream(hrn_ctx *ctx, void *stream);
  * CUDA events on the launching stream. */
 int hrn_set_timing(hrn_ctx *ctx, int32_t enable);
 
-/* Device time of the last hrn_forward / hrn_adjoint_gradient, and (timing on)
- * the summed duration and the number of launches of the fused stage kernel. */
+/* Device time of the last hrn_forward / hrn_adjoint_gradient, and the summed
+ * duration and number of launches of the fused stage kernel since timing was
+ * last enabled. */
 int hrn_last_timing(hrn_ctx *ctx, double *total_ms, double *stage_kernel_ms, int64_t *stage_launches);
+
+/* Number of kernels this context has launched since it was created. */
+int hrn_launch_count(hrn_ctx *ctx, int64_t *n);
 
 #ifdef __cplusplus
 }

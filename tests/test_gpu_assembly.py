@@ -29,8 +29,11 @@ def test_pattern_and_values_match_oracle(gpu_lib, npml):
             # same stored entries as PETSc with MAT_IGNORE_ZERO_ENTRIES
             assert np.array_equal(ia, ia_r), w
             assert np.array_equal(ja, ja_r), w
-            # element arithmetic is identical; only the order of the cross-element sum differs
-            assert np.max(np.abs(a - a_r) / np.maximum(np.abs(a_r), 1e-300)) < 1e-13, w
+            # element arithmetic is identical; only the order of the cross-element sum
+            # differs, so entries that cancel to round-off may differ in their residue
+            assert np.max(np.abs(a - a_r)) <= 1e-14 * np.abs(a_r).max(), w
+            big = np.abs(a_r) > 1e-8 * np.abs(a_r).max()
+            assert np.max(np.abs(a - a_r)[big] / np.abs(a_r)[big]) < 1e-13, w
         dm_r, _ = S.vectors()
         assert np.max(np.abs(s.diag_m() - dm_r) / dm_r) < 1e-14
 
