@@ -48,6 +48,18 @@ SIGNATURES = {
     "hrn_set_data": (C.c_int, [VP, VP, C.c_int32]),
     "hrn_get_gradient_device": (C.c_int, [VP, VP, VP]),
     "hrn_launch_count": (C.c_int, [VP, PI64]),
+    "hrn_set_variant": (C.c_int, [VP, C.c_int32, C.c_int32]),
+    "hrn_get_variant": (C.c_int, [VP, PI, PI]),
+    "hrn_vec_dot": (C.c_int, [VP, C.c_int32, VP, VP, PD]),
+    "hrn_vec_norm": (C.c_int, [VP, C.c_int32, VP, C.c_int32, PD]),
+    "hrn_vec_axpby": (C.c_int, [VP, C.c_int32, C.c_double, VP, C.c_double, VP, VP]),
+    "hrn_vec_mul": (C.c_int, [VP, C.c_int32, VP, VP, VP]),
+    "hrn_vec_clip": (C.c_int, [VP, C.c_int32, C.c_double, C.c_double, VP]),
+    "hrn_vec_gather": (C.c_int, [VP, C.c_int32, VP, VP, VP]),
+    "hrn_regularization_tv": (C.c_int, [VP, VP, VP, VP, VP, PD, PD]),
+    "hrn_gradient_mass": (C.c_int, [VP, VP]),
+    "hrn_lbfgs_setup": (C.c_int, [VP, C.c_int32, VP]),
+    "hrn_lbfgs_direction": (C.c_int, [VP, C.c_int32, C.c_int32] + [VP] * 10 + [PD]),
 }
 
 _lib = None

@@ -57,8 +57,27 @@ static int install_pattern(hrn_ctx *c, int32_t neq, std::vector<int32_t> &rowptr
                 colxT[t] = uint32_t(i) | (w << kTagBits);
                 permT[t] = p;
             }
+    // segment starts (first K entry, first G entry) of every forward and transposed row
+    std::vector<int32_t> seg(2 * static_cast<size_t>(neq)), segT(2 * static_cast<size_t>(neq));
+    for (int32_t i = 0; i < neq; ++i) {
+        int32_t p = rowptr[i];
+        while (p < rowptr[i + 1] && (colx[p] >> kTagBits) < 1u) ++p;
+        seg[2 * i] = p;
+        while (p < rowptr[i + 1] && (colx[p] >> kTagBits) < 2u) ++p;
+        seg[2 * i + 1] = p;
+        p = rowptrT[i];
+        while (p < rowptrT[i + 1] && (colxT[p] >> kTagBits) < 1u) ++p;
+        segT[2 * i] = p;
+        while (p < rowptrT[i + 1] && (colxT[p] >> kTagBits) < 2u) ++p;
+        segT[2 * i + 1] = p;
+    }
     c->neq = neq;
     c->nnz = nnz;
+    c->lanes_f = c->lanes_a = 0;
+    HRN_CUDA(c, c->d_seg.alloc(seg.size() * 4));
+    HRN_CUDA(c, c->d_segT.alloc(segT.size() * 4));
+    HRN_CUDA(c, cudaMemcpy(c->d_seg.p, seg.data(), seg.size() * 4, cudaMemcpyHostToDevice));
+    HRN_CUDA(c, cudaMemcpy(c->d_segT.p, segT.data(), segT.size() * 4, cudaMemcpyHostToDevice));
     HRN_CUDA(c, c->d_rowptr.alloc(rowptr.size() * 4));
     HRN_CUDA(c, c->d_colx.alloc(std::max<size_t>(colx.size(), 1) * 4));
     HRN_CUDA(c, c->d_rowidx.alloc(std::max<size_t>(rowidx.size(), 1) * 4));
@@ -238,6 +257,7 @@ static int ensure_state(hrn_ctx *c)
     const size_t S = size_t(c->nshot), eb = c->elem_bytes();
     HRN_CUDA(c, c->d_X.alloc(2 * 3 * size_t(c->neq) * S * eb));
     HRN_CUDA(c, c->d_KB.alloc(3 * size_t(c->neq) * S * eb));
+    HRN_CUDA(c, c->d_MB.alloc(2 * 3 * size_t(c->neq) * S * eb));
     HRN_CUDA(c, c->d_hist.alloc(std::max<size_t>(size_t(c->nstep + 1) * c->nstore * S * eb, 1)));
     return 0;
 }
@@ -608,6 +628,24 @@ int hrn_get_gradient_device(hrn_ctx *c, double *d_g_lambda, double *d_g_mu)
     if (d_g_lambda) HRN_CUDA(c, cudaMemcpyAsync(d_g_lambda, c->d_g.p, size_t(c->nj) * 8, cudaMemcpyDeviceToDevice, c->stream));
     if (d_g_mu)
         HRN_CUDA(c, cudaMemcpyAsync(d_g_mu, c->d_g.as<double>() + c->nj, size_t(c->nj) * 8, cudaMemcpyDeviceToDevice, c->stream));
+    return HRN_OK;
+}
+
+int hrn_set_variant(hrn_ctx *c, int32_t forward, int32_t adjoint)
+{
+    if (!c) return HRN_EARG;
+    auto ok = [](int v) { return v == 0 || v == 40 || v == 80 || v == 160 || v == 41 || v == 81 || v == 161; };
+    if (!ok(forward) || !ok(adjoint)) return set_error(c, HRN_EARG, "variant must be 0 (tune) or lanes*10+mat with lanes 4/8/16, mat 0/1");
+    c->lanes_f = forward;
+    c->lanes_a = adjoint;
+    return HRN_OK;
+}
+
+int hrn_get_variant(hrn_ctx *c, int32_t *forward, int32_t *adjoint)
+{
+    if (!c) return HRN_EARG;
+    if (forward) *forward = c->lanes_f;
+    if (adjoint) *adjoint = c->lanes_a;
     return HRN_OK;
 }
 

@@ -60,6 +60,8 @@ struct hrn_ctx {
     std::vector<uint32_t> h_colx;
     hrn::DevBuf d_rowptr, d_colx, d_rowidx;   // forward pattern (+ row of each entry)
     hrn::DevBuf d_rowptrT, d_colxT, d_permT;  // transposed pattern, perm into forward entries
+    hrn::DevBuf d_seg, d_segT;                // [neq] int2: first K and first G entry of each row
+    int lanes_f = 0, lanes_a = 0;             // stage-kernel variant, lanes*10+mat (0 = tune on first use)
     hrn::DevBuf d_raw;                        // unscaled values (FP64)
     hrn::DevBuf d_fwd, d_adj;                 // scaled forward values, transposed adjoint values (T)
     hrn::DevBuf d_diag_m, d_im;               // FP64 mass diagonal and its reciprocal
@@ -113,12 +115,20 @@ struct hrn_ctx {
     // ---- state and histories
     hrn::DevBuf d_X;              // [2][3][neq][S]
     hrn::DevBuf d_KB;             // [3][neq][S]
+    hrn::DevBuf d_MB;             // [2][3][neq][S] materialized stage inputs
     hrn::DevBuf d_hist;           // [nstep+1][nstore][S]
     hrn::DevBuf d_phist;          // adjoint history (optional)
     bool have_forward = false;
     bool have_phist = false;
     hrn::DevBuf d_g;              // [2][nj] FP64 gradient accumulators (lambda, mu)
     bool have_data = false;       // measured data resident on the device
+
+    // ---- inversion (model update)
+    hrn::DevBuf d_red;            // reduction partials
+    int lbfgs_m = 0;
+    hrn::DevBuf d_lbfgs;          // [4][M][nj] Ys_l, Ys_m, Ss_l, Ss_m, then 6 scratch vectors [nj]
+    hrn::DevBuf d_restrict;       // [nj] restriction to the regular domain (1 / 0)
+    std::vector<double> lbfgs_rho, lbfgs_alpha;
 
     // ---- timing
     int64_t launches = 0;          // kernels launched by this context (cumulative)
@@ -141,6 +151,8 @@ int run_misfit(hrn_ctx *c, double *cost);
 int build_rd_geometry(hrn_ctx *c);
 int assemble_device(hrn_ctx *c, bool discover_pattern);
 int finalize_pattern_from_keys(hrn_ctx *c, const std::vector<uint64_t> &keys);
+int vec_reduce(hrn_ctx *c, int kind, int n, const double *x, const double *y, double *out);
+int vec_axpby(hrn_ctx *c, int n, double a, const double *x, double b, const double *y, double *z);
 int set_error(hrn_ctx *c, int code, const std::string &msg);
 int cuda_error(hrn_ctx *c, cudaError_t e, const char *what);
 }  // namespace hrn

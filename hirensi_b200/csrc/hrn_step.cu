@@ -27,16 +27,35 @@ namespace hrn {
 // ----------------------------------------------------------------------------
 // small vector helpers
 
+// Read-only vector loads of the S shots of one row: one 256-bit load for 32
+// bytes (sm_100 ld.global.nc.v4.f64 / v8.f32), 128-bit or narrower otherwise, so
+// each gathered row record costs one request per 32-byte sector.
+__device__ __forceinline__ void ld256(const double *p, double &a, double &b, double &c, double &d)
+{
+    asm volatile("ld.global.nc.v4.f64 {%0,%1,%2,%3}, [%4];" : "=d"(a), "=d"(b), "=d"(c), "=d"(d) : "l"(p));
+}
+__device__ __forceinline__ void ld256(const float *p, float (&o)[8])
+{
+    asm volatile("ld.global.nc.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+                 : "=f"(o[0]), "=f"(o[1]), "=f"(o[2]), "=f"(o[3]), "=f"(o[4]), "=f"(o[5]), "=f"(o[6]), "=f"(o[7])
+                 : "l"(p));
+}
+
 template <typename T, int S>
 __device__ __forceinline__ void ldv(const T *__restrict__ p, T (&o)[S])
 {
-    if constexpr (sizeof(T) == 8 && S % 2 == 0) {
+    if constexpr (sizeof(T) == 8 && S % 4 == 0) {
+#pragma unroll
+        for (int s = 0; s < S; s += 4) ld256(p + s, o[s], o[s + 1], o[s + 2], o[s + 3]);
+    } else if constexpr (sizeof(T) == 8 && S % 2 == 0) {
 #pragma unroll
         for (int s = 0; s < S; s += 2) {
             double2 v = __ldg(reinterpret_cast<const double2 *>(p) + s / 2);
             o[s] = v.x;
             o[s + 1] = v.y;
         }
+    } else if constexpr (sizeof(T) == 4 && S % 8 == 0) {
+        ld256(p, o);
     } else if constexpr (sizeof(T) == 4 && S % 4 == 0) {
 #pragma unroll
         for (int s = 0; s < S; s += 4) {
@@ -81,12 +100,15 @@ template <typename T>
 struct StageArgs {
     int n;
     const int32_t *__restrict__ rowptr;
+    const int2 *__restrict__ seg;           // [n] first K entry, first G entry of each row
     const uint32_t *__restrict__ colx;
     const T *__restrict__ val;
     const T *__restrict__ x1, *__restrict__ x2, *__restrict__ x3;
     const T *__restrict__ kb1, *__restrict__ kb2, *__restrict__ kb3;
     T *__restrict__ kb_out;                 // stages 1-3
     T *__restrict__ y1, *__restrict__ y2, *__restrict__ y3;   // stage 4
+    const T *__restrict__ in_t, *__restrict__ in_m, *__restrict__ in_h;   // materialized stage inputs
+    T *__restrict__ out_t, *__restrict__ out_m, *__restrict__ out_h;      // next-stage inputs
     const int32_t *__restrict__ slot;       // [n] source slot or -1
     const T *__restrict__ srcv;             // [4][nslot][S] this step
     int nslot;
@@ -95,28 +117,27 @@ struct StageArgs {
     T c, D, d6;                             // dt/2, dt, dt/6 (negated for the adjoint)
 };
 
-// Stage-input value of matrix `tag` at column j (see the file comment).
-template <typename T, int S, int STAGE>
-__device__ __forceinline__ void gather(const StageArgs<T> &a, int tag, size_t j, T (&v)[S])
+// Stage-input value of matrix TAG at column j (see the file comment).
+template <typename T, int S, int STAGE, int TAG>
+__device__ __forceinline__ void gather(const StageArgs<T> &a, size_t j, T (&v)[S])
 {
     const size_t o = j * S;
     if constexpr (STAGE == 1) {
-        const T *src = tag == 0 ? a.x3 : (tag == 1 ? a.x2 : a.x1);
-        ldv<T, S>(src + o, v);
+        ldv<T, S>((TAG == 0 ? a.x3 : (TAG == 1 ? a.x2 : a.x1)) + o, v);
     } else if constexpr (STAGE == 2) {
         T p[S], q[S];
-        if (tag == 0) { ldv<T, S>(a.kb1 + o, p); ldv<T, S>(a.x3 + o, q); }
-        else if (tag == 1) { ldv<T, S>(a.x3 + o, p); ldv<T, S>(a.x2 + o, q); }
+        if constexpr (TAG == 0) { ldv<T, S>(a.kb1 + o, p); ldv<T, S>(a.x3 + o, q); }
+        else if constexpr (TAG == 1) { ldv<T, S>(a.x3 + o, p); ldv<T, S>(a.x2 + o, q); }
         else { ldv<T, S>(a.x2 + o, p); ldv<T, S>(a.x1 + o, q); }
 #pragma unroll
         for (int s = 0; s < S; ++s) v[s] = fmaT(a.c, p[s], q[s]);
     } else if constexpr (STAGE == 3) {
-        if (tag == 0) {
+        if constexpr (TAG == 0) {
             T p[S], q[S];
             ldv<T, S>(a.kb2 + o, p); ldv<T, S>(a.x3 + o, q);
 #pragma unroll
             for (int s = 0; s < S; ++s) v[s] = fmaT(a.c, p[s], q[s]);
-        } else if (tag == 1) {
+        } else if constexpr (TAG == 1) {
             T k1[S], x3[S], x2[S];
             ldv<T, S>(a.kb1 + o, k1); ldv<T, S>(a.x3 + o, x3); ldv<T, S>(a.x2 + o, x2);
 #pragma unroll
@@ -128,12 +149,12 @@ __device__ __forceinline__ void gather(const StageArgs<T> &a, int tag, size_t j,
             for (int s = 0; s < S; ++s) v[s] = fmaT(a.c, fmaT(a.c, x3[s], x2[s]), x1[s]);
         }
     } else {
-        if (tag == 0) {
+        if constexpr (TAG == 0) {
             T p[S], q[S];
             ldv<T, S>(a.kb3 + o, p); ldv<T, S>(a.x3 + o, q);
 #pragma unroll
             for (int s = 0; s < S; ++s) v[s] = fmaT(a.D, p[s], q[s]);
-        } else if (tag == 1) {
+        } else if constexpr (TAG == 1) {
             T k2[S], x3[S], x2[S];
             ldv<T, S>(a.kb2 + o, k2); ldv<T, S>(a.x3 + o, x3); ldv<T, S>(a.x2 + o, x2);
 #pragma unroll
@@ -147,8 +168,25 @@ __device__ __forceinline__ void gather(const StageArgs<T> &a, int tag, size_t j,
     }
 }
 
-// G lanes per row; rows of a warp are independent sub-groups.
-template <typename T, int S, int STAGE, int G>
+// Stage input of the entry's matrix at column j: rebuilt from x and earlier kb
+// (MAT = 0), or read from the vectors the previous stage materialized (MAT = 1).
+template <typename T, int S, int STAGE, int MAT>
+__device__ __forceinline__ void gather_any(const StageArgs<T> &a, int tag, size_t j, T (&v)[S])
+{
+    if constexpr (MAT == 1 && STAGE > 1) {
+        const T *src = tag == 0 ? a.in_m : (tag == 1 ? a.in_t : a.in_h);
+        ldv<T, S>(src + j * S, v);
+    } else {
+        if (tag == 0) gather<T, S, STAGE, 0>(a, j, v);
+        else if (tag == 1) gather<T, S, STAGE, 1>(a, j, v);
+        else gather<T, S, STAGE, 2>(a, j, v);
+    }
+}
+
+// G lanes per row; rows of a warp are independent sub-groups.  A row holds its
+// C, K and G entries back to back; seg[row] = (first K entry, first G entry).
+// Each lane takes four entries per trip so that their loads are in flight together.
+template <typename T, int S, int STAGE, int G, int MAT>
 __global__ void __launch_bounds__(256) rk4_stage(const StageArgs<T> a)
 {
     const int tid = blockIdx.x * blockDim.x + threadIdx.x;
@@ -160,14 +198,28 @@ __global__ void __launch_bounds__(256) rk4_stage(const StageArgs<T> a)
     T acc[S];
 #pragma unroll
     for (int s = 0; s < S; ++s) acc[s] = T(0);
-    const int k0 = __ldg(a.rowptr + row), k1 = __ldg(a.rowptr + row + 1);
-    for (int k = k0 + lane; k < k1; k += G) {
-        const uint32_t cx = __ldg(a.colx + k);
-        const T v = __ldg(a.val + k);
-        T x[S];
-        gather<T, S, STAGE>(a, int(cx >> kTagBits), size_t(cx & kColMask), x);
+    const int k0 = __ldg(a.rowptr + row), k3 = __ldg(a.rowptr + row + 1);
+    const int2 sg = __ldg(a.seg + row);
+    // four entries per lane per trip: all column/value loads (streamed, evict-first)
+    // issue before the gathers that depend on them
+    for (int k = k0 + lane; k < k3; k += 4 * G) {
+        uint32_t cx[4];
+        T vv[4];
 #pragma unroll
-        for (int s = 0; s < S; ++s) acc[s] = fmaT(v, x[s], acc[s]);
+        for (int u = 0; u < 4; ++u) {
+            const int kk = k + u * G;
+            const bool in = kk < k3;
+            cx[u] = in ? __ldcs(a.colx + kk) : __ldcs(a.colx + k);
+            vv[u] = in ? __ldcs(a.val + kk) : T(0);
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int kk = k + u * G;
+            T x[S];
+            gather_any<T, S, STAGE, MAT>(a, kk >= sg.y ? 2 : (kk >= sg.x ? 1 : 0), size_t(cx[u] & kColMask), x);
+#pragma unroll
+            for (int s = 0; s < S; ++s) acc[s] = fmaT(vv[u], x[s], acc[s]);
+        }
     }
 #pragma unroll
     for (int off = G / 2; off > 0; off >>= 1)
@@ -199,6 +251,28 @@ __global__ void __launch_bounds__(256) rk4_stage(const StageArgs<T> a)
     }
     if constexpr (STAGE < 4) {
         stv<T, S>(a.kb_out + o, kb);
+        if constexpr (MAT == 1) {
+            // next-stage inputs of this row: kt' = c km + x2, km' = c kb + x3, h' = c kt + x1
+            T x1[S], x2[S], x3[S], kt[S], km[S], nt[S], nm[S], nh[S];
+            ldv<T, S>(a.x1 + o, x1); ldv<T, S>(a.x2 + o, x2); ldv<T, S>(a.x3 + o, x3);
+            if constexpr (STAGE == 1) {
+#pragma unroll
+                for (int s = 0; s < S; ++s) { kt[s] = x2[s]; km[s] = x3[s]; }
+            } else {
+                ldv<T, S>(a.in_t + o, kt);
+                ldv<T, S>(a.in_m + o, km);
+            }
+            const T cc = STAGE == 3 ? a.D : a.c;
+#pragma unroll
+            for (int s = 0; s < S; ++s) {
+                nt[s] = fmaT(cc, km[s], x2[s]);
+                nm[s] = fmaT(cc, kb[s], x3[s]);
+                nh[s] = fmaT(cc, kt[s], x1[s]);
+            }
+            stv<T, S>(a.out_t + o, nt);
+            stv<T, S>(a.out_m + o, nm);
+            stv<T, S>(a.out_h + o, nh);
+        }
     } else {
         T x1[S], x2[S], x3[S], k1[S], k2[S], k3[S], n1[S], n2[S], n3[S];
         ldv<T, S>(a.x1 + o, x1); ldv<T, S>(a.x2 + o, x2); ldv<T, S>(a.x3 + o, x3);
@@ -471,16 +545,26 @@ int launch_scale_operator(hrn_ctx *c)
     return c->precision == HRN_FP64 ? scale_operator_t<double>(c) : scale_operator_t<float>(c);
 }
 
-// lanes per row of the stage kernel
-constexpr int kLanes = 8;
+// Stage-kernel variant: lanes per row (4, 8, 16) x stage inputs rebuilt at the
+// gather (0) or materialized by the previous stage (1); encoded lanes * 10 + mat
+// and chosen per operator by timing.
+constexpr int kVariants[6] = {40, 80, 160, 41, 81, 161};
 
 template <typename T, int S, int STAGE>
-static void launch_stage(const StageArgs<T> &a, cudaStream_t st)
+static void launch_stage(const StageArgs<T> &a, int variant, cudaStream_t st)
 {
     const int th = 256;
-    const int64_t threads = int64_t(a.n) * kLanes;
+    const int lanes = variant / 10;
+    const int64_t threads = int64_t(a.n) * lanes;
     const int blocks = int((threads + th - 1) / th);
-    rk4_stage<T, S, STAGE, kLanes><<<blocks, th, 0, st>>>(a);
+    switch (variant) {
+    case 40: rk4_stage<T, S, STAGE, 4, 0><<<blocks, th, 0, st>>>(a); break;
+    case 160: rk4_stage<T, S, STAGE, 16, 0><<<blocks, th, 0, st>>>(a); break;
+    case 41: rk4_stage<T, S, STAGE, 4, 1><<<blocks, th, 0, st>>>(a); break;
+    case 81: rk4_stage<T, S, STAGE, 8, 1><<<blocks, th, 0, st>>>(a); break;
+    case 161: rk4_stage<T, S, STAGE, 16, 1><<<blocks, th, 0, st>>>(a); break;
+    default: rk4_stage<T, S, STAGE, 8, 0><<<blocks, th, 0, st>>>(a); break;
+    }
 }
 
 struct StageTimer {
@@ -659,21 +743,25 @@ static int build_rd_store(hrn_ctx *c)
 // time loops
 
 template <typename T, int S>
-static void launch_step(hrn_ctx *c, StageArgs<T> a, T *X, T *Y, StageTimer *tm)
+static void launch_step(hrn_ctx *c, StageArgs<T> a, T *X, T *Y, StageTimer *tm, int lanes)
 {
     const size_t vn = size_t(c->neq) * S;
     T *kb = c->d_KB.as<T>();
     a.x1 = X; a.x2 = X + vn; a.x3 = X + 2 * vn;
     a.kb1 = kb; a.kb2 = kb + vn; a.kb3 = kb + 2 * vn;
     a.y1 = Y; a.y2 = Y + vn; a.y3 = Y + 2 * vn;
+    T *mA = c->d_MB.as<T>(), *mB = mA + 3 * vn;   // two sets of materialized stage inputs
     for (int st = 1; st <= 4; ++st) {
         if (tm) cudaEventRecord(tm->get(), c->stream);
         a.kb_out = st < 4 ? kb + size_t(st - 1) * vn : nullptr;
+        T *in = (st == 3) ? mB : mA, *out = (st == 2) ? mB : mA;   // stage s reads set (s%2), writes the other
+        a.in_t = in; a.in_m = in + vn; a.in_h = in + 2 * vn;
+        a.out_t = out; a.out_m = out + vn; a.out_h = out + 2 * vn;
         switch (st) {
-        case 1: launch_stage<T, S, 1>(a, c->stream); break;
-        case 2: launch_stage<T, S, 2>(a, c->stream); break;
-        case 3: launch_stage<T, S, 3>(a, c->stream); break;
-        default: launch_stage<T, S, 4>(a, c->stream); break;
+        case 1: launch_stage<T, S, 1>(a, lanes, c->stream); break;
+        case 2: launch_stage<T, S, 2>(a, lanes, c->stream); break;
+        case 3: launch_stage<T, S, 3>(a, lanes, c->stream); break;
+        default: launch_stage<T, S, 4>(a, lanes, c->stream); break;
         }
         ++c->launches;
         if (tm) cudaEventRecord(tm->get(), c->stream);
@@ -690,6 +778,33 @@ static double sum_timer(hrn_ctx *c, const StageTimer &tm)
         tot += ms;
     }
     return tot;
+}
+
+// Lanes per row for one operator: the fastest of 4, 8 and 16 over a few full
+// RK4 steps on the zero state (the traffic does not depend on the values).
+template <typename T, int S>
+static int autotune_lanes(hrn_ctx *c, StageArgs<T> a, T *X, T *Y)
+{
+    a.hist = nullptr;
+    float best = 1e30f;
+    int pick = 80;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    for (int lanes : kVariants) {
+        launch_step<T, S>(c, a, X, Y, nullptr, lanes);   // warm-up
+        cudaEventRecord(e0, c->stream);
+        for (int r = 0; r < 3; ++r) launch_step<T, S>(c, a, X, Y, nullptr, lanes);
+        cudaEventRecord(e1, c->stream);
+        cudaEventSynchronize(e1);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (ms < best) { best = ms; pick = lanes; }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    HRN_CUDA(c, cudaGetLastError());
+    return pick;
 }
 
 template <typename T, int S>
@@ -712,6 +827,7 @@ static int forward_t(hrn_ctx *c)
     StageArgs<T> a{};
     a.n = c->neq;
     a.rowptr = c->d_rowptr.as<int32_t>();
+    a.seg = c->d_seg.as<int2>();
     a.colx = c->d_colx.as<uint32_t>();
     a.val = c->d_fwd.as<T>();
     a.slot = c->d_slot_f.as<int32_t>();
@@ -720,12 +836,19 @@ static int forward_t(hrn_ctx *c)
     a.c = T(0.5 * c->dt);
     a.D = T(c->dt);
     a.d6 = T(c->dt / 6.0);
+    if (c->lanes_f <= 0) {
+        a.srcv = c->d_srcv_f.as<T>();
+        const int r = autotune_lanes<T, S>(c, a, X0, X1);
+        if (r < 40) return r;
+        c->lanes_f = r;
+        HRN_CUDA(c, cudaMemsetAsync(X0, 0, 3 * vn * sizeof(T), c->stream));
+    }
     StageTimer tm(c);
     for (int n = 0; n <= c->nstep; ++n) {
         a.srcv = c->nslot_f ? c->d_srcv_f.as<T>() + size_t(n) * 4 * c->nslot_f * S : nullptr;
         a.hist = c->d_hist.as<T>() + size_t(n) * c->nstore * S;
         T *X = (n & 1) ? X1 : X0, *Y = (n & 1) ? X0 : X1;
-        launch_step<T, S>(c, a, X, Y, c->timing ? &tm : nullptr);
+        launch_step<T, S>(c, a, X, Y, c->timing ? &tm : nullptr, c->lanes_f);
     }
     HRN_CUDA(c, cudaGetLastError());
     cudaEventRecord(t1, c->stream);
@@ -764,6 +887,7 @@ static int adjoint_t(hrn_ctx *c, int lambda_2mu, int keep_p)
     StageArgs<T> a{};
     a.n = c->neq;
     a.rowptr = c->d_rowptrT.as<int32_t>();
+    a.seg = c->d_segT.as<int2>();
     a.colx = c->d_colxT.as<uint32_t>();
     a.val = c->d_adj.as<T>();
     a.slot = c->d_slot_a.as<int32_t>();
@@ -773,6 +897,12 @@ static int adjoint_t(hrn_ctx *c, int lambda_2mu, int keep_p)
     a.c = T(-0.5 * c->dt);
     a.D = T(-c->dt);
     a.d6 = T(-c->dt / 6.0);
+    if (c->lanes_a <= 0) {
+        const int r = autotune_lanes<T, S>(c, a, X0, X1);
+        if (r < 40) return r;
+        c->lanes_a = r;
+        HRN_CUDA(c, cudaMemsetAsync(X0, 0, 3 * vn * sizeof(T), c->stream));
+    }
     StageTimer tm(c);
     double *gl = c->d_g.as<double>(), *gmu = gl + c->nj;
     const int gblocks = (c->nel_rd + kGradElems - 1) / kGradElems;
@@ -785,7 +915,7 @@ static int adjoint_t(hrn_ctx *c, int lambda_2mu, int keep_p)
                 c->d_im.as<double>(), c->d_srcv_a.as<T>()); ++c->launches;
         a.hist = keep_p ? c->d_phist.as<T>() + size_t(n) * c->nstore * S : nullptr;
         T *X = (it & 1) ? X1 : X0, *Y = (it & 1) ? X0 : X1;
-        launch_step<T, S>(c, a, X, Y, c->timing ? &tm : nullptr);
+        launch_step<T, S>(c, a, X, Y, c->timing ? &tm : nullptr, c->lanes_a);
         if (n <= c->nstep - 1 && c->nel_rd > 0)
             k_gradient<T, S><<<gblocks, 128, 0, c->stream>>>(c->nel_rd, c->d_rd_store.as<int32_t>(), c->d_rd_elems.as<int32_t>(),
                                                              c->d_inod.as<int32_t>(), c->d_rd_geom.as<double>(),

@@ -157,6 +157,15 @@ class Solver:
             d = self._dis(dis_meas)
             self._check(self._L.hrn_set_data(self.h, d.ctypes.data_as(C.c_void_p), 0))
 
+    def set_variant(self, forward: int = 0, adjoint: int = 0):
+        """Force the stage-kernel variant (lanes*10 + materialized), 0 = autotune."""
+        self._check(self._L.hrn_set_variant(self.h, int(forward), int(adjoint)))
+
+    def variant(self):
+        f, a = C.c_int32(), C.c_int32()
+        self._check(self._L.hrn_get_variant(self.h, C.byref(f), C.byref(a)))
+        return f.value, a.value
+
     def launch_count(self) -> int:
         n = C.c_int64()
         self._check(self._L.hrn_launch_count(self.h, C.byref(n)))

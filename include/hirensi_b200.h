@@ -130,6 +130,39 @@ int hrn_get_adjoint_history(hrn_ctx *ctx, int32_t shot, double *p_store);
 /* Copy the accumulated gradient to device buffers [nj] (either may be NULL). */
 int hrn_get_gradient_device(hrn_ctx *ctx, double *d_g_lambda, double *d_g_mu);
 
+/* ---- model update of the inversion loop (device vectors, FP64) ------------------
+ * All vector arguments are device pointers of length n (nodal vectors: n = nj).
+ * Reductions are deterministic (fixed-order two-pass sums). */
+
+/* out = x . y  (VecDot) */
+int hrn_vec_dot(hrn_ctx *ctx, int32_t n, const double *x, const double *y, double *out);
+/* kind 2: Euclidean norm, kind 0: max norm (VecNorm NORM_2 / NORM_INFINITY) */
+int hrn_vec_norm(hrn_ctx *ctx, int32_t n, const double *x, int32_t kind, double *out);
+/* z = a x + b y (y may be NULL: z = a x); covers VecAXPY, VecWAXPY, VecScale, VecCopy */
+int hrn_vec_axpby(hrn_ctx *ctx, int32_t n, double a, const double *x, double b, const double *y, double *z);
+/* z = x .* y (VecPointwiseMult) */
+int hrn_vec_mul(hrn_ctx *ctx, int32_t n, const double *x, const double *y, double *z);
+/* x = min(max(x, lo), hi): the material bounds of S4/Program_Main.F90:651-678 */
+int hrn_vec_clip(hrn_ctx *ctx, int32_t n, double lo, double hi, double *x);
+/* y[i] = x[map[i]]: the PML material extension scatter (vscat_mat_extend, :633-636) */
+int hrn_vec_gather(hrn_ctx *ctx, int32_t n, const int32_t *map, const double *x, double *y);
+
+/* TV regularization vectors and costs of the nodal lambda, mu
+ * (Assem_TV_TN_Regularization, S4/Assemble_PETSc_3D.F90:755-849, unweighted). */
+int hrn_regularization_tv(hrn_ctx *ctx, const double *d_lambda, const double *d_mu, double *d_reg_lambda,
+                          double *d_reg_mu, double *cost_lambda, double *cost_mu);
+/* Lumped gradient mass Mg per node (Assem_R_Mg_3D, S4/Assemble_PETSc_3D.F90:670-747). */
+int hrn_gradient_mass(hrn_ctx *ctx, double *d_mg);
+
+/* Coupled L-BFGS with memory m (S4/LBFGS_Coupled.F90).  restriction[nj] is 1 in
+ * the regular domain, 0 in the PML (S4/Control_Problem_Operators.F90:14-22). */
+int hrn_lbfgs_setup(hrn_ctx *ctx, int32_t m, const double *d_restriction);
+/* p = -H g for iteration `iter` (p = -g when iter == iter_begin); rho_out gets
+ * 1 / (y_lambda.s_lambda + y_mu.s_mu) of the new pair (may be NULL). */
+int hrn_lbfgs_direction(hrn_ctx *ctx, int32_t iter, int32_t iter_begin, const double *g_lambda, const double *g_mu,
+                        const double *g_lambda_pre, const double *g_mu_pre, const double *lambda, const double *mu,
+                        const double *lambda_pre, const double *mu_pre, double *p_lambda, double *p_mu, double *rho_out);
+
 /* ---- streams and timing -------------------------------------------------------- */
 
 /* Launch all work of this context on `stream` (a cudaStream_t, NULL = the
@@ -144,6 +177,13 @@ int hrn_set_timing(hrn_ctx *ctx, int32_t enable);
  * duration and number of launches of the fused stage kernel since timing was
  * last enabled. */
 int hrn_last_timing(hrn_ctx *ctx, double *total_ms, double *stage_kernel_ms, int64_t *stage_launches);
+
+/* Stage-kernel variant per operator (forward, adjoint): lanes per row * 10 +
+ * (1 if the stage inputs are materialized by the previous stage, 0 if rebuilt
+ * at every gather), lanes in {4, 8, 16}; 0 = time all variants on first use
+ * and keep the fastest (the default after every new sparsity pattern). */
+int hrn_set_variant(hrn_ctx *ctx, int32_t forward, int32_t adjoint);
+int hrn_get_variant(hrn_ctx *ctx, int32_t *forward, int32_t *adjoint);
 
 /* Number of kernels this context has launched since it was created. */
 int hrn_launch_count(hrn_ctx *ctx, int64_t *n);

@@ -97,3 +97,20 @@ def test_gradient_fp32_within_1e4(gpu_lib):
         gl, gm = s.adjoint_gradient(dis)
         assert rel_l2(gl, gl_ref) < TOL32_GRAD
         assert rel_l2(gm, gm_ref) < TOL32_GRAD
+
+
+@pytest.mark.parametrize("variant", [40, 80, 160, 41, 81, 161])
+def test_every_stage_kernel_variant_matches_oracle(gpu_lib, variant):
+    p = tiny(nshot=2, nstep=120)
+    _, _, hist_t = oracle_forward(p, p["lam_t"], p["mu_t"])
+    om, S, hist = oracle_forward(p, p["lam"], p["mu"])
+    dis = np.stack([traces_from_history(p, h) for h in hist_t])
+    pk = S.adjoint(p["nstep"], p["dt"], p["mesh"].store_eq, hist[0], p["eqdis"], p["eqdis_map"], dis[0])
+    with _solver(p, S) as s:
+        s.set_variant(variant, variant)
+        s.forward()
+        assert s.variant() == (variant, variant)
+        for k in range(2):
+            assert rel_l2(s.history(k), hist[k]) < TOL64
+        s.adjoint_gradient(dis, keep_p=True)
+        assert rel_l2(s.adjoint_history(0)[1:], pk[1:]) < TOL64
