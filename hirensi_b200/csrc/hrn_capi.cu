@@ -71,6 +71,25 @@ static int install_pattern(hrn_ctx *c, int32_t neq, std::vector<int32_t> &rowptr
         while (p < rowptrT[i + 1] && (colxT[p] >> kTagBits) < 2u) ++p;
         segT[2 * i + 1] = p;
     }
+    // tiles of consecutive rows with at most kTileEntries entries (tiled stage kernel)
+    auto make_tiles = [&](const std::vector<int32_t> &rp, std::vector<int32_t> &tl) -> bool {
+        tl.assign(1, 0);
+        for (int32_t i = 0; i < neq; ++i) {
+            if (rp[i + 1] - rp[i] > kTileEntries) return false;
+            if (rp[i + 1] - rp[tl.back()] > kTileEntries) tl.push_back(i);
+        }
+        tl.push_back(neq);
+        return true;
+    };
+    std::vector<int32_t> tiles, tilesT;
+    if (!make_tiles(rowptr, tiles) || !make_tiles(rowptrT, tilesT))
+        return set_error(c, HRN_EARG, "a row has more stored entries than a tile holds");
+    HRN_CUDA(c, c->d_tiles.alloc(tiles.size() * 4));
+    HRN_CUDA(c, c->d_tilesT.alloc(tilesT.size() * 4));
+    HRN_CUDA(c, cudaMemcpy(c->d_tiles.p, tiles.data(), tiles.size() * 4, cudaMemcpyHostToDevice));
+    HRN_CUDA(c, cudaMemcpy(c->d_tilesT.p, tilesT.data(), tilesT.size() * 4, cudaMemcpyHostToDevice));
+    c->ntiles = int(tiles.size()) - 1;
+    c->ntilesT = int(tilesT.size()) - 1;
     c->neq = neq;
     c->nnz = nnz;
     c->lanes_f = c->lanes_a = 0;
@@ -79,10 +98,10 @@ static int install_pattern(hrn_ctx *c, int32_t neq, std::vector<int32_t> &rowptr
     HRN_CUDA(c, cudaMemcpy(c->d_seg.p, seg.data(), seg.size() * 4, cudaMemcpyHostToDevice));
     HRN_CUDA(c, cudaMemcpy(c->d_segT.p, segT.data(), segT.size() * 4, cudaMemcpyHostToDevice));
     HRN_CUDA(c, c->d_rowptr.alloc(rowptr.size() * 4));
-    HRN_CUDA(c, c->d_colx.alloc(std::max<size_t>(colx.size(), 1) * 4));
+    HRN_CUDA(c, c->d_colx.alloc(colx.size() * 4 + kBulkPad));
     HRN_CUDA(c, c->d_rowidx.alloc(std::max<size_t>(rowidx.size(), 1) * 4));
     HRN_CUDA(c, c->d_rowptrT.alloc(rowptrT.size() * 4));
-    HRN_CUDA(c, c->d_colxT.alloc(std::max<size_t>(colxT.size(), 1) * 4));
+    HRN_CUDA(c, c->d_colxT.alloc(colxT.size() * 4 + kBulkPad));
     HRN_CUDA(c, c->d_permT.alloc(std::max<size_t>(permT.size(), 1) * 8));
     HRN_CUDA(c, c->d_raw.alloc(std::max<size_t>(size_t(nnz), 1) * 8));
     HRN_CUDA(c, cudaMemcpy(c->d_rowptr.p, rowptr.data(), rowptr.size() * 4, cudaMemcpyHostToDevice));
@@ -306,6 +325,12 @@ int hrn_create(int device, int precision, hrn_ctx **out)
         return HRN_ECUDA;
     }
     c->stream = c->own_stream;
+    cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device);
+    if (c->d_step_err.alloc(16) != cudaSuccess || cudaMemset(c->d_step_err.p, 0, 16) != cudaSuccess) {
+        cudaGetLastError();
+        delete c;
+        return HRN_EOOM;
+    }
     *out = c;
     return HRN_OK;
 }
@@ -634,8 +659,8 @@ int hrn_get_gradient_device(hrn_ctx *c, double *d_g_lambda, double *d_g_mu)
 int hrn_set_variant(hrn_ctx *c, int32_t forward, int32_t adjoint)
 {
     if (!c) return HRN_EARG;
-    auto ok = [](int v) { return v == 0 || v == 40 || v == 80 || v == 160 || v == 41 || v == 81 || v == 161; };
-    if (!ok(forward) || !ok(adjoint)) return set_error(c, HRN_EARG, "variant must be 0 (tune) or lanes*10+mat with lanes 4/8/16, mat 0/1");
+    auto ok = [](int v) { return v == 0 || v == 40 || v == 80 || v == 160 || v == 41 || v == 81 || v == 161 || v == 42 || v == 43 || v == 82 || v == 83; };
+    if (!ok(forward) || !ok(adjoint)) return set_error(c, HRN_EARG, "variant must be 0 (tune) or lanes*10 + mat + tiled (lanes 4/8/16, mat 0/1, tiled 0/2; tiled only with lanes 4/8)");
     c->lanes_f = forward;
     c->lanes_a = adjoint;
     return HRN_OK;

@@ -38,6 +38,8 @@ struct DevBuf {
 };
 
 constexpr int kTagBits = 30;
+constexpr int kTileEntries = 4096;     // entries per tile of the tiled stage kernel
+constexpr size_t kBulkPad = 64;        // bytes past the end of bulk-copied arrays
 constexpr uint32_t kColMask = (1u << kTagBits) - 1u;
 
 }  // namespace hrn
@@ -62,6 +64,10 @@ struct hrn_ctx {
     hrn::DevBuf d_rowptrT, d_colxT, d_permT;  // transposed pattern, perm into forward entries
     hrn::DevBuf d_seg, d_segT;                // [neq] int2: first K and first G entry of each row
     int lanes_f = 0, lanes_a = 0;             // stage-kernel variant, lanes*10+mat (0 = tune on first use)
+    hrn::DevBuf d_tiles, d_tilesT;            // row boundaries of the tiles of the tiled stage kernel
+    int ntiles = 0, ntilesT = 0;
+    int num_sms = 148;
+    hrn::DevBuf d_step_err;                   // device flag: a bounded wait of a stage kernel timed out
     hrn::DevBuf d_raw;                        // unscaled values (FP64)
     hrn::DevBuf d_fwd, d_adj;                 // scaled forward values, transposed adjoint values (T)
     hrn::DevBuf d_diag_m, d_im;               // FP64 mass diagonal and its reciprocal

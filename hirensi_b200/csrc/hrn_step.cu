@@ -183,50 +183,11 @@ __device__ __forceinline__ void gather_any(const StageArgs<T> &a, int tag, size_
     }
 }
 
-// G lanes per row; rows of a warp are independent sub-groups.  A row holds its
-// C, K and G entries back to back; seg[row] = (first K entry, first G entry).
-// Each lane takes four entries per trip so that their loads are in flight together.
-template <typename T, int S, int STAGE, int G, int MAT>
-__global__ void __launch_bounds__(256) rk4_stage(const StageArgs<T> a)
+// Row epilogue: stage source, history (stage 1), kb or the next-stage inputs
+// (stages 1-3) or the RK4 update into the other state buffer (stage 4).
+template <typename T, int S, int STAGE, int MAT>
+__device__ __forceinline__ void finish_row(const StageArgs<T> &a, int row, const T (&acc)[S])
 {
-    const int tid = blockIdx.x * blockDim.x + threadIdx.x;
-    const int row = tid / G;
-    const int lane = threadIdx.x & (G - 1);
-    if (row >= a.n) return;   // uniform over the G lanes of a row
-    const unsigned gmask = (G == 32) ? 0xffffffffu : (((1u << G) - 1u) << ((threadIdx.x & 31) & ~(G - 1)));
-
-    T acc[S];
-#pragma unroll
-    for (int s = 0; s < S; ++s) acc[s] = T(0);
-    const int k0 = __ldg(a.rowptr + row), k3 = __ldg(a.rowptr + row + 1);
-    const int2 sg = __ldg(a.seg + row);
-    // four entries per lane per trip: all column/value loads (streamed, evict-first)
-    // issue before the gathers that depend on them
-    for (int k = k0 + lane; k < k3; k += 4 * G) {
-        uint32_t cx[4];
-        T vv[4];
-#pragma unroll
-        for (int u = 0; u < 4; ++u) {
-            const int kk = k + u * G;
-            const bool in = kk < k3;
-            cx[u] = in ? __ldcs(a.colx + kk) : __ldcs(a.colx + k);
-            vv[u] = in ? __ldcs(a.val + kk) : T(0);
-        }
-#pragma unroll
-        for (int u = 0; u < 4; ++u) {
-            const int kk = k + u * G;
-            T x[S];
-            gather_any<T, S, STAGE, MAT>(a, kk >= sg.y ? 2 : (kk >= sg.x ? 1 : 0), size_t(cx[u] & kColMask), x);
-#pragma unroll
-            for (int s = 0; s < S; ++s) acc[s] = fmaT(vv[u], x[s], acc[s]);
-        }
-    }
-#pragma unroll
-    for (int off = G / 2; off > 0; off >>= 1)
-#pragma unroll
-        for (int s = 0; s < S; ++s) acc[s] += __shfl_xor_sync(gmask, acc[s], off, G);
-    if (lane != 0) return;
-
     const size_t o = size_t(row) * S;
     T kb[S];
     const int sl = __ldg(a.slot + row);
@@ -297,6 +258,202 @@ __global__ void __launch_bounds__(256) rk4_stage(const StageArgs<T> a)
         stv<T, S>(a.y2 + o, n2);
         stv<T, S>(a.y3 + o, n3);
     }
+}
+
+// G lanes per row; rows of a warp are independent sub-groups.  A row holds its
+// C, K and G entries back to back; seg[row] = (first K entry, first G entry).
+// Each lane takes four entries per trip so that their loads are in flight together.
+template <typename T, int S, int STAGE, int G, int MAT>
+__global__ void __launch_bounds__(256) rk4_stage(const StageArgs<T> a)
+{
+    const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+    const int row = tid / G;
+    const int lane = threadIdx.x & (G - 1);
+    if (row >= a.n) return;   // uniform over the G lanes of a row
+    const unsigned gmask = (G == 32) ? 0xffffffffu : (((1u << G) - 1u) << ((threadIdx.x & 31) & ~(G - 1)));
+
+    T acc[S];
+#pragma unroll
+    for (int s = 0; s < S; ++s) acc[s] = T(0);
+    const int k0 = __ldg(a.rowptr + row), k3 = __ldg(a.rowptr + row + 1);
+    const int2 sg = __ldg(a.seg + row);
+    // four entries per lane per trip: all column/value loads (streamed, evict-first)
+    // issue before the gathers that depend on them
+    for (int k = k0 + lane; k < k3; k += 4 * G) {
+        uint32_t cx[4];
+        T vv[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int kk = k + u * G;
+            const bool in = kk < k3;
+            cx[u] = in ? __ldcs(a.colx + kk) : __ldcs(a.colx + k);
+            vv[u] = in ? __ldcs(a.val + kk) : T(0);
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int kk = k + u * G;
+            T x[S];
+            gather_any<T, S, STAGE, MAT>(a, kk >= sg.y ? 2 : (kk >= sg.x ? 1 : 0), size_t(cx[u] & kColMask), x);
+#pragma unroll
+            for (int s = 0; s < S; ++s) acc[s] = fmaT(vv[u], x[s], acc[s]);
+        }
+    }
+#pragma unroll
+    for (int off = G / 2; off > 0; off >>= 1)
+#pragma unroll
+        for (int s = 0; s < S; ++s) acc[s] += __shfl_xor_sync(gmask, acc[s], off, G);
+    if (lane != 0) return;
+
+    finish_row<T, S, STAGE, MAT>(a, row, acc);
+}
+
+// ----------------------------------------------------------------------------
+// tiled stage kernel: each CTA walks tiles of consecutive rows (at most
+// kTileE entries); the column and value slab of the next tile is streamed into
+// shared memory by 1-D bulk copies (cp.async.bulk, completion on an mbarrier)
+// while the current tile is processed, so the gathers only wait on
+// shared-memory reads.  Waits are bounded; a timeout sets *err and stops the CTA.
+
+constexpr int kTileE = kTileEntries;  // entries per tile
+constexpr int kTileThreads = 512;
+constexpr int kTileSlack = 8;         // alignment slack of a buffer, entries
+
+template <typename T>
+constexpr size_t tile_smem_bytes()
+{
+    return 128 + 2 * (size_t(kTileE + kTileSlack) * 4 + size_t(kTileE + kTileSlack) * sizeof(T));
+}
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) { return uint32_t(__cvta_generic_to_shared(p)); }
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                 ::"r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(bar)) : "memory");
+}
+
+// bounded wait for the phase with the given parity; false on timeout
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity)
+{
+    const uint32_t addr = smem_u32(bar);
+    for (int i = 0; i < (1 << 20); ++i) {
+        uint32_t done;
+        asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+                     : "=r"(done) : "r"(addr), "r"(parity) : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+template <typename T>
+__device__ __forceinline__ void tile_issue(const StageArgs<T> &a, const int32_t *tiles, int t, uint32_t *cb, T *vb,
+                                           uint64_t *bar)
+{
+    const int e0 = __ldg(a.rowptr + __ldg(tiles + t)), e1 = __ldg(a.rowptr + __ldg(tiles + t + 1));
+    constexpr int va_mask = int(16 / sizeof(T)) - 1;
+    const int ca = e0 & ~3, va = e0 & ~va_mask;
+    const uint32_t cn = uint32_t(((e1 - ca) * 4 + 15) & ~15);
+    const uint32_t vn = uint32_t(((e1 - va) * int(sizeof(T)) + 15) & ~15);
+    if (e1 == e0) {
+        asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+        return;
+    }
+    mbar_expect_tx(bar, cn + vn);
+    bulk_g2s(cb, a.colx + ca, cn, bar);
+    bulk_g2s(vb, a.val + va, vn, bar);
+}
+
+template <typename T, int S, int STAGE, int G, int MAT>
+__global__ void __launch_bounds__(kTileThreads) rk4_stage_tile(const StageArgs<T> a, const int32_t *__restrict__ tiles,
+                                                               int ntiles, int *__restrict__ err)
+{
+    extern __shared__ __align__(128) unsigned char smem[];
+    uint64_t *bar = reinterpret_cast<uint64_t *>(smem);
+    uint32_t *cbuf[2];
+    T *vbuf[2];
+    {
+        size_t off = 128;
+        for (int b = 0; b < 2; ++b) {
+            cbuf[b] = reinterpret_cast<uint32_t *>(smem + off);
+            off += size_t(kTileE + kTileSlack) * 4;
+            vbuf[b] = reinterpret_cast<T *>(smem + off);
+            off += size_t(kTileE + kTileSlack) * sizeof(T);
+        }
+    }
+    __shared__ int abort_flag;
+    if (threadIdx.x == 0) {
+        mbar_init(bar, 1);
+        mbar_init(bar + 1, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        abort_flag = 0;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0 && int(blockIdx.x) < ntiles) tile_issue<T>(a, tiles, blockIdx.x, cbuf[0], vbuf[0], bar);
+    const int lane = threadIdx.x & (G - 1);
+    const unsigned gmask = (G == 32) ? 0xffffffffu : (((1u << G) - 1u) << ((threadIdx.x & 31) & ~(G - 1)));
+    int it = 0;
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++it) {
+        const int b = it & 1;
+        const int tn = t + gridDim.x;
+        if (threadIdx.x == 0 && tn < ntiles) tile_issue<T>(a, tiles, tn, cbuf[b ^ 1], vbuf[b ^ 1], bar + (b ^ 1));
+        const bool ok = mbar_wait(bar + b, uint32_t((it >> 1) & 1));
+        if (__syncthreads_or(!ok)) {
+            if (threadIdx.x == 0) {
+                atomicExch(err, 1);
+                abort_flag = 1;
+            }
+            break;
+        }
+        const int r0 = __ldg(tiles + t), r1 = __ldg(tiles + t + 1);
+        const int e0 = __ldg(a.rowptr + r0);
+        const int ca = e0 & ~3, va = e0 & ~(int(16 / sizeof(T)) - 1);
+        const uint32_t *cb = cbuf[b];
+        const T *vb = vbuf[b];
+        for (int row = r0 + int(threadIdx.x) / G; row < r1; row += kTileThreads / G) {
+            T acc[S];
+#pragma unroll
+            for (int s = 0; s < S; ++s) acc[s] = T(0);
+            const int k0 = __ldg(a.rowptr + row), k3 = __ldg(a.rowptr + row + 1);
+            const int2 sg = __ldg(a.seg + row);
+            for (int k = k0 + lane; k < k3; k += 4 * G) {
+                uint32_t cx[4];
+                T vv[4];
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const int kk = k + u * G;
+                    const bool in = kk < k3;
+                    cx[u] = cb[(in ? kk : k) - ca];
+                    vv[u] = in ? vb[kk - va] : T(0);
+                }
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const int kk = k + u * G;
+                    T x[S];
+                    gather_any<T, S, STAGE, MAT>(a, kk >= sg.y ? 2 : (kk >= sg.x ? 1 : 0), size_t(cx[u] & kColMask), x);
+#pragma unroll
+                    for (int s = 0; s < S; ++s) acc[s] = fmaT(vv[u], x[s], acc[s]);
+                }
+            }
+#pragma unroll
+            for (int off = G / 2; off > 0; off >>= 1)
+#pragma unroll
+                for (int s = 0; s < S; ++s) acc[s] += __shfl_xor_sync(gmask, acc[s], off, G);
+            if (lane == 0) finish_row<T, S, STAGE, MAT>(a, row, acc);
+        }
+        __syncthreads();   // buffer b is refilled only after every thread is done with it
+    }
+    // on abort, let the copy still in flight into the other buffer land (bounded)
+    if (abort_flag && threadIdx.x == 0) mbar_wait(bar + ((it & 1) ^ 1), uint32_t(((it + 1) >> 1) & 1));
 }
 
 // ----------------------------------------------------------------------------
@@ -527,8 +684,9 @@ template <typename T>
 static int scale_operator_t(hrn_ctx *c)
 {
     const int th = 256;
-    if (c->d_fwd.bytes != size_t(c->nnz) * sizeof(T)) HRN_CUDA(c, c->d_fwd.alloc(size_t(c->nnz) * sizeof(T)));
-    if (c->d_adj.bytes != size_t(c->nnz) * sizeof(T)) HRN_CUDA(c, c->d_adj.alloc(size_t(c->nnz) * sizeof(T)));
+    const size_t vb = size_t(c->nnz) * sizeof(T) + kBulkPad;
+    if (c->d_fwd.bytes != vb) HRN_CUDA(c, c->d_fwd.alloc(vb));
+    if (c->d_adj.bytes != vb) HRN_CUDA(c, c->d_adj.alloc(vb));
     if (c->nnz == 0) return 0;
     k_scale_fwd<T><<<blocks_for(c->nnz, th), th, 0, c->stream>>>(c->nnz, c->d_rowidx.as<int32_t>(), c->d_raw.as<double>(),
                                                                   c->d_im.as<double>(), c->d_fwd.as<T>()); ++c->launches;
@@ -545,14 +703,40 @@ int launch_scale_operator(hrn_ctx *c)
     return c->precision == HRN_FP64 ? scale_operator_t<double>(c) : scale_operator_t<float>(c);
 }
 
+struct TileArgs {
+    const int32_t *tiles;
+    int ntiles, grid;
+    int *err;
+};
+
 // Stage-kernel variant: lanes per row (4, 8, 16) x stage inputs rebuilt at the
-// gather (0) or materialized by the previous stage (1); encoded lanes * 10 + mat
-// and chosen per operator by timing.
-constexpr int kVariants[6] = {40, 80, 160, 41, 81, 161};
+// gather (0) or materialized by the previous stage (1) x row-parallel (0) or
+// tiled with bulk-copied matrix slabs (2); encoded lanes * 10 + mat + tiled,
+// chosen per operator by timing.
+constexpr int kVariants[10] = {40, 80, 160, 41, 81, 161, 42, 43, 82, 83};
+
+template <typename T, int S, int STAGE, int G, int MAT>
+static void launch_tile(const StageArgs<T> &a, const TileArgs &ta, cudaStream_t st)
+{
+    static bool attr_set = false;
+    constexpr size_t smem = tile_smem_bytes<T>();
+    if (!attr_set) {
+        cudaFuncSetAttribute(rk4_stage_tile<T, S, STAGE, G, MAT>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+        attr_set = true;
+    }
+    rk4_stage_tile<T, S, STAGE, G, MAT><<<ta.grid, kTileThreads, smem, st>>>(a, ta.tiles, ta.ntiles, ta.err);
+}
 
 template <typename T, int S, int STAGE>
-static void launch_stage(const StageArgs<T> &a, int variant, cudaStream_t st)
+static void launch_stage(const StageArgs<T> &a, int variant, cudaStream_t st, const TileArgs &ta)
 {
+    switch (variant) {
+    case 42: launch_tile<T, S, STAGE, 4, 0>(a, ta, st); return;
+    case 43: launch_tile<T, S, STAGE, 4, 1>(a, ta, st); return;
+    case 82: launch_tile<T, S, STAGE, 8, 0>(a, ta, st); return;
+    case 83: launch_tile<T, S, STAGE, 8, 1>(a, ta, st); return;
+    default: break;
+    }
     const int th = 256;
     const int lanes = variant / 10;
     const int64_t threads = int64_t(a.n) * lanes;
@@ -743,7 +927,7 @@ static int build_rd_store(hrn_ctx *c)
 // time loops
 
 template <typename T, int S>
-static void launch_step(hrn_ctx *c, StageArgs<T> a, T *X, T *Y, StageTimer *tm, int lanes)
+static void launch_step(hrn_ctx *c, StageArgs<T> a, T *X, T *Y, StageTimer *tm, int lanes, const TileArgs &ta)
 {
     const size_t vn = size_t(c->neq) * S;
     T *kb = c->d_KB.as<T>();
@@ -758,10 +942,10 @@ static void launch_step(hrn_ctx *c, StageArgs<T> a, T *X, T *Y, StageTimer *tm, 
         a.in_t = in; a.in_m = in + vn; a.in_h = in + 2 * vn;
         a.out_t = out; a.out_m = out + vn; a.out_h = out + 2 * vn;
         switch (st) {
-        case 1: launch_stage<T, S, 1>(a, lanes, c->stream); break;
-        case 2: launch_stage<T, S, 2>(a, lanes, c->stream); break;
-        case 3: launch_stage<T, S, 3>(a, lanes, c->stream); break;
-        default: launch_stage<T, S, 4>(a, lanes, c->stream); break;
+        case 1: launch_stage<T, S, 1>(a, lanes, c->stream, ta); break;
+        case 2: launch_stage<T, S, 2>(a, lanes, c->stream, ta); break;
+        case 3: launch_stage<T, S, 3>(a, lanes, c->stream, ta); break;
+        default: launch_stage<T, S, 4>(a, lanes, c->stream, ta); break;
         }
         ++c->launches;
         if (tm) cudaEventRecord(tm->get(), c->stream);
@@ -783,7 +967,7 @@ static double sum_timer(hrn_ctx *c, const StageTimer &tm)
 // Lanes per row for one operator: the fastest of 4, 8 and 16 over a few full
 // RK4 steps on the zero state (the traffic does not depend on the values).
 template <typename T, int S>
-static int autotune_lanes(hrn_ctx *c, StageArgs<T> a, T *X, T *Y)
+static int autotune_lanes(hrn_ctx *c, StageArgs<T> a, T *X, T *Y, const TileArgs &ta)
 {
     a.hist = nullptr;
     float best = 1e30f;
@@ -792,9 +976,9 @@ static int autotune_lanes(hrn_ctx *c, StageArgs<T> a, T *X, T *Y)
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
     for (int lanes : kVariants) {
-        launch_step<T, S>(c, a, X, Y, nullptr, lanes);   // warm-up
+        launch_step<T, S>(c, a, X, Y, nullptr, lanes, ta);   // warm-up
         cudaEventRecord(e0, c->stream);
-        for (int r = 0; r < 3; ++r) launch_step<T, S>(c, a, X, Y, nullptr, lanes);
+        for (int r = 0; r < 3; ++r) launch_step<T, S>(c, a, X, Y, nullptr, lanes, ta);
         cudaEventRecord(e1, c->stream);
         cudaEventSynchronize(e1);
         float ms = 0.f;
@@ -805,6 +989,17 @@ static int autotune_lanes(hrn_ctx *c, StageArgs<T> a, T *X, T *Y)
     cudaEventDestroy(e1);
     HRN_CUDA(c, cudaGetLastError());
     return pick;
+}
+
+static int check_step_error(hrn_ctx *c)
+{
+    int err = 0;
+    HRN_CUDA(c, cudaMemcpy(&err, c->d_step_err.p, 4, cudaMemcpyDeviceToHost));
+    if (err) {
+        cudaMemset(c->d_step_err.p, 0, 4);
+        return set_error(c, HRN_ECUDA, "a bounded wait of the tiled stage kernel timed out");
+    }
+    return 0;
 }
 
 template <typename T, int S>
@@ -836,9 +1031,10 @@ static int forward_t(hrn_ctx *c)
     a.c = T(0.5 * c->dt);
     a.D = T(c->dt);
     a.d6 = T(c->dt / 6.0);
+    TileArgs ta{c->d_tiles.as<int32_t>(), c->ntiles, std::min(c->ntiles, 2 * c->num_sms), c->d_step_err.as<int>()};
     if (c->lanes_f <= 0) {
         a.srcv = c->d_srcv_f.as<T>();
-        const int r = autotune_lanes<T, S>(c, a, X0, X1);
+        const int r = autotune_lanes<T, S>(c, a, X0, X1, ta);
         if (r < 40) return r;
         c->lanes_f = r;
         HRN_CUDA(c, cudaMemsetAsync(X0, 0, 3 * vn * sizeof(T), c->stream));
@@ -848,7 +1044,7 @@ static int forward_t(hrn_ctx *c)
         a.srcv = c->nslot_f ? c->d_srcv_f.as<T>() + size_t(n) * 4 * c->nslot_f * S : nullptr;
         a.hist = c->d_hist.as<T>() + size_t(n) * c->nstore * S;
         T *X = (n & 1) ? X1 : X0, *Y = (n & 1) ? X0 : X1;
-        launch_step<T, S>(c, a, X, Y, c->timing ? &tm : nullptr, c->lanes_f);
+        launch_step<T, S>(c, a, X, Y, c->timing ? &tm : nullptr, c->lanes_f, ta);
     }
     HRN_CUDA(c, cudaGetLastError());
     cudaEventRecord(t1, c->stream);
@@ -862,6 +1058,7 @@ static int forward_t(hrn_ctx *c)
     c->last_stage_launches = c->timing ? int64_t(tm.used / 2) : 0;
     c->acc_stage_ms += c->last_stage_ms;
     c->acc_stage_launches += c->last_stage_launches;
+    if (int rc = check_step_error(c)) return rc;
     c->have_forward = true;
     c->have_phist = false;
     return 0;
@@ -897,8 +1094,9 @@ static int adjoint_t(hrn_ctx *c, int lambda_2mu, int keep_p)
     a.c = T(-0.5 * c->dt);
     a.D = T(-c->dt);
     a.d6 = T(-c->dt / 6.0);
+    TileArgs ta{c->d_tilesT.as<int32_t>(), c->ntilesT, std::min(c->ntilesT, 2 * c->num_sms), c->d_step_err.as<int>()};
     if (c->lanes_a <= 0) {
-        const int r = autotune_lanes<T, S>(c, a, X0, X1);
+        const int r = autotune_lanes<T, S>(c, a, X0, X1, ta);
         if (r < 40) return r;
         c->lanes_a = r;
         HRN_CUDA(c, cudaMemsetAsync(X0, 0, 3 * vn * sizeof(T), c->stream));
@@ -915,7 +1113,7 @@ static int adjoint_t(hrn_ctx *c, int lambda_2mu, int keep_p)
                 c->d_im.as<double>(), c->d_srcv_a.as<T>()); ++c->launches;
         a.hist = keep_p ? c->d_phist.as<T>() + size_t(n) * c->nstore * S : nullptr;
         T *X = (it & 1) ? X1 : X0, *Y = (it & 1) ? X0 : X1;
-        launch_step<T, S>(c, a, X, Y, c->timing ? &tm : nullptr, c->lanes_a);
+        launch_step<T, S>(c, a, X, Y, c->timing ? &tm : nullptr, c->lanes_a, ta);
         if (n <= c->nstep - 1 && c->nel_rd > 0)
             k_gradient<T, S><<<gblocks, 128, 0, c->stream>>>(c->nel_rd, c->d_rd_store.as<int32_t>(), c->d_rd_elems.as<int32_t>(),
                                                              c->d_inod.as<int32_t>(), c->d_rd_geom.as<double>(),
@@ -934,6 +1132,7 @@ static int adjoint_t(hrn_ctx *c, int lambda_2mu, int keep_p)
     c->last_stage_launches = c->timing ? int64_t(tm.used / 2) : 0;
     c->acc_stage_ms += c->last_stage_ms;
     c->acc_stage_launches += c->last_stage_launches;
+    if (int rc = check_step_error(c)) return rc;
     c->have_phist = keep_p != 0;
     return 0;
 }
