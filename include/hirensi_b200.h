@@ -116,6 +116,18 @@ int hrn_get_traces(hrn_ctx *ctx, double *traces);
  * dis_meas NULL uses the data of hrn_set_data. */
 int hrn_misfit(hrn_ctx *ctx, const double *dis_meas, double *cost);
 
+/* The misfit of hrn_misfit for callers that cannot allocate device memory.
+ * It has no counterpart in the reference.  d_dis_meas is a DEVICE pointer to
+ * Dis_meas laid out as for hrn_set_data ([nshot][nrec3][nstep+1]); it is read
+ * in place and not kept.  The scratch is one static device array shared by
+ * every context and call in the process, so nothing is allocated.  Limit:
+ * nshot * (nstep + 1) <= 131072, larger problems return HRN_EARG.  The first
+ * call on a device looks the array's address up (cudaGetSymbolAddress) with
+ * that device current; make that first call before any stream capture.  Calls
+ * whose kernels overlap on one GPU (other streams, other contexts, other host
+ * threads) race on the scratch: serialize them.  Blocks until *cost is ready. */
+int hrn_misfit_noalloc(hrn_ctx *ctx, const double *d_dis_meas, double *cost);
+
 /* Adjoint RK4 (OtD) with the zero-lag gradient fused into each step:
  * EXPLICIT_RK4_PETSC_PML_3D_Adjoint_OtD (:1125-1405) followed by
  * EXPLICIT_RK4_PETSC_PML_3D_Control_OtD (:1413-1522), summed over shots.
