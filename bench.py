@@ -50,6 +50,8 @@ def parse_args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fwi", action="store_true", help="skip the FWI time-to-misfit leg")
     ap.add_argument("--fwi-iters", type=int, default=10)
+    ap.add_argument("--variant", type=int, default=0,
+                    help="stage-kernel variant for forward and adjoint (0 = chosen by timing on first use)")
     return ap.parse_args()
 
 
@@ -135,7 +137,7 @@ def stage_bytes(nnz_total: int, n: int, shots: int, bv: int) -> float:
     """Average algorithmic bytes of one RK4 stage launch: every stored entry once
     (value + 4-byte column), three row pointers, and per shot four stage vectors
     read/written per stage plus the x1..x3 update once per step
-    (B_step / 4 of the per-step formula of the scope table)."""
+    (one quarter of the bytes of a whole RK4 step)."""
     matrix = nnz_total * (bv + 4) + 3 * 4 * (n + 1)
     vectors = shots * (4 * n * bv + 6 * n * bv / 4.0)
     return float(matrix + vectors)
@@ -166,6 +168,8 @@ def run_native(args, rank, world, local_rank):
         s.set_history(m.store_eq)
         s.set_shots(prob.nstep, prob.dt, prob.src_eq, prob.src_b, prob.ftab)
         s.set_receivers(prob.eqdis, prob.eqdis_map)
+        if args.variant:
+            s.set_variant(args.variant, args.variant)
         return s
 
     # measured data: FP64 forward of the true model (set-up, untimed)

@@ -399,6 +399,9 @@ int hrn_set_operator_csr(hrn_ctx *c, int32_t neq, const int32_t *c_ia, const int
     if (int rc = launch_scale_operator(c)) return rc;
     HRN_CUDA(c, cudaStreamSynchronize(c->stream));
     c->have_operator = true;
+    c->op_from_mesh = false;
+    if (c->lanes_f == 90 || c->lanes_f == 91) c->lanes_f = 0;   // matrix-free needs an assembled operator: tune again
+    if (c->lanes_a == 90 || c->lanes_a == 91) c->lanes_a = 0;
     c->have_forward = false;
     return rebind(c);
 }
@@ -417,6 +420,8 @@ int hrn_set_mesh(hrn_ctx *c, int32_t nj, int32_t nel, int32_t neq, const double 
     for (int e = 0; e < nel; ++e)
         if (mtel[e] != 1 && mtel[e] != 2) return set_error(c, HRN_EARG, "MTEL must be 1 (RD) or 2 (PML)");
     cudaSetDevice(c->device);
+    c->have_elem = false;
+    c->op_from_mesh = false;
     c->nj = nj;
     c->nel = nel;
     c->neq = neq;
@@ -462,6 +467,7 @@ static int assemble_common(hrn_ctx *c, const double *lambda, const double *mu, b
     const bool first = !c->have_pattern;
     if (int rc = assemble_device(c, first)) return rc;
     c->have_operator = true;
+    c->op_from_mesh = true;
     c->have_forward = false;
     if (first) return rebind(c);
     return HRN_OK;
@@ -659,8 +665,13 @@ int hrn_get_gradient_device(hrn_ctx *c, double *d_g_lambda, double *d_g_mu)
 int hrn_set_variant(hrn_ctx *c, int32_t forward, int32_t adjoint)
 {
     if (!c) return HRN_EARG;
-    auto ok = [](int v) { return v == 0 || v == 40 || v == 80 || v == 160 || v == 41 || v == 81 || v == 161 || v == 42 || v == 43 || v == 82 || v == 83; };
-    if (!ok(forward) || !ok(adjoint)) return set_error(c, HRN_EARG, "variant must be 0 (tune) or lanes*10 + mat + tiled (lanes 4/8/16, mat 0/1, tiled 0/2; tiled only with lanes 4/8)");
+    auto ok = [](int v) {
+        return v == 0 || v == 40 || v == 80 || v == 160 || v == 41 || v == 81 || v == 161 || v == 42 || v == 43 || v == 82 ||
+               v == 83 || v == 90 || v == 91;
+    };
+    if (!ok(forward) || !ok(adjoint))
+        return set_error(c, HRN_EARG, "variant must be 0 (tune), lanes*10 + mat + tiled (lanes 4/8/16, mat 0/1, tiled 0/2; "
+                                      "tiled only with lanes 4/8) or 90 / 91 (matrix-free, element slots / atomics)");
     c->lanes_f = forward;
     c->lanes_a = adjoint;
     return HRN_OK;

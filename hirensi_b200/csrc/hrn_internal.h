@@ -89,6 +89,15 @@ struct hrn_ctx {
     hrn::DevBuf d_lam, d_mu;      // nodal material (FP64)
     hrn::DevBuf d_touched;        // pattern discovery flags
     hrn::DevBuf d_asm_err;        // device error flag of the assembly kernels
+    // matrix-free element operator (variants 90 and 91 of the stage kernels)
+    bool op_from_mesh = false;    // the operator was assembled from the current mesh and material
+    bool have_elem = false;       // element lists, node slot lists and the row map are built
+    int nel_pml_e = 0, nel_rd_e = 0;
+    hrn::DevBuf d_el_pml, d_el_rde;   // element ids of the PML and of the regular domain
+    hrn::DevBuf d_nslot_ptr, d_nslot; // [nj + 1], per node: element * 27 + point (top bit: RD element)
+    hrn::DevBuf d_row_info;       // [neq] node << 4 | DOF
+    hrn::DevBuf d_eslots;         // [nel * 27][9][S] element contributions (T)
+    hrn::DevBuf d_eacc;           // [neq][S] row accumulator of the atomic variant (T), kept zero between stages
 
     // ---- history
     int nstore = 0;
@@ -158,6 +167,9 @@ int build_rd_geometry(hrn_ctx *c);
 int assemble_device(hrn_ctx *c, bool discover_pattern);
 int finalize_pattern_from_keys(hrn_ctx *c, const std::vector<uint64_t> &keys);
 int vec_reduce(hrn_ctx *c, int kind, int n, const double *x, const double *y, double *out);
+int elem_prepare(hrn_ctx *c);
+int elem_ready(hrn_ctx *c);
+int elem_stage(hrn_ctx *c, const void *stage_args, int stage, int adj, int acc);
 int vec_axpby(hrn_ctx *c, int n, double a, const double *x, double b, const double *y, double *z);
 int set_error(hrn_ctx *c, int code, const std::string &msg);
 int cuda_error(hrn_ctx *c, cudaError_t e, const char *what);

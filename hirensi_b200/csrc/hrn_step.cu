@@ -21,101 +21,10 @@
 #include <vector>
 
 #include "hrn_internal.h"
+#include "hrn_stage.cuh"
 
 namespace hrn {
 
-// ----------------------------------------------------------------------------
-// small vector helpers
-
-// Read-only vector loads of the S shots of one row: one 256-bit load for 32
-// bytes (sm_100 ld.global.nc.v4.f64 / v8.f32), 128-bit or narrower otherwise, so
-// each gathered row record costs one request per 32-byte sector.
-__device__ __forceinline__ void ld256(const double *p, double &a, double &b, double &c, double &d)
-{
-    asm volatile("ld.global.nc.v4.f64 {%0,%1,%2,%3}, [%4];" : "=d"(a), "=d"(b), "=d"(c), "=d"(d) : "l"(p));
-}
-__device__ __forceinline__ void ld256(const float *p, float (&o)[8])
-{
-    asm volatile("ld.global.nc.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
-                 : "=f"(o[0]), "=f"(o[1]), "=f"(o[2]), "=f"(o[3]), "=f"(o[4]), "=f"(o[5]), "=f"(o[6]), "=f"(o[7])
-                 : "l"(p));
-}
-
-template <typename T, int S>
-__device__ __forceinline__ void ldv(const T *__restrict__ p, T (&o)[S])
-{
-    if constexpr (sizeof(T) == 8 && S % 4 == 0) {
-#pragma unroll
-        for (int s = 0; s < S; s += 4) ld256(p + s, o[s], o[s + 1], o[s + 2], o[s + 3]);
-    } else if constexpr (sizeof(T) == 8 && S % 2 == 0) {
-#pragma unroll
-        for (int s = 0; s < S; s += 2) {
-            double2 v = __ldg(reinterpret_cast<const double2 *>(p) + s / 2);
-            o[s] = v.x;
-            o[s + 1] = v.y;
-        }
-    } else if constexpr (sizeof(T) == 4 && S % 8 == 0) {
-        ld256(p, o);
-    } else if constexpr (sizeof(T) == 4 && S % 4 == 0) {
-#pragma unroll
-        for (int s = 0; s < S; s += 4) {
-            float4 v = __ldg(reinterpret_cast<const float4 *>(p) + s / 4);
-            o[s] = v.x; o[s + 1] = v.y; o[s + 2] = v.z; o[s + 3] = v.w;
-        }
-    } else if constexpr (sizeof(T) == 4 && S % 2 == 0) {
-#pragma unroll
-        for (int s = 0; s < S; s += 2) {
-            float2 v = __ldg(reinterpret_cast<const float2 *>(p) + s / 2);
-            o[s] = v.x; o[s + 1] = v.y;
-        }
-    } else {
-#pragma unroll
-        for (int s = 0; s < S; ++s) o[s] = __ldg(p + s);
-    }
-}
-
-template <typename T, int S>
-__device__ __forceinline__ void stv(T *__restrict__ p, const T (&o)[S])
-{
-    if constexpr (sizeof(T) == 8 && S % 2 == 0) {
-#pragma unroll
-        for (int s = 0; s < S; s += 2) reinterpret_cast<double2 *>(p)[s / 2] = make_double2(o[s], o[s + 1]);
-    } else if constexpr (sizeof(T) == 4 && S % 4 == 0) {
-#pragma unroll
-        for (int s = 0; s < S; s += 4)
-            reinterpret_cast<float4 *>(p)[s / 4] = make_float4(o[s], o[s + 1], o[s + 2], o[s + 3]);
-    } else {
-#pragma unroll
-        for (int s = 0; s < S; ++s) p[s] = o[s];
-    }
-}
-
-__device__ __forceinline__ double fmaT(double a, double b, double c) { return fma(a, b, c); }
-__device__ __forceinline__ float fmaT(float a, float b, float c) { return fmaf(a, b, c); }
-
-// ----------------------------------------------------------------------------
-// stage kernel
-
-template <typename T>
-struct StageArgs {
-    int n;
-    const int32_t *__restrict__ rowptr;
-    const int2 *__restrict__ seg;           // [n] first K entry, first G entry of each row
-    const uint32_t *__restrict__ colx;
-    const T *__restrict__ val;
-    const T *__restrict__ x1, *__restrict__ x2, *__restrict__ x3;
-    const T *__restrict__ kb1, *__restrict__ kb2, *__restrict__ kb3;
-    T *__restrict__ kb_out;                 // stages 1-3
-    T *__restrict__ y1, *__restrict__ y2, *__restrict__ y3;   // stage 4
-    const T *__restrict__ in_t, *__restrict__ in_m, *__restrict__ in_h;   // materialized stage inputs
-    T *__restrict__ out_t, *__restrict__ out_m, *__restrict__ out_h;      // next-stage inputs
-    const int32_t *__restrict__ slot;       // [n] source slot or -1
-    const T *__restrict__ srcv;             // [4][nslot][S] this step
-    int nslot;
-    const int32_t *__restrict__ store_pos;  // [n] history position or -1 (stage 1)
-    T *__restrict__ hist;                   // [nstore][S] of this step, or null
-    T c, D, d6;                             // dt/2, dt, dt/6 (negated for the adjoint)
-};
 
 // Stage-input value of matrix TAG at column j (see the file comment).
 template <typename T, int S, int STAGE, int TAG>
@@ -183,82 +92,6 @@ __device__ __forceinline__ void gather_any(const StageArgs<T> &a, int tag, size_
     }
 }
 
-// Row epilogue: stage source, history (stage 1), kb or the next-stage inputs
-// (stages 1-3) or the RK4 update into the other state buffer (stage 4).
-template <typename T, int S, int STAGE, int MAT>
-__device__ __forceinline__ void finish_row(const StageArgs<T> &a, int row, const T (&acc)[S])
-{
-    const size_t o = size_t(row) * S;
-    T kb[S];
-    const int sl = __ldg(a.slot + row);
-    if (sl >= 0) {
-        T sv[S];
-        ldv<T, S>(a.srcv + (size_t(STAGE - 1) * a.nslot + sl) * S, sv);
-#pragma unroll
-        for (int s = 0; s < S; ++s) kb[s] = sv[s] + acc[s];
-    } else {
-#pragma unroll
-        for (int s = 0; s < S; ++s) kb[s] = acc[s];
-    }
-    if constexpr (STAGE == 1) {
-        if (a.hist) {
-            const int p = __ldg(a.store_pos + row);
-            if (p >= 0) {
-                T x2[S];
-                ldv<T, S>(a.x2 + o, x2);
-                stv<T, S>(a.hist + size_t(p) * S, x2);
-            }
-        }
-    }
-    if constexpr (STAGE < 4) {
-        stv<T, S>(a.kb_out + o, kb);
-        if constexpr (MAT == 1) {
-            // next-stage inputs of this row: kt' = c km + x2, km' = c kb + x3, h' = c kt + x1
-            T x1[S], x2[S], x3[S], kt[S], km[S], nt[S], nm[S], nh[S];
-            ldv<T, S>(a.x1 + o, x1); ldv<T, S>(a.x2 + o, x2); ldv<T, S>(a.x3 + o, x3);
-            if constexpr (STAGE == 1) {
-#pragma unroll
-                for (int s = 0; s < S; ++s) { kt[s] = x2[s]; km[s] = x3[s]; }
-            } else {
-                ldv<T, S>(a.in_t + o, kt);
-                ldv<T, S>(a.in_m + o, km);
-            }
-            const T cc = STAGE == 3 ? a.D : a.c;
-#pragma unroll
-            for (int s = 0; s < S; ++s) {
-                nt[s] = fmaT(cc, km[s], x2[s]);
-                nm[s] = fmaT(cc, kb[s], x3[s]);
-                nh[s] = fmaT(cc, kt[s], x1[s]);
-            }
-            stv<T, S>(a.out_t + o, nt);
-            stv<T, S>(a.out_m + o, nm);
-            stv<T, S>(a.out_h + o, nh);
-        }
-    } else {
-        T x1[S], x2[S], x3[S], k1[S], k2[S], k3[S], n1[S], n2[S], n3[S];
-        ldv<T, S>(a.x1 + o, x1); ldv<T, S>(a.x2 + o, x2); ldv<T, S>(a.x3 + o, x3);
-        ldv<T, S>(a.kb1 + o, k1); ldv<T, S>(a.kb2 + o, k2); ldv<T, S>(a.kb3 + o, k3);
-#pragma unroll
-        for (int s = 0; s < S; ++s) {
-            // stage inputs of this row, built exactly as gather() builds them
-            const T km2 = fmaT(a.c, k1[s], x3[s]);
-            const T km3 = fmaT(a.c, k2[s], x3[s]);
-            const T km4 = fmaT(a.D, k3[s], x3[s]);
-            const T kt2 = fmaT(a.c, x3[s], x2[s]);
-            const T kt3 = fmaT(a.c, km2, x2[s]);
-            const T kt4 = fmaT(a.D, km3, x2[s]);
-            const T ht = ((x2[s] + T(2) * kt2) + T(2) * kt3) + kt4;
-            const T hm = ((x3[s] + T(2) * km2) + T(2) * km3) + km4;
-            const T hb = ((k1[s] + T(2) * k2[s]) + T(2) * k3[s]) + kb[s];
-            n1[s] = fmaT(a.d6, ht, x1[s]);
-            n2[s] = fmaT(a.d6, hm, x2[s]);
-            n3[s] = fmaT(a.d6, hb, x3[s]);
-        }
-        stv<T, S>(a.y1 + o, n1);
-        stv<T, S>(a.y2 + o, n2);
-        stv<T, S>(a.y3 + o, n3);
-    }
-}
 
 // G lanes per row; rows of a warp are independent sub-groups.  A row holds its
 // C, K and G entries back to back; seg[row] = (first K entry, first G entry).
@@ -714,6 +547,8 @@ struct TileArgs {
 // tiled with bulk-copied matrix slabs (2); encoded lanes * 10 + mat + tiled,
 // chosen per operator by timing.
 constexpr int kVariants[10] = {40, 80, 160, 41, 81, 161, 42, 43, 82, 83};
+// 90 / 91: matrix-free element kernels with element slots / atomic row sums
+inline bool is_elem_variant(int v) { return v == 90 || v == 91; }
 
 template <typename T, int S, int STAGE, int G, int MAT>
 static void launch_tile(const StageArgs<T> &a, const TileArgs &ta, cudaStream_t st)
@@ -927,7 +762,7 @@ static int build_rd_store(hrn_ctx *c)
 // time loops
 
 template <typename T, int S>
-static void launch_step(hrn_ctx *c, StageArgs<T> a, T *X, T *Y, StageTimer *tm, int lanes, const TileArgs &ta)
+static void launch_step(hrn_ctx *c, StageArgs<T> a, T *X, T *Y, StageTimer *tm, int lanes, const TileArgs &ta, int adj)
 {
     const size_t vn = size_t(c->neq) * S;
     T *kb = c->d_KB.as<T>();
@@ -941,11 +776,15 @@ static void launch_step(hrn_ctx *c, StageArgs<T> a, T *X, T *Y, StageTimer *tm, 
         T *in = (st == 3) ? mB : mA, *out = (st == 2) ? mB : mA;   // stage s reads set (s%2), writes the other
         a.in_t = in; a.in_m = in + vn; a.in_h = in + 2 * vn;
         a.out_t = out; a.out_m = out + vn; a.out_h = out + 2 * vn;
-        switch (st) {
-        case 1: launch_stage<T, S, 1>(a, lanes, c->stream, ta); break;
-        case 2: launch_stage<T, S, 2>(a, lanes, c->stream, ta); break;
-        case 3: launch_stage<T, S, 3>(a, lanes, c->stream, ta); break;
-        default: launch_stage<T, S, 4>(a, lanes, c->stream, ta); break;
+        if (is_elem_variant(lanes)) {
+            elem_stage(c, &a, st, adj, lanes - 90);
+        } else {
+            switch (st) {
+            case 1: launch_stage<T, S, 1>(a, lanes, c->stream, ta); break;
+            case 2: launch_stage<T, S, 2>(a, lanes, c->stream, ta); break;
+            case 3: launch_stage<T, S, 3>(a, lanes, c->stream, ta); break;
+            default: launch_stage<T, S, 4>(a, lanes, c->stream, ta); break;
+            }
         }
         ++c->launches;
         if (tm) cudaEventRecord(tm->get(), c->stream);
@@ -967,18 +806,24 @@ static double sum_timer(hrn_ctx *c, const StageTimer &tm)
 // Lanes per row for one operator: the fastest of 4, 8 and 16 over a few full
 // RK4 steps on the zero state (the traffic does not depend on the values).
 template <typename T, int S>
-static int autotune_lanes(hrn_ctx *c, StageArgs<T> a, T *X, T *Y, const TileArgs &ta)
+static int autotune_lanes(hrn_ctx *c, StageArgs<T> a, T *X, T *Y, const TileArgs &ta, int adj)
 {
     a.hist = nullptr;
     float best = 1e30f;
     int pick = 80;
+    std::vector<int> cand(kVariants, kVariants + 10);
+    if (c->op_from_mesh) {
+        if (int rc = elem_ready(c)) return rc;
+        cand.push_back(90);
+        cand.push_back(91);
+    }
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
-    for (int lanes : kVariants) {
-        launch_step<T, S>(c, a, X, Y, nullptr, lanes, ta);   // warm-up
+    for (int lanes : cand) {
+        launch_step<T, S>(c, a, X, Y, nullptr, lanes, ta, adj);   // warm-up
         cudaEventRecord(e0, c->stream);
-        for (int r = 0; r < 3; ++r) launch_step<T, S>(c, a, X, Y, nullptr, lanes, ta);
+        for (int r = 0; r < 3; ++r) launch_step<T, S>(c, a, X, Y, nullptr, lanes, ta, adj);
         cudaEventRecord(e1, c->stream);
         cudaEventSynchronize(e1);
         float ms = 0.f;
@@ -1034,17 +879,19 @@ static int forward_t(hrn_ctx *c)
     TileArgs ta{c->d_tiles.as<int32_t>(), c->ntiles, std::min(c->ntiles, 2 * c->num_sms), c->d_step_err.as<int>()};
     if (c->lanes_f <= 0) {
         a.srcv = c->d_srcv_f.as<T>();
-        const int r = autotune_lanes<T, S>(c, a, X0, X1, ta);
+        const int r = autotune_lanes<T, S>(c, a, X0, X1, ta, 0);
         if (r < 40) return r;
         c->lanes_f = r;
         HRN_CUDA(c, cudaMemsetAsync(X0, 0, 3 * vn * sizeof(T), c->stream));
+    } else if (is_elem_variant(c->lanes_f)) {
+        if (int rc = elem_ready(c)) return rc;
     }
     StageTimer tm(c);
     for (int n = 0; n <= c->nstep; ++n) {
         a.srcv = c->nslot_f ? c->d_srcv_f.as<T>() + size_t(n) * 4 * c->nslot_f * S : nullptr;
         a.hist = c->d_hist.as<T>() + size_t(n) * c->nstore * S;
         T *X = (n & 1) ? X1 : X0, *Y = (n & 1) ? X0 : X1;
-        launch_step<T, S>(c, a, X, Y, c->timing ? &tm : nullptr, c->lanes_f, ta);
+        launch_step<T, S>(c, a, X, Y, c->timing ? &tm : nullptr, c->lanes_f, ta, 0);
     }
     HRN_CUDA(c, cudaGetLastError());
     cudaEventRecord(t1, c->stream);
@@ -1096,10 +943,12 @@ static int adjoint_t(hrn_ctx *c, int lambda_2mu, int keep_p)
     a.d6 = T(-c->dt / 6.0);
     TileArgs ta{c->d_tilesT.as<int32_t>(), c->ntilesT, std::min(c->ntilesT, 2 * c->num_sms), c->d_step_err.as<int>()};
     if (c->lanes_a <= 0) {
-        const int r = autotune_lanes<T, S>(c, a, X0, X1, ta);
+        const int r = autotune_lanes<T, S>(c, a, X0, X1, ta, 1);
         if (r < 40) return r;
         c->lanes_a = r;
         HRN_CUDA(c, cudaMemsetAsync(X0, 0, 3 * vn * sizeof(T), c->stream));
+    } else if (is_elem_variant(c->lanes_a)) {
+        if (int rc = elem_ready(c)) return rc;
     }
     StageTimer tm(c);
     double *gl = c->d_g.as<double>(), *gmu = gl + c->nj;
@@ -1113,7 +962,7 @@ static int adjoint_t(hrn_ctx *c, int lambda_2mu, int keep_p)
                 c->d_im.as<double>(), c->d_srcv_a.as<T>()); ++c->launches;
         a.hist = keep_p ? c->d_phist.as<T>() + size_t(n) * c->nstore * S : nullptr;
         T *X = (it & 1) ? X1 : X0, *Y = (it & 1) ? X0 : X1;
-        launch_step<T, S>(c, a, X, Y, c->timing ? &tm : nullptr, c->lanes_a, ta);
+        launch_step<T, S>(c, a, X, Y, c->timing ? &tm : nullptr, c->lanes_a, ta, 1);
         if (n <= c->nstep - 1 && c->nel_rd > 0)
             k_gradient<T, S><<<gblocks, 128, 0, c->stream>>>(c->nel_rd, c->d_rd_store.as<int32_t>(), c->d_rd_elems.as<int32_t>(),
                                                              c->d_inod.as<int32_t>(), c->d_rd_geom.as<double>(),
