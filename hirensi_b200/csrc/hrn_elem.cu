@@ -29,6 +29,7 @@
 #include <stdint.h>
 
 #include <algorithm>
+#include <type_traits>
 #include <vector>
 
 #include "hrn_internal.h"
@@ -36,7 +37,6 @@
 
 namespace hrn {
 
-__constant__ unsigned char e_node_at[27];   // local node at GLL point q = 9c + 3b + a
 __constant__ double e_pml[24];              // PML_PARAM rows x+, x-, y+, y-, z+, z-; cols alpha0, beta0, L, x0
 
 constexpr uint32_t kRdSlot = 0x80000000u;   // slot of a regular-domain element (displacements only)
@@ -87,209 +87,317 @@ __device__ void pml_coefs(const double *x, double A[10])
 
 template <typename T>
 struct ElemArgs {
-    const int32_t *el_pml, *el_rd;   // element ids by kind
-    int nel_pml, nel_rd, nb_pml;     // counts, blocks of PML elements
-    const int32_t *inod, *id;
-    const double *xyz, *geom, *lam, *mu, *rho;
+    int nel_pml, nel_rd, nb_pml;     // elements in processing order: PML first, then the regular domain
+    const int32_t *el_eq;            // [P][27][9] equation of each point's DOF (-1 fixed)
+    const int32_t *el_node;          // [P][27] node of each point
+    const double *el_geom;           // [P][27][10] DJI and w*detJ
+    const double *el_rho;            // [P]
+    const double *lam, *mu, *pmlw;   // nodal lambda, mu; [nj][12] PML weights
     const T *in_m, *in_t, *in_h;     // stage inputs of C, K, G
-    T *slots;                        // [nel * 27][9][S]
+    T *slots;                        // [P * 27][9][S]
     T *acc;                          // [neq][S] (atomic variant)
 };
 
-template <int S>
-constexpr int elems_per_block() { return S >= 8 ? 1 : 8 / S; }
+// Shot blocking: one thread handles SV consecutive shots of a point (vector
+// shared-memory and global accesses), TP = S / SV threads per point, and a block
+// takes EPB = 8 / TP elements (216 threads).
+template <int S, int SV>
+constexpr int elems_per_block() { return (S / SV) >= 8 ? 1 : 8 / (S / SV); }
 
-template <typename T, int S>
+constexpr int kCoef = 14;   // per point: lam, mu, F3 F2 F1 of kinds e, p, w, then b, c, d
+
+// displacement inputs Uu [EPB][3][27][3][S], fluxes V [EPB][27][9][S],
+// coefficients [EPB][27][kCoef], equation numbers [EPB][27][9]
+template <typename T, int S, int SV>
 constexpr size_t elem_smem_bytes()
 {
-    return size_t(elems_per_block<S>()) * (4 * 27 * 9 * S * sizeof(T) + 27 * sizeof(int));
+    return size_t(elems_per_block<S, SV>()) * ((3 * 81 * S + 243 * S + 27 * kCoef) * sizeof(T) + 243 * sizeof(int));
 }
 
-// One thread per (element, GLL point, shot).  ACC = 0: write the element's slot;
-// ACC = 1: add into the row accumulator.
-template <typename T, int S, int ADJ, int ACC>
-__global__ void __launch_bounds__(216, 2) k_elem(const ElemArgs<T> A)
+// N consecutive values from shared or global memory, vectorized when N values
+// fill 8 or 16 bytes (the callers keep such runs aligned to their size).
+template <typename T, int N>
+__device__ __forceinline__ void ld_n(const T *p, T (&o)[N])
 {
-    constexpr int EPB = elems_per_block<S>();
-    constexpr int NT = EPB * 27 * S;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    T *U = reinterpret_cast<T *>(smem_raw);                 // [EPB][3][27][9][S] stage inputs
-    T *V = U + EPB * 3 * 27 * 9 * S;                        // [EPB][27][3 c][3 m][S] divergence fluxes
-    int *nodes = reinterpret_cast<int *>(V + EPB * 27 * 9 * S);   // [EPB][27]
-
-    const bool pml = int(blockIdx.x) < A.nb_pml;
-    const int e0 = (pml ? int(blockIdx.x) : int(blockIdx.x) - A.nb_pml) * EPB;
-    const int ngrp = pml ? A.nel_pml : A.nel_rd;
-    const int32_t *list = pml ? A.el_pml : A.el_rd;
-
-    for (int i = threadIdx.x; i < EPB * 27; i += NT) {
-        const int el = i / 27;
-        nodes[i] = e0 + el < ngrp ? __ldg(A.inod + size_t(__ldg(list + e0 + el)) * 27 + e_node_at[i % 27]) : -1;
-    }
-    __syncthreads();
-    // stage inputs of the element's nodes (PML: C, K, G inputs x 9 DOF; RD: K input x 3 DOF)
-    const int ntag = pml ? 3 : 1, ndof = pml ? 9 : 3;
-    const int nitem = EPB * ntag * 27 * ndof;
-    for (int it = threadIdx.x; it < nitem; it += NT) {
-        const int dof = it % ndof;
-        int r = it / ndof;
-        const int q = r % 27;
-        r /= 27;
-        const int t = pml ? r % ntag : 1, el = r / ntag;
-        const int node = nodes[el * 27 + q];
-        const int eq = node >= 0 ? __ldg(A.id + size_t(node) * 9 + dof) : -1;
-        T v[S];
-        if (eq >= 0) {
-            ldv<T, S>((t == 0 ? A.in_m : (t == 1 ? A.in_t : A.in_h)) + size_t(eq) * S, v);
-        } else {
+    if constexpr (N * sizeof(T) == 16 && sizeof(T) == 4) {
+        const float4 v = *reinterpret_cast<const float4 *>(p);
+        o[0] = v.x; o[1] = v.y; o[2] = v.z; o[3] = v.w;
+    } else if constexpr (N * sizeof(T) == 16 && sizeof(T) == 8) {
+        const double2 v = *reinterpret_cast<const double2 *>(p);
+        o[0] = v.x; o[1] = v.y;
+    } else if constexpr (N * sizeof(T) == 8 && sizeof(T) == 4) {
+        const float2 v = *reinterpret_cast<const float2 *>(p);
+        o[0] = v.x; o[1] = v.y;
+    } else {
 #pragma unroll
-            for (int s = 0; s < S; ++s) v[s] = T(0);
-        }
-        T *dst = U + (((el * 3 + t) * 27 + q) * 9 + dof) * S;
-#pragma unroll
-        for (int s = 0; s < S; ++s) dst[s] = v[s];
+        for (int i = 0; i < N; ++i) o[i] = p[i];
     }
-    __syncthreads();
+}
+template <typename T, int N>
+__device__ __forceinline__ void ldg_n(const T *p, T (&o)[N])
+{
+    if constexpr (N * sizeof(T) == 16 && sizeof(T) == 4) {
+        const float4 v = __ldg(reinterpret_cast<const float4 *>(p));
+        o[0] = v.x; o[1] = v.y; o[2] = v.z; o[3] = v.w;
+    } else if constexpr (N * sizeof(T) == 16 && sizeof(T) == 8) {
+        const double2 v = __ldg(reinterpret_cast<const double2 *>(p));
+        o[0] = v.x; o[1] = v.y;
+    } else if constexpr (N * sizeof(T) == 8 && sizeof(T) == 4) {
+        const float2 v = __ldg(reinterpret_cast<const float2 *>(p));
+        o[0] = v.x; o[1] = v.y;
+    } else {
+#pragma unroll
+        for (int i = 0; i < N; ++i) o[i] = __ldg(p + i);
+    }
+}
+template <typename T, int N>
+__device__ __forceinline__ void st_n(T *p, const T (&o)[N])
+{
+    if constexpr (N * sizeof(T) == 16 && sizeof(T) == 4) {
+        *reinterpret_cast<float4 *>(p) = make_float4(o[0], o[1], o[2], o[3]);
+    } else if constexpr (N * sizeof(T) == 16 && sizeof(T) == 8) {
+        *reinterpret_cast<double2 *>(p) = make_double2(o[0], o[1]);
+    } else if constexpr (N * sizeof(T) == 8 && sizeof(T) == 4) {
+        *reinterpret_cast<float2 *>(p) = make_float2(o[0], o[1]);
+    } else {
+#pragma unroll
+        for (int i = 0; i < N; ++i) p[i] = o[i];
+    }
+}
+// Atomic add of N consecutive values (vector reductions for FP32).
+template <typename T, int N>
+__device__ __forceinline__ void red_n(T *p, const T (&o)[N])
+{
+    if constexpr (sizeof(T) == 4 && N == 4) {
+        asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(p), "f"(o[0]), "f"(o[1]), "f"(o[2]), "f"(o[3])
+                     : "memory");
+    } else if constexpr (sizeof(T) == 4 && N == 2) {
+        asm volatile("red.global.add.v2.f32 [%0], {%1, %2};" ::"l"(p), "f"(o[0]), "f"(o[1]) : "memory");
+    } else {
+#pragma unroll
+        for (int i = 0; i < N; ++i) atomicAdd(p + i, o[i]);
+    }
+}
 
+template <typename T, int S, int SV, int ADJ, int ACC, bool PML>
+__device__ __forceinline__ void elem_body(const ElemArgs<T> &A, int pbase, int ngrp, int e0, T *U, T *V, T *coef, int *eqs)
+{
+    constexpr int TP = S / SV;
+    constexpr int NTAG = PML ? 3 : 1;
+    constexpr int NDOF = PML ? 9 : 3;
     const int tid = threadIdx.x;
-    const int s = tid % S, q = (tid / S) % 27, el = tid / (27 * S);
+    const int tp = tid % TP, q = (tid / TP) % 27, el = tid / (27 * TP);
+    const int s0 = tp * SV;
     const bool active = e0 + el < ngrp;
-    const int qm[3] = {q % 3, (q / 3) % 3, q / 9};
-    const int base[3] = {q - qm[0], q - 3 * qm[1], q - 9 * qm[2]};
-    constexpr int kStride[3] = {1, 3, 9};
-    T yu[3] = {T(0), T(0), T(0)};
-    T ys[6] = {T(0), T(0), T(0), T(0), T(0), T(0)};
-    T W[3][3] = {{T(0), T(0), T(0)}, {T(0), T(0), T(0)}, {T(0), T(0), T(0)}};
+    const int p = pbase + e0 + el;
+    const size_t pq = size_t(p) * 27 + q;
+    T *Ue = U + el * 3 * 81 * S;
     T ji[9];
-    T f0 = T(0);
+    T f0 = T(0), rho = T(0);
+    // all global loads of the block are issued in this one phase; the TP
+    // threads of a point share its displacement values and coefficients
     if (active) {
-        const int e = __ldg(list + e0 + el);
-        const double *g = A.geom + (size_t(e) * 27 + q) * 10;
+        const double *g = A.el_geom + pq * 10;
 #pragma unroll
         for (int k = 0; k < 9; ++k) ji[k] = T(__ldg(g + k));
         f0 = T(__ldg(g + 9));
-        const int node = nodes[el * 27 + q];
-        const T lam = T(__ldg(A.lam + node)), mu = T(__ldg(A.mu + node));
-        const T *Ue = U + el * 3 * 27 * 9 * S;
-        // du_c/dxi_m at q along the three lines, then g_ck = sum_m du_cm DJI(m,k)
-        auto grad = [&](const T *Ut, T (&gr)[3][3]) {
-            T du[3][3];
+        if constexpr (PML) rho = T(__ldg(A.el_rho + p));
+        const int32_t *eqp = A.el_eq + pq * 9;
+        for (int i = tp; i < NTAG * 3; i += TP) {
+            const int t = i / 3, c = i % 3;
+            const int eq = __ldg(eqp + c);
+            const T *src = PML ? (t == 0 ? A.in_m : (t == 1 ? A.in_t : A.in_h)) : A.in_t;
+            T v[S];
+            if (eq >= 0) {
+                ldv<T, S>(src + size_t(eq) * S, v);
+            } else {
 #pragma unroll
-            for (int m = 0; m < 3; ++m) {
-                double d0, d1, d2;
-                gll_row(qm[m], d0, d1, d2);
-                const T *p = Ut + base[m] * 9 * S + s;
-                const int st = kStride[m] * 9 * S;
-#pragma unroll
-                for (int c = 0; c < 3; ++c)
-                    du[c][m] = fmaT(T(d2), p[2 * st + c * S], fmaT(T(d1), p[st + c * S], T(d0) * p[c * S]));
+                for (int k = 0; k < S; ++k) v[k] = T(0);
             }
+            T *dst = Ue + ((t * 27 + q) * 3 + c) * S;
 #pragma unroll
-            for (int c = 0; c < 3; ++c)
-#pragma unroll
-                for (int k = 0; k < 3; ++k)
-                    gr[c][k] = fmaT(du[c][2], ji[6 + k], fmaT(du[c][1], ji[3 + k], du[c][0] * ji[k]));
-        };
-        if (pml) {
-            double ab[10];
-            pml_coefs(A.xyz + size_t(node) * 3, ab);
-            const T rho = T(__ldg(A.rho + e));
-#pragma unroll
-            for (int t = 0; t < 3; ++t) {
-                // direction weights (F3, F2, F1) of kind e / p / w and the diagonal factor b / c / d
-                T w[3];
-                if (t == 0) { w[0] = T(ab[1] * ab[2]); w[1] = T(ab[0] * ab[2]); w[2] = T(ab[0] * ab[1]); }
-                else if (t == 1) {
-                    w[0] = T(ab[1] * ab[5] + ab[2] * ab[4]);
-                    w[1] = T(ab[0] * ab[5] + ab[2] * ab[3]);
-                    w[2] = T(ab[0] * ab[4] + ab[1] * ab[3]);
-                } else { w[0] = T(ab[4] * ab[5]); w[1] = T(ab[3] * ab[5]); w[2] = T(ab[3] * ab[4]); }
-                const T dg = T(ab[7 + t]);
-                const T sg = (ADJ && t != 1) ? T(-1) : T(1);
-                const T *Ut = Ue + t * 27 * 9 * S;
-                T gr[3][3];
-                grad(Ut, gr);
-                T G[3][3];
-#pragma unroll
-                for (int c = 0; c < 3; ++c)
-#pragma unroll
-                    for (int k = 0; k < 3; ++k) G[c][k] = w[k] * gr[c][k];
-                const T *own = Ut + q * 9 * S + s;
-                const T s0 = own[3 * S], s1 = own[4 * S], s2 = own[5 * S], s3 = own[6 * S], s4 = own[7 * S], s5 = own[8 * S];
-                if (!ADJ) {
-                    // EA upper: stress rows take the weighted strain components at q
-                    ys[0] += G[0][0];
-                    ys[1] += G[1][1];
-                    ys[2] += G[2][2];
-                    ys[3] += G[0][1] + G[1][0];
-                    ys[4] += G[0][2] + G[2][0];
-                    ys[5] += G[1][2] + G[2][1];
-                    // EA lower: displacement rows take minus the divergence of w_k (C : s)
-                    const T l2 = lam + T(2) * mu, m2 = T(2) * mu;
-                    const T sxx = l2 * s0 + lam * (s1 + s2), syy = lam * (s0 + s2) + l2 * s1, szz = lam * (s0 + s1) + l2 * s2;
-                    const T sxy = m2 * s3, sxz = m2 * s4, syz = m2 * s5;
-                    W[0][0] += w[0] * sxx; W[0][1] += w[1] * sxy; W[0][2] += w[2] * sxz;
-                    W[1][0] += w[0] * sxy; W[1][1] += w[1] * syy; W[1][2] += w[2] * syz;
-                    W[2][0] += w[0] * sxz; W[2][1] += w[1] * syz; W[2][2] += w[2] * szz;
-                } else {
-                    // transposed EA lower: stress rows take minus C : (weighted strain)
-                    const T l2 = lam + T(2) * mu, m2 = T(2) * mu;
-                    ys[0] -= sg * (l2 * G[0][0] + lam * (G[1][1] + G[2][2]));
-                    ys[1] -= sg * (lam * (G[0][0] + G[2][2]) + l2 * G[1][1]);
-                    ys[2] -= sg * (lam * (G[0][0] + G[1][1]) + l2 * G[2][2]);
-                    ys[3] -= sg * m2 * (G[0][1] + G[1][0]);
-                    ys[4] -= sg * m2 * (G[0][2] + G[2][0]);
-                    ys[5] -= sg * m2 * (G[1][2] + G[2][1]);
-                    // transposed EA upper: displacement rows take the divergence of w_k s
-                    const T ws0 = sg * w[0], ws1 = sg * w[1], ws2 = sg * w[2];
-                    W[0][0] += ws0 * s0; W[0][1] += ws1 * s3; W[0][2] += ws2 * s4;
-                    W[1][0] += ws0 * s3; W[1][1] += ws1 * s1; W[1][2] += ws2 * s5;
-                    W[2][0] += ws0 * s4; W[2][1] += ws1 * s5; W[2][2] += ws2 * s2;
-                }
-                // diagonal EM (rho * f) and EN (f, 2 f) blocks
-                const T du_ = sg * rho * dg, dn = sg * dg;
-                yu[0] += du_ * own[0];
-                yu[1] += du_ * own[S];
-                yu[2] += du_ * own[2 * S];
-                ys[0] += dn * s0;
-                ys[1] += dn * s1;
-                ys[2] += dn * s2;
-                ys[3] += T(2) * dn * s3;
-                ys[4] += T(2) * dn * s4;
-                ys[5] += T(2) * dn * s5;
-            }
-#pragma unroll
-            for (int d = 0; d < 6; ++d) ys[d] *= f0;
-#pragma unroll
-            for (int c = 0; c < 3; ++c) yu[c] *= f0;
-            if (!ADJ) {
-#pragma unroll
-                for (int c = 0; c < 3; ++c)
-#pragma unroll
-                    for (int k = 0; k < 3; ++k) W[c][k] = -W[c][k];
-            }
-        } else {
-            T gr[3][3];
-            grad(Ue + 27 * 9 * S, gr);   // K input
-            const T tr = gr[0][0] + gr[1][1] + gr[2][2];
-            const T m2 = T(2) * mu;
-            W[0][0] = fmaT(m2, gr[0][0], lam * tr);
-            W[1][1] = fmaT(m2, gr[1][1], lam * tr);
-            W[2][2] = fmaT(m2, gr[2][2], lam * tr);
-            W[0][1] = W[1][0] = mu * (gr[0][1] + gr[1][0]);
-            W[0][2] = W[2][0] = mu * (gr[0][2] + gr[2][0]);
-            W[1][2] = W[2][1] = mu * (gr[1][2] + gr[2][1]);
+            for (int k = 0; k < S; ++k) dst[k] = v[k];
         }
+        if constexpr (ACC == 1)
+            for (int d = tp; d < NDOF; d += TP) eqs[(el * 27 + q) * 9 + d] = __ldg(eqp + d);
+        const int node = __ldg(A.el_node + pq);
+        T *cf = coef + (el * 27 + q) * kCoef;
+        for (int j = tp; j < (PML ? kCoef : 2); j += TP)
+            cf[j] = T(j == 0 ? __ldg(A.lam + node) : (j == 1 ? __ldg(A.mu + node) : __ldg(A.pmlw + size_t(node) * 12 + j - 2)));
     }
-    // fluxes v_cm = w detJ sum_k DJI(m,k) W_ck for the divergence along the xi_m lines
-    {
-        T *v = V + (el * 27 + q) * 9 * S + s;
+    __syncthreads();
+
+    const int qm[3] = {q % 3, (q / 3) % 3, q / 9};
+    const int base[3] = {q - qm[0], q - 3 * qm[1], q - 9 * qm[2]};
+    constexpr int kStride[3] = {1, 3, 9};
+    T yu[3][SV], ys[6][SV];
+#pragma unroll
+    for (int v = 0; v < SV; ++v) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) yu[c][v] = T(0);
+#pragma unroll
+        for (int d = 0; d < 6; ++d) ys[d][v] = T(0);
+    }
+    // du_c/dxi_m at q along the three lines (component c of input Ut), then
+    // gr_k = sum_m du_m DJI(m,k)
+    auto grad_c = [&](const T *Ut, int c, T (&gr)[3][SV]) {
+        T du[3][SV];
+#pragma unroll
+        for (int m = 0; m < 3; ++m) {
+            double d0, d1, d2;
+            gll_row(qm[m], d0, d1, d2);
+            const T *pp = Ut + (base[m] * 3 + c) * S + s0;
+            const int st = kStride[m] * 3 * S;
+            T a0[SV], a1[SV], a2[SV];
+            ld_n<T, SV>(pp, a0);
+            ld_n<T, SV>(pp + st, a1);
+            ld_n<T, SV>(pp + 2 * st, a2);
+#pragma unroll
+            for (int v = 0; v < SV; ++v) du[m][v] = fmaT(T(d2), a2[v], fmaT(T(d1), a1[v], T(d0) * a0[v]));
+        }
+#pragma unroll
+        for (int k = 0; k < 3; ++k)
+#pragma unroll
+            for (int v = 0; v < SV; ++v) gr[k][v] = fmaT(du[2][v], ji[6 + k], fmaT(du[1][v], ji[3 + k], du[0][v] * ji[k]));
+    };
+    auto put_flux = [&](const T (&W)[3][3][SV], T sign) {
+        T *vb = V + (el * 27 + q) * 9 * S + s0;
 #pragma unroll
         for (int c = 0; c < 3; ++c)
 #pragma unroll
-            for (int m = 0; m < 3; ++m)
-                v[(c * 3 + m) * S] = active ? f0 * fmaT(ji[3 * m + 2], W[c][2], fmaT(ji[3 * m + 1], W[c][1], ji[3 * m] * W[c][0]))
-                                            : T(0);
+            for (int m = 0; m < 3; ++m) {
+                T o[SV];
+#pragma unroll
+                for (int v = 0; v < SV; ++v)
+                    o[v] = sign * f0 * fmaT(ji[3 * m + 2], W[c][2][v], fmaT(ji[3 * m + 1], W[c][1][v], ji[3 * m] * W[c][0][v]));
+                st_n<T, SV>(vb + (c * 3 + m) * S, o);
+            }
+    };
+    if (active) {
+        const T *cf = coef + (el * 27 + q) * kCoef;
+        const T lam = cf[0], mu = cf[1];
+        const T l2 = lam + T(2) * mu, m2 = T(2) * mu;
+        if constexpr (PML) {
+            // pass 1: the stresses of the point give the fluxes of the divergence
+            // and the diagonal EN terms
+            {
+                T W[3][3][SV];
+#pragma unroll
+                for (int c = 0; c < 3; ++c)
+#pragma unroll
+                    for (int k = 0; k < 3; ++k)
+#pragma unroll
+                        for (int v = 0; v < SV; ++v) W[c][k][v] = T(0);
+                const int32_t *eqp = A.el_eq + pq * 9;
+#pragma unroll
+                for (int t = 0; t < 3; ++t) {
+                    const T *src = t == 0 ? A.in_m : (t == 1 ? A.in_t : A.in_h);
+                    T sv[6][SV];
+#pragma unroll
+                    for (int d = 0; d < 6; ++d) {
+                        const int eq = __ldg(eqp + 3 + d);
+                        if (eq >= 0) {
+                            ldg_n<T, SV>(src + size_t(eq) * S + s0, sv[d]);
+                        } else {
+#pragma unroll
+                            for (int v = 0; v < SV; ++v) sv[d][v] = T(0);
+                        }
+                    }
+                    const T w0 = cf[2 + 3 * t], w1 = cf[3 + 3 * t], w2 = cf[4 + 3 * t];
+                    const T sgn = (ADJ && t != 1) ? T(-1) : T(1);
+                    const T dn = sgn * cf[11 + t];
+#pragma unroll
+                    for (int v = 0; v < SV; ++v) {
+                        const T s_0 = sv[0][v], s_1 = sv[1][v], s_2 = sv[2][v], s_3 = sv[3][v], s_4 = sv[4][v], s_5 = sv[5][v];
+                        if (!ADJ) {
+                            // EA lower: displacement rows take minus the divergence of w_k (C : s)
+                            const T sxx = l2 * s_0 + lam * (s_1 + s_2);
+                            const T syy = lam * (s_0 + s_2) + l2 * s_1;
+                            const T szz = lam * (s_0 + s_1) + l2 * s_2;
+                            const T sxy = m2 * s_3, sxz = m2 * s_4, syz = m2 * s_5;
+                            W[0][0][v] = fmaT(w0, sxx, W[0][0][v]); W[0][1][v] = fmaT(w1, sxy, W[0][1][v]); W[0][2][v] = fmaT(w2, sxz, W[0][2][v]);
+                            W[1][0][v] = fmaT(w0, sxy, W[1][0][v]); W[1][1][v] = fmaT(w1, syy, W[1][1][v]); W[1][2][v] = fmaT(w2, syz, W[1][2][v]);
+                            W[2][0][v] = fmaT(w0, sxz, W[2][0][v]); W[2][1][v] = fmaT(w1, syz, W[2][1][v]); W[2][2][v] = fmaT(w2, szz, W[2][2][v]);
+                        } else {
+                            // transposed EA upper: displacement rows take the divergence of w_k s
+                            const T ws0 = sgn * w0, ws1 = sgn * w1, ws2 = sgn * w2;
+                            W[0][0][v] = fmaT(ws0, s_0, W[0][0][v]); W[0][1][v] = fmaT(ws1, s_3, W[0][1][v]); W[0][2][v] = fmaT(ws2, s_4, W[0][2][v]);
+                            W[1][0][v] = fmaT(ws0, s_3, W[1][0][v]); W[1][1][v] = fmaT(ws1, s_1, W[1][1][v]); W[1][2][v] = fmaT(ws2, s_5, W[1][2][v]);
+                            W[2][0][v] = fmaT(ws0, s_4, W[2][0][v]); W[2][1][v] = fmaT(ws1, s_5, W[2][1][v]); W[2][2][v] = fmaT(ws2, s_2, W[2][2][v]);
+                        }
+                        // diagonal EN (f, 2 f) blocks
+                        ys[0][v] = fmaT(dn, s_0, ys[0][v]);
+                        ys[1][v] = fmaT(dn, s_1, ys[1][v]);
+                        ys[2][v] = fmaT(dn, s_2, ys[2][v]);
+                        ys[3][v] = fmaT(T(2) * dn, s_3, ys[3][v]);
+                        ys[4][v] = fmaT(T(2) * dn, s_4, ys[4][v]);
+                        ys[5][v] = fmaT(T(2) * dn, s_5, ys[5][v]);
+                    }
+                }
+                put_flux(W, ADJ ? T(1) : T(-1));
+            }
+            // pass 2: displacement gradients give the stress rows, and the
+            // diagonal EM terms
+#pragma unroll
+            for (int t = 0; t < 3; ++t) {
+                const T *Ut = Ue + t * 81 * S;
+                const T w[3] = {cf[2 + 3 * t], cf[3 + 3 * t], cf[4 + 3 * t]};
+                const T sgn = (ADJ && t != 1) ? T(-1) : T(1);
+                const T dgu = sgn * rho * cf[11 + t];
+#pragma unroll
+                for (int c = 0; c < 3; ++c) {
+                    T gr[3][SV];
+                    grad_c(Ut, c, gr);
+                    T own[SV];
+                    ld_n<T, SV>(Ut + (q * 3 + c) * S + s0, own);
+#pragma unroll
+                    for (int v = 0; v < SV; ++v) {
+                        yu[c][v] = fmaT(dgu, own[v], yu[c][v]);
+#pragma unroll
+                        for (int k = 0; k < 3; ++k) {
+                            const T G = w[k] * gr[k][v];   // weighted strain component (c, k)
+                            if (!ADJ) {
+                                // EA upper: stress rows take the weighted strain components
+                                if (k == c) ys[c][v] += G;
+                                else ys[2 + c + k][v] += G;
+                            } else {
+                                // transposed EA lower: stress rows take minus C : (weighted strain)
+                                if (k == c) {
+#pragma unroll
+                                    for (int d = 0; d < 3; ++d) ys[d][v] -= sgn * (d == c ? l2 : lam) * G;
+                                } else {
+                                    ys[2 + c + k][v] -= sgn * m2 * G;
+                                }
+                            }
+                        }
+                    }
+                }
+            }
+#pragma unroll
+            for (int v = 0; v < SV; ++v) {
+#pragma unroll
+                for (int d = 0; d < 6; ++d) ys[d][v] *= f0;
+#pragma unroll
+                for (int c = 0; c < 3; ++c) yu[c][v] *= f0;
+            }
+        } else {
+            // regular domain: stress of the K input's gradient gives the fluxes
+            T gr[3][3][SV];
+#pragma unroll
+            for (int c = 0; c < 3; ++c) grad_c(Ue, c, gr[c]);
+            T W[3][3][SV];
+#pragma unroll
+            for (int v = 0; v < SV; ++v) {
+                const T tr = gr[0][0][v] + gr[1][1][v] + gr[2][2][v];
+                W[0][0][v] = fmaT(m2, gr[0][0][v], lam * tr);
+                W[1][1][v] = fmaT(m2, gr[1][1][v], lam * tr);
+                W[2][2][v] = fmaT(m2, gr[2][2][v], lam * tr);
+                W[0][1][v] = W[1][0][v] = mu * (gr[0][1][v] + gr[1][0][v]);
+                W[0][2][v] = W[2][0][v] = mu * (gr[0][2][v] + gr[2][0][v]);
+                W[1][2][v] = W[2][1][v] = mu * (gr[1][2][v] + gr[2][1][v]);
+            }
+            put_flux(W, T(1));
+        }
     }
     __syncthreads();
     if (!active) return;
@@ -298,44 +406,90 @@ __global__ void __launch_bounds__(216, 2) k_elem(const ElemArgs<T> A)
     for (int m = 0; m < 3; ++m) {
         double d0, d1, d2;
         gll_col(qm[m], d0, d1, d2);
-        const T *p = V + (el * 27 + base[m]) * 9 * S + s;
+        const T *pp = V + (el * 27 + base[m]) * 9 * S + s0;
         const int st = kStride[m] * 9 * S;
 #pragma unroll
-        for (int c = 0; c < 3; ++c)
-            yu[c] += fmaT(T(d2), p[2 * st + (c * 3 + m) * S], fmaT(T(d1), p[st + (c * 3 + m) * S], T(d0) * p[(c * 3 + m) * S]));
+        for (int c = 0; c < 3; ++c) {
+            T a0[SV], a1[SV], a2[SV];
+            ld_n<T, SV>(pp + (c * 3 + m) * S, a0);
+            ld_n<T, SV>(pp + st + (c * 3 + m) * S, a1);
+            ld_n<T, SV>(pp + 2 * st + (c * 3 + m) * S, a2);
+#pragma unroll
+            for (int v = 0; v < SV; ++v) yu[c][v] += fmaT(T(d2), a2[v], fmaT(T(d1), a1[v], T(d0) * a0[v]));
+        }
     }
-    const int e = __ldg(list + e0 + el);
     if constexpr (ACC == 0) {
-        T *o = A.slots + (size_t(e) * 27 + q) * 9 * S + s;
+        T *o = A.slots + pq * 9 * S + s0;
 #pragma unroll
-        for (int c = 0; c < 3; ++c) o[c * S] = yu[c];
-        if (pml) {
+        for (int c = 0; c < 3; ++c) st_n<T, SV>(o + c * S, yu[c]);
+        if constexpr (PML) {
 #pragma unroll
-            for (int d = 0; d < 6; ++d) o[(3 + d) * S] = ys[d];
+            for (int d = 0; d < 6; ++d) st_n<T, SV>(o + (3 + d) * S, ys[d]);
         }
     } else {
-        const int node = nodes[el * 27 + q];
-        const int32_t *idn = A.id + size_t(node) * 9;
+        const int *eqo = eqs + (el * 27 + q) * 9;
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
-            const int eq = __ldg(idn + c);
-            if (eq >= 0) atomicAdd(A.acc + size_t(eq) * S + s, yu[c]);
+            const int eq = eqo[c];
+            if (eq >= 0) red_n<T, SV>(A.acc + size_t(eq) * S + s0, yu[c]);
         }
-        if (pml) {
+        if constexpr (PML) {
 #pragma unroll
             for (int d = 0; d < 6; ++d) {
-                const int eq = __ldg(idn + 3 + d);
-                if (eq >= 0) atomicAdd(A.acc + size_t(eq) * S + s, ys[d]);
+                const int eq = eqo[3 + d];
+                if (eq >= 0) red_n<T, SV>(A.acc + size_t(eq) * S + s0, ys[d]);
             }
         }
     }
+}
+
+// One thread per (element, GLL point, SV shots); the first nb_pml blocks take
+// PML elements, the rest regular-domain elements.  ACC = 0: write the
+// element's slot; ACC = 1: add into the row accumulator.
+template <typename T, int S, int SV, int ADJ, int ACC>
+__global__ void __launch_bounds__(216, 2) k_elem(const ElemArgs<T> A)
+{
+    constexpr int EPB = elems_per_block<S, SV>();
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T *U = reinterpret_cast<T *>(smem_raw);
+    T *V = U + EPB * 3 * 81 * S;
+    T *coef = V + EPB * 243 * S;
+    int *eqs = reinterpret_cast<int *>(coef + EPB * 27 * kCoef);
+    if (int(blockIdx.x) < A.nb_pml)
+        elem_body<T, S, SV, ADJ, ACC, true>(A, 0, A.nel_pml, int(blockIdx.x) * EPB, U, V, coef, eqs);
+    else
+        elem_body<T, S, SV, ADJ, ACC, false>(A, A.nel_pml, A.nel_rd, (int(blockIdx.x) - A.nb_pml) * EPB, U, V, coef, eqs);
+}
+
+// PML weights of every node: F3, F2, F1 (directions x, y, z) of the kinds
+// e, p, w and the diagonal factors b, c, d.
+__global__ void k_pml_weights(int nj, const double *__restrict__ xyz, double *__restrict__ out)
+{
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= nj) return;
+    double ab[10];
+    pml_coefs(xyz + size_t(j) * 3, ab);
+    double *o = out + size_t(j) * 12;
+    o[0] = ab[1] * ab[2]; o[1] = ab[0] * ab[2]; o[2] = ab[0] * ab[1];
+    o[3] = ab[1] * ab[5] + ab[2] * ab[4]; o[4] = ab[0] * ab[5] + ab[2] * ab[3]; o[5] = ab[0] * ab[4] + ab[1] * ab[3];
+    o[6] = ab[4] * ab[5]; o[7] = ab[3] * ab[5]; o[8] = ab[3] * ab[4];
+    o[9] = ab[7]; o[10] = ab[8]; o[11] = ab[9];
+}
+
+// Element geometry in processing order.
+__global__ void k_gather_geom(int np, const int32_t *__restrict__ order, const double *__restrict__ geom, double *__restrict__ out)
+{
+    const int64_t t = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+    if (t >= int64_t(np) * 270) return;
+    const int p = int(t / 270), k = int(t % 270);
+    out[t] = geom[size_t(order[p]) * 270 + k];
 }
 
 template <typename T>
 struct NodeArgs {
     const int32_t *row_info;   // [neq] node << 4 | dof
     const int32_t *nptr;       // [nj + 1]
-    const uint32_t *nslot;     // element * 27 + point, | kRdSlot for regular-domain elements
+    const uint32_t *nslot;     // processing index * 27 + point, | kRdSlot for regular-domain elements
     const T *slots;
     T *acc;
     const double *im;
@@ -389,32 +543,37 @@ int elem_prepare(hrn_ctx *c)
                                              {2, 1, 1}, {1, 2, 1}, {0, 1, 1}, {1, 0, 1}, {1, 1, 2}, {1, 1, 1}};
     unsigned char node_at[27];
     for (int i = 0; i < 27; ++i) node_at[9 * ijk[i][2] + 3 * ijk[i][1] + ijk[i][0]] = (unsigned char)i;
-    HRN_CUDA(c, cudaMemcpyToSymbol(e_node_at, node_at, sizeof(node_at)));
     HRN_CUDA(c, cudaMemcpyToSymbol(e_pml, c->h_pml.data(), 24 * sizeof(double)));
-    std::vector<int32_t> pml, rd;
-    for (int e = 0; e < c->nel; ++e) {
-        if (c->h_mtel[e] == 2) pml.push_back(e);
-        else if (c->h_mtel[e] == 1) rd.push_back(e);
-    }
-    c->nel_pml_e = int(pml.size());
-    c->nel_rd_e = int(rd.size());
-    // slots of each node, ascending element order
+    // processing order: PML elements, then regular-domain elements
+    std::vector<int32_t> order;
+    for (int e = 0; e < c->nel; ++e)
+        if (c->h_mtel[e] == 2) order.push_back(e);
+    c->nel_pml_e = int(order.size());
+    for (int e = 0; e < c->nel; ++e)
+        if (c->h_mtel[e] == 1) order.push_back(e);
+    c->nel_rd_e = int(order.size()) - c->nel_pml_e;
+    const int np = int(order.size());
+    if (int64_t(np) * 27 >= int64_t(kRdSlot)) return set_error(c, HRN_EARG, "too many elements for the slot index");
+    std::vector<int32_t> el_eq(size_t(np) * 243), el_node(size_t(np) * 27);
+    std::vector<double> el_rho(std::max(np, 1));
     std::vector<int32_t> nptr(size_t(c->nj) + 1, 0);
-    for (int e = 0; e < c->nel; ++e) {
-        if (c->h_mtel[e] != 1 && c->h_mtel[e] != 2) continue;
-        for (int q = 0; q < 27; ++q) nptr[c->h_inod[size_t(e) * 27 + node_at[q]] + 1]++;
+    for (int p = 0; p < np; ++p) {
+        const int e = order[p];
+        el_rho[p] = c->h_rho[e];
+        for (int q = 0; q < 27; ++q) {
+            const int node = c->h_inod[size_t(e) * 27 + node_at[q]];
+            el_node[size_t(p) * 27 + q] = node;
+            for (int d = 0; d < 9; ++d) el_eq[(size_t(p) * 27 + q) * 9 + d] = c->h_id[size_t(node) * 9 + d];
+            nptr[node + 1]++;
+        }
     }
+    // slots of each node, ascending processing order
     for (int j = 0; j < c->nj; ++j) nptr[j + 1] += nptr[j];
     std::vector<uint32_t> ns(static_cast<size_t>(nptr[c->nj]));
     std::vector<int32_t> pos(nptr.begin(), nptr.end() - 1);
-    for (int e = 0; e < c->nel; ++e) {
-        if (c->h_mtel[e] != 1 && c->h_mtel[e] != 2) continue;
-        for (int q = 0; q < 27; ++q) {
-            const int node = c->h_inod[size_t(e) * 27 + node_at[q]];
-            ns[pos[node]++] = uint32_t(e * 27 + q) | (c->h_mtel[e] == 1 ? kRdSlot : 0u);
-        }
-    }
-    if (int64_t(c->nel) * 27 >= int64_t(kRdSlot)) return set_error(c, HRN_EARG, "too many elements for the slot index");
+    for (int p = 0; p < np; ++p)
+        for (int q = 0; q < 27; ++q)
+            ns[pos[el_node[size_t(p) * 27 + q]]++] = uint32_t(p * 27 + q) | (p >= c->nel_pml_e ? kRdSlot : 0u);
     std::vector<int32_t> info(size_t(c->neq), -1);
     for (int j = 0; j < c->nj; ++j)
         for (int d = 0; d < 9; ++d) {
@@ -423,16 +582,32 @@ int elem_prepare(hrn_ctx *c)
         }
     for (int32_t v : info)
         if (v < 0) return set_error(c, HRN_EMESH, "an equation has no (node, DOF) in ID");
-    HRN_CUDA(c, c->d_el_pml.alloc(std::max<size_t>(pml.size(), 1) * 4));
-    HRN_CUDA(c, c->d_el_rde.alloc(std::max<size_t>(rd.size(), 1) * 4));
+    const size_t npa = std::max<size_t>(np, 1);
+    HRN_CUDA(c, c->d_el_order.alloc(npa * 4));
+    HRN_CUDA(c, c->d_el_eq.alloc(npa * 243 * 4));
+    HRN_CUDA(c, c->d_el_node.alloc(npa * 27 * 4));
+    HRN_CUDA(c, c->d_el_geom.alloc(npa * 270 * 8));
+    HRN_CUDA(c, c->d_el_rho.alloc(npa * 8));
     HRN_CUDA(c, c->d_nslot_ptr.alloc(nptr.size() * 4));
     HRN_CUDA(c, c->d_nslot.alloc(std::max<size_t>(ns.size(), 1) * 4));
     HRN_CUDA(c, c->d_row_info.alloc(info.size() * 4));
-    if (!pml.empty()) HRN_CUDA(c, cudaMemcpy(c->d_el_pml.p, pml.data(), pml.size() * 4, cudaMemcpyHostToDevice));
-    if (!rd.empty()) HRN_CUDA(c, cudaMemcpy(c->d_el_rde.p, rd.data(), rd.size() * 4, cudaMemcpyHostToDevice));
+    HRN_CUDA(c, c->d_pmlw.alloc(size_t(c->nj) * 12 * 8));
+    if (np > 0) {
+        HRN_CUDA(c, cudaMemcpy(c->d_el_order.p, order.data(), size_t(np) * 4, cudaMemcpyHostToDevice));
+        HRN_CUDA(c, cudaMemcpy(c->d_el_eq.p, el_eq.data(), el_eq.size() * 4, cudaMemcpyHostToDevice));
+        HRN_CUDA(c, cudaMemcpy(c->d_el_node.p, el_node.data(), el_node.size() * 4, cudaMemcpyHostToDevice));
+        HRN_CUDA(c, cudaMemcpy(c->d_el_rho.p, el_rho.data(), size_t(np) * 8, cudaMemcpyHostToDevice));
+        k_gather_geom<<<int((int64_t(np) * 270 + 255) / 256), 256, 0, c->stream>>>(np, c->d_el_order.as<int32_t>(),
+                                                                                   c->d_asm_geom.as<double>(), c->d_el_geom.as<double>());
+        ++c->launches;
+    }
     HRN_CUDA(c, cudaMemcpy(c->d_nslot_ptr.p, nptr.data(), nptr.size() * 4, cudaMemcpyHostToDevice));
     if (!ns.empty()) HRN_CUDA(c, cudaMemcpy(c->d_nslot.p, ns.data(), ns.size() * 4, cudaMemcpyHostToDevice));
     HRN_CUDA(c, cudaMemcpy(c->d_row_info.p, info.data(), info.size() * 4, cudaMemcpyHostToDevice));
+    k_pml_weights<<<(c->nj + 255) / 256, 256, 0, c->stream>>>(c->nj, c->d_xyz.as<double>(), c->d_pmlw.as<double>());
+    ++c->launches;
+    HRN_CUDA(c, cudaGetLastError());
+    HRN_CUDA(c, cudaStreamSynchronize(c->stream));
     c->have_elem = true;
     return 0;
 }
@@ -441,7 +616,7 @@ int elem_prepare(hrn_ctx *c)
 static int elem_buffers(hrn_ctx *c)
 {
     const size_t S = size_t(c->nshot), eb = c->elem_bytes();
-    HRN_CUDA(c, c->d_eslots.alloc(size_t(c->nel) * 27 * 9 * S * eb));
+    HRN_CUDA(c, c->d_eslots.alloc(std::max<size_t>(size_t(c->nel_pml_e + c->nel_rd_e), 1) * 27 * 9 * S * eb));
     const size_t accb = size_t(c->neq) * S * eb;
     if (c->d_eacc.bytes != accb) {
         HRN_CUDA(c, c->d_eacc.alloc(accb));
@@ -450,50 +625,65 @@ static int elem_buffers(hrn_ctx *c)
     return 0;
 }
 
-template <typename T, int S, int ADJ, int ACC>
+template <typename T, int S, int SV, int ADJ, int ACC>
 static void launch_elem(const ElemArgs<T> &A, int blocks, cudaStream_t st)
 {
     static bool attr_set = false;
-    constexpr size_t smem = elem_smem_bytes<T, S>();
+    constexpr size_t smem = elem_smem_bytes<T, S, SV>();
     if (!attr_set) {
-        cudaFuncSetAttribute(k_elem<T, S, ADJ, ACC>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+        cudaFuncSetAttribute(k_elem<T, S, SV, ADJ, ACC>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
         attr_set = true;
     }
-    k_elem<T, S, ADJ, ACC><<<blocks, elems_per_block<S>() * 27 * S, smem, st>>>(A);
+    k_elem<T, S, SV, ADJ, ACC><<<blocks, elems_per_block<S, SV>() * 27 * (S / SV), smem, st>>>(A);
+}
+
+template <typename T, int S, int SV>
+static void launch_elem_any(const ElemArgs<T> &A, int blocks, int adj, int acc, cudaStream_t st)
+{
+    if (adj) {
+        if (acc) launch_elem<T, S, SV, 1, 1>(A, blocks, st);
+        else launch_elem<T, S, SV, 1, 0>(A, blocks, st);
+    } else {
+        if (acc) launch_elem<T, S, SV, 0, 1>(A, blocks, st);
+        else launch_elem<T, S, SV, 0, 0>(A, blocks, st);
+    }
 }
 
 template <typename T, int S>
-static int elem_stage_t(hrn_ctx *c, const StageArgs<T> &a, int stage, int adj, int acc)
+static int elem_stage_t(hrn_ctx *c, const StageArgs<T> &a, int stage, int adj, int acc, int sv)
 {
-    constexpr int EPB = elems_per_block<S>();
     ElemArgs<T> A{};
-    A.el_pml = c->d_el_pml.as<int32_t>();
-    A.el_rd = c->d_el_rde.as<int32_t>();
     A.nel_pml = c->nel_pml_e;
     A.nel_rd = c->nel_rd_e;
-    A.nb_pml = (c->nel_pml_e + EPB - 1) / EPB;
-    A.inod = c->d_inod.as<int32_t>();
-    A.id = c->d_id.as<int32_t>();
-    A.xyz = c->d_xyz.as<double>();
-    A.geom = c->d_asm_geom.as<double>();
+    A.el_eq = c->d_el_eq.as<int32_t>();
+    A.el_node = c->d_el_node.as<int32_t>();
+    A.el_geom = c->d_el_geom.as<double>();
+    A.el_rho = c->d_el_rho.as<double>();
     A.lam = c->d_lam.as<double>();
     A.mu = c->d_mu.as<double>();
-    A.rho = c->d_rho.as<double>();
+    A.pmlw = c->d_pmlw.as<double>();
     if (stage == 1) { A.in_m = a.x3; A.in_t = a.x2; A.in_h = a.x1; }
     else { A.in_m = a.in_m; A.in_t = a.in_t; A.in_h = a.in_h; }
     A.slots = c->d_eslots.as<T>();
     A.acc = c->d_eacc.as<T>();
-    const int blocks = A.nb_pml + (c->nel_rd_e + EPB - 1) / EPB;
-    if (blocks > 0) {
-        if (adj) {
-            if (acc) launch_elem<T, S, 1, 1>(A, blocks, c->stream);
-            else launch_elem<T, S, 1, 0>(A, blocks, c->stream);
-        } else {
-            if (acc) launch_elem<T, S, 0, 1>(A, blocks, c->stream);
-            else launch_elem<T, S, 0, 0>(A, blocks, c->stream);
+    auto go = [&](auto svc) {
+        constexpr int SV = decltype(svc)::value;
+        constexpr int EPB = elems_per_block<S, SV>();
+        A.nb_pml = (c->nel_pml_e + EPB - 1) / EPB;
+        const int blocks = A.nb_pml + (c->nel_rd_e + EPB - 1) / EPB;
+        if (blocks > 0) {
+            launch_elem_any<T, S, SV>(A, blocks, adj, acc, c->stream);
+            ++c->launches;
         }
-        ++c->launches;
+    };
+    bool done = false;
+    if constexpr (S % 4 == 0 && sizeof(T) == 4) {
+        if (sv == 4) { go(std::integral_constant<int, 4>{}); done = true; }
     }
+    if constexpr (S % 2 == 0) {
+        if (!done && sv == 2) { go(std::integral_constant<int, 2>{}); done = true; }
+    }
+    if (!done) go(std::integral_constant<int, 1>{});
     NodeArgs<T> na{c->d_row_info.as<int32_t>(), c->d_nslot_ptr.as<int32_t>(), c->d_nslot.as<uint32_t>(),
                    c->d_eslots.as<T>(), c->d_eacc.as<T>(), c->d_im.as<double>()};
     const int th = 256, nb = (c->neq + th - 1) / th;
@@ -512,22 +702,32 @@ static int elem_stage_t(hrn_ctx *c, const StageArgs<T> &a, int stage, int adj, i
 
 #define HRN_ELEM_DISPATCH(T)                                                       \
     switch (c->nshot) {                                                            \
-    case 1: return elem_stage_t<T, 1>(c, *static_cast<const StageArgs<T> *>(args), stage, adj, acc); \
-    case 2: return elem_stage_t<T, 2>(c, *static_cast<const StageArgs<T> *>(args), stage, adj, acc); \
-    case 3: return elem_stage_t<T, 3>(c, *static_cast<const StageArgs<T> *>(args), stage, adj, acc); \
-    case 4: return elem_stage_t<T, 4>(c, *static_cast<const StageArgs<T> *>(args), stage, adj, acc); \
-    case 5: return elem_stage_t<T, 5>(c, *static_cast<const StageArgs<T> *>(args), stage, adj, acc); \
-    case 6: return elem_stage_t<T, 6>(c, *static_cast<const StageArgs<T> *>(args), stage, adj, acc); \
-    case 7: return elem_stage_t<T, 7>(c, *static_cast<const StageArgs<T> *>(args), stage, adj, acc); \
-    default: return elem_stage_t<T, 8>(c, *static_cast<const StageArgs<T> *>(args), stage, adj, acc); \
+    case 1: return elem_stage_t<T, 1>(c, *static_cast<const StageArgs<T> *>(args), stage, adj, acc, sv); \
+    case 2: return elem_stage_t<T, 2>(c, *static_cast<const StageArgs<T> *>(args), stage, adj, acc, sv); \
+    case 3: return elem_stage_t<T, 3>(c, *static_cast<const StageArgs<T> *>(args), stage, adj, acc, sv); \
+    case 4: return elem_stage_t<T, 4>(c, *static_cast<const StageArgs<T> *>(args), stage, adj, acc, sv); \
+    case 5: return elem_stage_t<T, 5>(c, *static_cast<const StageArgs<T> *>(args), stage, adj, acc, sv); \
+    case 6: return elem_stage_t<T, 6>(c, *static_cast<const StageArgs<T> *>(args), stage, adj, acc, sv); \
+    case 7: return elem_stage_t<T, 7>(c, *static_cast<const StageArgs<T> *>(args), stage, adj, acc, sv); \
+    default: return elem_stage_t<T, 8>(c, *static_cast<const StageArgs<T> *>(args), stage, adj, acc, sv); \
     }
 
 // One matrix-free RK4 stage (element kernel + node kernel) on the stage
 // arguments of the CSR kernels; args points to a StageArgs of the context's precision.
-int elem_stage(hrn_ctx *c, const void *args, int stage, int adj, int acc)
+int elem_stage(hrn_ctx *c, const void *args, int stage, int adj, int acc, int sv)
 {
     if (c->precision == HRN_FP64) { HRN_ELEM_DISPATCH(double) }
     HRN_ELEM_DISPATCH(float)
+}
+
+// Variants 90-95: element slots (even) or atomic row sums (odd) with 1, 2 or 4
+// shots per thread; 2 needs an even shot count, 4 a multiple of 4 in FP32.
+bool elem_variant_valid(const hrn_ctx *c, int v)
+{
+    if (v < 90 || v > 95) return false;
+    const int sv = 1 << ((v - 90) / 2);
+    if (c->nshot % sv != 0) return false;
+    return sv < 4 || c->precision == HRN_FP32;
 }
 
 int elem_ready(hrn_ctx *c)

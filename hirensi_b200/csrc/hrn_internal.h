@@ -93,10 +93,15 @@ struct hrn_ctx {
     bool op_from_mesh = false;    // the operator was assembled from the current mesh and material
     bool have_elem = false;       // element lists, node slot lists and the row map are built
     int nel_pml_e = 0, nel_rd_e = 0;
-    hrn::DevBuf d_el_pml, d_el_rde;   // element ids of the PML and of the regular domain
-    hrn::DevBuf d_nslot_ptr, d_nslot; // [nj + 1], per node: element * 27 + point (top bit: RD element)
+    hrn::DevBuf d_el_order;       // element ids in processing order: PML, then regular domain
+    hrn::DevBuf d_el_eq;          // [P][27][9] equations of each point's DOF (-1 fixed)
+    hrn::DevBuf d_el_node;        // [P][27] node of each point
+    hrn::DevBuf d_el_geom;        // [P][27][10] DJI and w*detJ (FP64)
+    hrn::DevBuf d_el_rho;         // [P] density
+    hrn::DevBuf d_nslot_ptr, d_nslot; // [nj + 1], per node: processing index * 27 + point (top bit: RD element)
     hrn::DevBuf d_row_info;       // [neq] node << 4 | DOF
-    hrn::DevBuf d_eslots;         // [nel * 27][9][S] element contributions (T)
+    hrn::DevBuf d_pmlw;           // [nj][12] PML direction weights of kinds e, p, w and b, c, d (FP64)
+    hrn::DevBuf d_eslots;         // [P * 27][9][S] element contributions (T)
     hrn::DevBuf d_eacc;           // [neq][S] row accumulator of the atomic variant (T), kept zero between stages
 
     // ---- history
@@ -169,7 +174,8 @@ int finalize_pattern_from_keys(hrn_ctx *c, const std::vector<uint64_t> &keys);
 int vec_reduce(hrn_ctx *c, int kind, int n, const double *x, const double *y, double *out);
 int elem_prepare(hrn_ctx *c);
 int elem_ready(hrn_ctx *c);
-int elem_stage(hrn_ctx *c, const void *stage_args, int stage, int adj, int acc);
+int elem_stage(hrn_ctx *c, const void *stage_args, int stage, int adj, int acc, int shots_per_thread);
+bool elem_variant_valid(const hrn_ctx *c, int variant);
 int vec_axpby(hrn_ctx *c, int n, double a, const double *x, double b, const double *y, double *z);
 int set_error(hrn_ctx *c, int code, const std::string &msg);
 int cuda_error(hrn_ctx *c, cudaError_t e, const char *what);

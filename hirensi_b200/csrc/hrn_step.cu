@@ -547,8 +547,9 @@ struct TileArgs {
 // tiled with bulk-copied matrix slabs (2); encoded lanes * 10 + mat + tiled,
 // chosen per operator by timing.
 constexpr int kVariants[10] = {40, 80, 160, 41, 81, 161, 42, 43, 82, 83};
-// 90 / 91: matrix-free element kernels with element slots / atomic row sums
-inline bool is_elem_variant(int v) { return v == 90 || v == 91; }
+// 90-95: matrix-free element kernels, element slots (even) or atomic row sums
+// (odd), with 1 (90, 91), 2 (92, 93) or 4 (94, 95) shots per thread
+inline bool is_elem_variant(int v) { return v >= 90 && v <= 95; }
 
 template <typename T, int S, int STAGE, int G, int MAT>
 static void launch_tile(const StageArgs<T> &a, const TileArgs &ta, cudaStream_t st)
@@ -777,7 +778,7 @@ static void launch_step(hrn_ctx *c, StageArgs<T> a, T *X, T *Y, StageTimer *tm, 
         a.in_t = in; a.in_m = in + vn; a.in_h = in + 2 * vn;
         a.out_t = out; a.out_m = out + vn; a.out_h = out + 2 * vn;
         if (is_elem_variant(lanes)) {
-            elem_stage(c, &a, st, adj, lanes - 90);
+            elem_stage(c, &a, st, adj, (lanes - 90) % 2, 1 << ((lanes - 90) / 2));
         } else {
             switch (st) {
             case 1: launch_stage<T, S, 1>(a, lanes, c->stream, ta); break;
@@ -814,8 +815,8 @@ static int autotune_lanes(hrn_ctx *c, StageArgs<T> a, T *X, T *Y, const TileArgs
     std::vector<int> cand(kVariants, kVariants + 10);
     if (c->op_from_mesh) {
         if (int rc = elem_ready(c)) return rc;
-        cand.push_back(90);
-        cand.push_back(91);
+        for (int v = 90; v <= 95; ++v)
+            if (elem_variant_valid(c, v)) cand.push_back(v);
     }
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
@@ -884,6 +885,7 @@ static int forward_t(hrn_ctx *c)
         c->lanes_f = r;
         HRN_CUDA(c, cudaMemsetAsync(X0, 0, 3 * vn * sizeof(T), c->stream));
     } else if (is_elem_variant(c->lanes_f)) {
+        if (!elem_variant_valid(c, c->lanes_f)) return set_error(c, HRN_EARG, "matrix-free variant not available for this shot count and precision");
         if (int rc = elem_ready(c)) return rc;
     }
     StageTimer tm(c);
@@ -948,6 +950,7 @@ static int adjoint_t(hrn_ctx *c, int lambda_2mu, int keep_p)
         c->lanes_a = r;
         HRN_CUDA(c, cudaMemsetAsync(X0, 0, 3 * vn * sizeof(T), c->stream));
     } else if (is_elem_variant(c->lanes_a)) {
+        if (!elem_variant_valid(c, c->lanes_a)) return set_error(c, HRN_EARG, "matrix-free variant not available for this shot count and precision");
         if (int rc = elem_ready(c)) return rc;
     }
     StageTimer tm(c);

@@ -1,9 +1,10 @@
 """Matrix-free stage variants against the FP64 oracle, with the operator assembled
 on the device from the mesh.
 
-Variant 90 writes each element's contribution to a slot and sums the slots of a
-row in ascending element order (reproducible run to run); variant 91 adds the
-contributions atomically.  Tolerances as in the CSR parity tests: FP64 1e-10
+Even variants (90, 92, 94) write each element's contribution to a slot and sum
+the slots of a row in ascending element order (reproducible run to run); odd
+variants (91, 93, 95) add the contributions atomically.  90/91 take one shot per
+thread, 92/93 two, 94/95 four (FP32 only).  Tolerances as in the CSR parity tests: FP64 1e-10
 relative L2 for histories, adjoint histories and gradients; FP32 1e-4 for
 histories and 1e-3 for gradients.
 """
@@ -44,8 +45,7 @@ def _oracle_adjoint(p, om, S, hist, dis):
     return padj, gl, gm
 
 
-@pytest.mark.parametrize("nshot", [1, 3])
-@pytest.mark.parametrize("variant", [90, 91])
+@pytest.mark.parametrize("variant,nshot", [(90, 1), (91, 1), (90, 3), (91, 3), (92, 2), (93, 4)])
 def test_matrix_free_fp64_matches_oracle(gpu_lib, variant, nshot):
     p = tiny(nshot=nshot, nstep=150)
     _, _, hist_t = oracle_forward(p, p["lam_t"], p["mu_t"])
@@ -67,9 +67,9 @@ def test_matrix_free_fp64_matches_oracle(gpu_lib, variant, nshot):
         assert rel_l2(gm, gm_ref) < TOL64
 
 
-@pytest.mark.parametrize("variant", [90, 91])
+@pytest.mark.parametrize("variant", [90, 91, 92, 93, 94, 95])
 def test_matrix_free_fp32_within_bars(gpu_lib, variant):
-    p = tiny(nshot=2, nstep=150)
+    p = tiny(nshot=4, nstep=150)
     _, _, hist_t = oracle_forward(p, p["lam_t"], p["mu_t"])
     om, S, hist = oracle_forward(p, p["lam"], p["mu"])
     dis = np.stack([traces_from_history(p, h) for h in hist_t])
@@ -77,7 +77,7 @@ def test_matrix_free_fp32_within_bars(gpu_lib, variant):
     with _solver(p, "fp32") as s:
         s.set_variant(variant, variant)
         s.forward()
-        for k in range(2):
+        for k in range(4):
             assert rel_l2(s.history(k), hist[k]) < TOL32
         gl, gm = s.adjoint_gradient(dis)
         assert rel_l2(gl, gl_ref) < TOL32_GRAD
@@ -93,6 +93,20 @@ def test_element_slot_variant_is_reproducible(gpu_lib):
         s.forward()
         for k in range(2):
             assert np.array_equal(s.history(k), h1[k])
+
+
+def test_matrix_free_variant_must_fit_shots_and_precision(gpu_lib):
+    from hirensi_b200.solver import HrnError
+    p = tiny(nshot=3, nstep=20)
+    with _solver(p) as s:
+        s.set_variant(92, 92)   # two shots per thread: 3 shots do not divide
+        with pytest.raises(HrnError):
+            s.forward()
+    p = tiny(nshot=4, nstep=20)
+    with _solver(p) as s:
+        s.set_variant(94, 94)   # four shots per thread: FP32 only
+        with pytest.raises(HrnError):
+            s.forward()
 
 
 def test_matrix_free_needs_an_assembled_operator(gpu_lib):
