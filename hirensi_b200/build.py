@@ -8,6 +8,7 @@ from __future__ import annotations
 import os
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
@@ -33,14 +34,17 @@ def build(force: bool = False, verbose: bool = False) -> str:
     if not force and not _stale():
         return LIB
     os.makedirs(OUT_DIR, exist_ok=True)
-    objs = []
-    for src in SOURCES:
-        obj = os.path.join(OUT_DIR, src.replace(".cu", ".o"))
-        cmd = [NVCC, *ARCH, *FLAGS, "-c", os.path.join(CSRC, src), "-o", obj]
-        if verbose:
+    objs = [os.path.join(OUT_DIR, src.replace(".cu", ".o")) for src in SOURCES]
+    cmds = [[NVCC, *ARCH, *FLAGS, "-c", os.path.join(CSRC, src), "-o", obj] for src, obj in zip(SOURCES, objs)]
+    if verbose:
+        for cmd in cmds:
             print(" ".join(cmd), file=sys.stderr)
-        subprocess.run(cmd, check=True)
-        objs.append(obj)
+    # the translation units are independent: compile them concurrently
+    with ThreadPoolExecutor(max_workers=max(1, min(len(cmds), os.cpu_count() or 1))) as pool:
+        for r in pool.map(lambda cmd: subprocess.run(cmd, capture_output=True, text=True), cmds):
+            if r.returncode != 0:
+                sys.stderr.write(r.stdout + r.stderr)
+                raise subprocess.CalledProcessError(r.returncode, r.args, r.stdout, r.stderr)
     cmd = [NVCC, *ARCH, "-shared", "-o", LIB, *objs]
     subprocess.run(cmd, check=True)
     return LIB

@@ -400,8 +400,8 @@ int hrn_set_operator_csr(hrn_ctx *c, int32_t neq, const int32_t *c_ia, const int
     HRN_CUDA(c, cudaStreamSynchronize(c->stream));
     c->have_operator = true;
     c->op_from_mesh = false;
-    if (c->lanes_f >= 90 && c->lanes_f <= 95) c->lanes_f = 0;   // matrix-free needs an assembled operator: tune again
-    if (c->lanes_a >= 90 && c->lanes_a <= 95) c->lanes_a = 0;
+    if (c->lanes_f >= 90 && c->lanes_f <= 105) c->lanes_f = 0;   // matrix-free needs an assembled operator: tune again
+    if (c->lanes_a >= 90 && c->lanes_a <= 105) c->lanes_a = 0;
     c->have_forward = false;
     return rebind(c);
 }
@@ -667,11 +667,12 @@ int hrn_set_variant(hrn_ctx *c, int32_t forward, int32_t adjoint)
     if (!c) return HRN_EARG;
     auto ok = [](int v) {
         return v == 0 || v == 40 || v == 80 || v == 160 || v == 41 || v == 81 || v == 161 || v == 42 || v == 43 || v == 82 ||
-               v == 83 || (v >= 90 && v <= 95);
+               v == 83 || (v >= 90 && v <= 95) || (v >= 100 && v <= 105);
     };
     if (!ok(forward) || !ok(adjoint))
         return set_error(c, HRN_EARG, "variant must be 0 (tune), lanes*10 + mat + tiled (lanes 4/8/16, mat 0/1, tiled 0/2; "
-                                      "tiled only with lanes 4/8) or 90-95 (matrix-free: slots even, atomics odd; 1, 2, 4 shots per thread)");
+                                      "tiled only with lanes 4/8) or 90-95 / 100-105 (matrix-free with materialized / rebuilt stage inputs: "
+                                      "slots even, atomics odd; 1, 2, 4 shots per thread)");
     c->lanes_f = forward;
     c->lanes_a = adjoint;
     return HRN_OK;

@@ -93,7 +93,6 @@ struct ElemArgs {
     const double *el_geom;           // [P][27][10] DJI and w*detJ
     const double *el_rho;            // [P]
     const double *lam, *mu, *pmlw;   // nodal lambda, mu; [nj][12] PML weights
-    const T *in_m, *in_t, *in_h;     // stage inputs of C, K, G
     T *slots;                        // [P * 27][9][S]
     T *acc;                          // [neq][S] (atomic variant)
 };
@@ -179,8 +178,64 @@ __device__ __forceinline__ void red_n(T *p, const T (&o)[N])
     }
 }
 
+// N shots (from s0) of the stage input of matrix TAG (0 = C, 1 = K, 2 = G) at row
+// j: read from the vectors the previous stage materialized (MAT), or rebuilt
+// from x1, x2, x3 and the earlier kb with the same fused multiply-adds as the
+// row epilogue, e.g. km_3 = c*kb_2 + x3, kt_3 = c*km_2 + x2, h_3 = c*kt_2 + x1.
+template <typename T, int S, int N>
+__device__ __forceinline__ void stage_input_n(const StageArgs<T> &a, int stage, int mat, int tag, size_t j, int s0, T (&v)[N])
+{
+    const size_t o = j * S + s0;
+    T p1[N], p2[N], p3[N], p4[N];
+    if (stage == 1) {
+        ldg_n<T, N>((tag == 0 ? a.x3 : (tag == 1 ? a.x2 : a.x1)) + o, v);
+        return;
+    }
+    if (mat) {
+        ldg_n<T, N>((tag == 0 ? a.in_m : (tag == 1 ? a.in_t : a.in_h)) + o, v);
+        return;
+    }
+    const T c = a.c, D = a.D;
+    if (stage == 2) {
+        if (tag == 0) { ldg_n<T, N>(a.kb1 + o, p1); ldg_n<T, N>(a.x3 + o, p2); }
+        else if (tag == 1) { ldg_n<T, N>(a.x3 + o, p1); ldg_n<T, N>(a.x2 + o, p2); }
+        else { ldg_n<T, N>(a.x2 + o, p1); ldg_n<T, N>(a.x1 + o, p2); }
+#pragma unroll
+        for (int i = 0; i < N; ++i) v[i] = fmaT(c, p1[i], p2[i]);
+    } else if (stage == 3) {
+        if (tag == 0) {
+            ldg_n<T, N>(a.kb2 + o, p1); ldg_n<T, N>(a.x3 + o, p2);
+#pragma unroll
+            for (int i = 0; i < N; ++i) v[i] = fmaT(c, p1[i], p2[i]);
+        } else if (tag == 1) {
+            ldg_n<T, N>(a.kb1 + o, p1); ldg_n<T, N>(a.x3 + o, p2); ldg_n<T, N>(a.x2 + o, p3);
+#pragma unroll
+            for (int i = 0; i < N; ++i) v[i] = fmaT(c, fmaT(c, p1[i], p2[i]), p3[i]);
+        } else {
+            ldg_n<T, N>(a.x3 + o, p1); ldg_n<T, N>(a.x2 + o, p2); ldg_n<T, N>(a.x1 + o, p3);
+#pragma unroll
+            for (int i = 0; i < N; ++i) v[i] = fmaT(c, fmaT(c, p1[i], p2[i]), p3[i]);
+        }
+    } else {
+        if (tag == 0) {
+            ldg_n<T, N>(a.kb3 + o, p1); ldg_n<T, N>(a.x3 + o, p2);
+#pragma unroll
+            for (int i = 0; i < N; ++i) v[i] = fmaT(D, p1[i], p2[i]);
+        } else if (tag == 1) {
+            ldg_n<T, N>(a.kb2 + o, p1); ldg_n<T, N>(a.x3 + o, p2); ldg_n<T, N>(a.x2 + o, p3);
+#pragma unroll
+            for (int i = 0; i < N; ++i) v[i] = fmaT(D, fmaT(c, p1[i], p2[i]), p3[i]);
+        } else {
+            ldg_n<T, N>(a.kb1 + o, p1); ldg_n<T, N>(a.x3 + o, p2); ldg_n<T, N>(a.x2 + o, p3); ldg_n<T, N>(a.x1 + o, p4);
+#pragma unroll
+            for (int i = 0; i < N; ++i) v[i] = fmaT(D, fmaT(c, fmaT(c, p1[i], p2[i]), p3[i]), p4[i]);
+        }
+    }
+}
+
 template <typename T, int S, int SV, int ADJ, int ACC, bool PML>
-__device__ __forceinline__ void elem_body(const ElemArgs<T> &A, int pbase, int ngrp, int e0, T *U, T *V, T *coef, int *eqs)
+__device__ __forceinline__ void elem_body(const ElemArgs<T> &A, const StageArgs<T> &a, int stage, int mat, int pbase, int ngrp,
+                                          int e0, T *U, T *V, T *coef, int *eqs)
 {
     constexpr int TP = S / SV;
     constexpr int NTAG = PML ? 3 : 1;
@@ -206,10 +261,9 @@ __device__ __forceinline__ void elem_body(const ElemArgs<T> &A, int pbase, int n
         for (int i = tp; i < NTAG * 3; i += TP) {
             const int t = i / 3, c = i % 3;
             const int eq = __ldg(eqp + c);
-            const T *src = PML ? (t == 0 ? A.in_m : (t == 1 ? A.in_t : A.in_h)) : A.in_t;
             T v[S];
             if (eq >= 0) {
-                ldv<T, S>(src + size_t(eq) * S, v);
+                stage_input_n<T, S, S>(a, stage, mat, PML ? t : 1, size_t(eq), 0, v);
             } else {
 #pragma unroll
                 for (int k = 0; k < S; ++k) v[k] = T(0);
@@ -291,13 +345,12 @@ __device__ __forceinline__ void elem_body(const ElemArgs<T> &A, int pbase, int n
                 const int32_t *eqp = A.el_eq + pq * 9;
 #pragma unroll
                 for (int t = 0; t < 3; ++t) {
-                    const T *src = t == 0 ? A.in_m : (t == 1 ? A.in_t : A.in_h);
                     T sv[6][SV];
 #pragma unroll
                     for (int d = 0; d < 6; ++d) {
                         const int eq = __ldg(eqp + 3 + d);
                         if (eq >= 0) {
-                            ldg_n<T, SV>(src + size_t(eq) * S + s0, sv[d]);
+                            stage_input_n<T, S, SV>(a, stage, mat, t, size_t(eq), s0, sv[d]);
                         } else {
 #pragma unroll
                             for (int v = 0; v < SV; ++v) sv[d][v] = T(0);
@@ -447,7 +500,7 @@ __device__ __forceinline__ void elem_body(const ElemArgs<T> &A, int pbase, int n
 // PML elements, the rest regular-domain elements.  ACC = 0: write the
 // element's slot; ACC = 1: add into the row accumulator.
 template <typename T, int S, int SV, int ADJ, int ACC>
-__global__ void __launch_bounds__(216, 2) k_elem(const ElemArgs<T> A)
+__global__ void __launch_bounds__(216, 2) k_elem(const ElemArgs<T> A, const StageArgs<T> a, int stage, int mat)
 {
     constexpr int EPB = elems_per_block<S, SV>();
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -456,9 +509,10 @@ __global__ void __launch_bounds__(216, 2) k_elem(const ElemArgs<T> A)
     T *coef = V + EPB * 243 * S;
     int *eqs = reinterpret_cast<int *>(coef + EPB * 27 * kCoef);
     if (int(blockIdx.x) < A.nb_pml)
-        elem_body<T, S, SV, ADJ, ACC, true>(A, 0, A.nel_pml, int(blockIdx.x) * EPB, U, V, coef, eqs);
+        elem_body<T, S, SV, ADJ, ACC, true>(A, a, stage, mat, 0, A.nel_pml, int(blockIdx.x) * EPB, U, V, coef, eqs);
     else
-        elem_body<T, S, SV, ADJ, ACC, false>(A, A.nel_pml, A.nel_rd, (int(blockIdx.x) - A.nb_pml) * EPB, U, V, coef, eqs);
+        elem_body<T, S, SV, ADJ, ACC, false>(A, a, stage, mat, A.nel_pml, A.nel_rd, (int(blockIdx.x) - A.nb_pml) * EPB, U, V,
+                                             coef, eqs);
 }
 
 // PML weights of every node: F3, F2, F1 (directions x, y, z) of the kinds
@@ -496,7 +550,7 @@ struct NodeArgs {
 };
 
 // Row sum of the element contributions, -iM scaling and the stage epilogue.
-template <typename T, int S, int STAGE, int ACC>
+template <typename T, int S, int STAGE, int ACC, int MAT>
 __global__ void __launch_bounds__(256) k_node(const StageArgs<T> a, const NodeArgs<T> na)
 {
     const int row = blockIdx.x * blockDim.x + threadIdx.x;
@@ -527,7 +581,7 @@ __global__ void __launch_bounds__(256) k_node(const StageArgs<T> a, const NodeAr
     const T im = T(__ldg(na.im + row));
 #pragma unroll
     for (int s = 0; s < S; ++s) acc[s] = -im * acc[s];
-    finish_row<T, S, STAGE, 1>(a, row, acc);
+    finish_row<T, S, STAGE, MAT>(a, row, acc);
 }
 
 // ----------------------------------------------------------------------------
@@ -626,7 +680,7 @@ static int elem_buffers(hrn_ctx *c)
 }
 
 template <typename T, int S, int SV, int ADJ, int ACC>
-static void launch_elem(const ElemArgs<T> &A, int blocks, cudaStream_t st)
+static void launch_elem(const ElemArgs<T> &A, const StageArgs<T> &a, int stage, int mat, int blocks, cudaStream_t st)
 {
     static bool attr_set = false;
     constexpr size_t smem = elem_smem_bytes<T, S, SV>();
@@ -634,23 +688,24 @@ static void launch_elem(const ElemArgs<T> &A, int blocks, cudaStream_t st)
         cudaFuncSetAttribute(k_elem<T, S, SV, ADJ, ACC>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
         attr_set = true;
     }
-    k_elem<T, S, SV, ADJ, ACC><<<blocks, elems_per_block<S, SV>() * 27 * (S / SV), smem, st>>>(A);
+    k_elem<T, S, SV, ADJ, ACC><<<blocks, elems_per_block<S, SV>() * 27 * (S / SV), smem, st>>>(A, a, stage, mat);
 }
 
 template <typename T, int S, int SV>
-static void launch_elem_any(const ElemArgs<T> &A, int blocks, int adj, int acc, cudaStream_t st)
+static void launch_elem_any(const ElemArgs<T> &A, const StageArgs<T> &a, int stage, int mat, int blocks, int adj, int acc,
+                            cudaStream_t st)
 {
     if (adj) {
-        if (acc) launch_elem<T, S, SV, 1, 1>(A, blocks, st);
-        else launch_elem<T, S, SV, 1, 0>(A, blocks, st);
+        if (acc) launch_elem<T, S, SV, 1, 1>(A, a, stage, mat, blocks, st);
+        else launch_elem<T, S, SV, 1, 0>(A, a, stage, mat, blocks, st);
     } else {
-        if (acc) launch_elem<T, S, SV, 0, 1>(A, blocks, st);
-        else launch_elem<T, S, SV, 0, 0>(A, blocks, st);
+        if (acc) launch_elem<T, S, SV, 0, 1>(A, a, stage, mat, blocks, st);
+        else launch_elem<T, S, SV, 0, 0>(A, a, stage, mat, blocks, st);
     }
 }
 
 template <typename T, int S>
-static int elem_stage_t(hrn_ctx *c, const StageArgs<T> &a, int stage, int adj, int acc, int sv)
+static int elem_stage_t(hrn_ctx *c, const StageArgs<T> &a, int stage, int adj, int acc, int sv, int mat)
 {
     ElemArgs<T> A{};
     A.nel_pml = c->nel_pml_e;
@@ -662,8 +717,6 @@ static int elem_stage_t(hrn_ctx *c, const StageArgs<T> &a, int stage, int adj, i
     A.lam = c->d_lam.as<double>();
     A.mu = c->d_mu.as<double>();
     A.pmlw = c->d_pmlw.as<double>();
-    if (stage == 1) { A.in_m = a.x3; A.in_t = a.x2; A.in_h = a.x1; }
-    else { A.in_m = a.in_m; A.in_t = a.in_t; A.in_h = a.in_h; }
     A.slots = c->d_eslots.as<T>();
     A.acc = c->d_eacc.as<T>();
     auto go = [&](auto svc) {
@@ -672,7 +725,7 @@ static int elem_stage_t(hrn_ctx *c, const StageArgs<T> &a, int stage, int adj, i
         A.nb_pml = (c->nel_pml_e + EPB - 1) / EPB;
         const int blocks = A.nb_pml + (c->nel_rd_e + EPB - 1) / EPB;
         if (blocks > 0) {
-            launch_elem_any<T, S, SV>(A, blocks, adj, acc, c->stream);
+            launch_elem_any<T, S, SV>(A, a, stage, mat, blocks, adj, acc, c->stream);
             ++c->launches;
         }
     };
@@ -687,45 +740,52 @@ static int elem_stage_t(hrn_ctx *c, const StageArgs<T> &a, int stage, int adj, i
     NodeArgs<T> na{c->d_row_info.as<int32_t>(), c->d_nslot_ptr.as<int32_t>(), c->d_nslot.as<uint32_t>(),
                    c->d_eslots.as<T>(), c->d_eacc.as<T>(), c->d_im.as<double>()};
     const int th = 256, nb = (c->neq + th - 1) / th;
-    switch (stage * 2 + (acc ? 1 : 0)) {
-    case 2: k_node<T, S, 1, 0><<<nb, th, 0, c->stream>>>(a, na); break;
-    case 3: k_node<T, S, 1, 1><<<nb, th, 0, c->stream>>>(a, na); break;
-    case 4: k_node<T, S, 2, 0><<<nb, th, 0, c->stream>>>(a, na); break;
-    case 5: k_node<T, S, 2, 1><<<nb, th, 0, c->stream>>>(a, na); break;
-    case 6: k_node<T, S, 3, 0><<<nb, th, 0, c->stream>>>(a, na); break;
-    case 7: k_node<T, S, 3, 1><<<nb, th, 0, c->stream>>>(a, na); break;
-    case 8: k_node<T, S, 4, 0><<<nb, th, 0, c->stream>>>(a, na); break;
-    default: k_node<T, S, 4, 1><<<nb, th, 0, c->stream>>>(a, na); break;
-    }
+    auto node = [&](auto stc, auto accc, auto matc) {
+        k_node<T, S, decltype(stc)::value, decltype(accc)::value, decltype(matc)::value><<<nb, th, 0, c->stream>>>(a, na);
+    };
+    using I0 = std::integral_constant<int, 0>;
+    using I1 = std::integral_constant<int, 1>;
+    auto node_st = [&](auto accc, auto matc) {
+        switch (stage) {
+        case 1: node(std::integral_constant<int, 1>{}, accc, matc); break;
+        case 2: node(std::integral_constant<int, 2>{}, accc, matc); break;
+        case 3: node(std::integral_constant<int, 3>{}, accc, matc); break;
+        default: node(std::integral_constant<int, 4>{}, accc, matc); break;
+        }
+    };
+    if (acc) { if (mat) node_st(I1{}, I1{}); else node_st(I1{}, I0{}); }
+    else { if (mat) node_st(I0{}, I1{}); else node_st(I0{}, I0{}); }
     return 0;
 }
 
 #define HRN_ELEM_DISPATCH(T)                                                       \
     switch (c->nshot) {                                                            \
-    case 1: return elem_stage_t<T, 1>(c, *static_cast<const StageArgs<T> *>(args), stage, adj, acc, sv); \
-    case 2: return elem_stage_t<T, 2>(c, *static_cast<const StageArgs<T> *>(args), stage, adj, acc, sv); \
-    case 3: return elem_stage_t<T, 3>(c, *static_cast<const StageArgs<T> *>(args), stage, adj, acc, sv); \
-    case 4: return elem_stage_t<T, 4>(c, *static_cast<const StageArgs<T> *>(args), stage, adj, acc, sv); \
-    case 5: return elem_stage_t<T, 5>(c, *static_cast<const StageArgs<T> *>(args), stage, adj, acc, sv); \
-    case 6: return elem_stage_t<T, 6>(c, *static_cast<const StageArgs<T> *>(args), stage, adj, acc, sv); \
-    case 7: return elem_stage_t<T, 7>(c, *static_cast<const StageArgs<T> *>(args), stage, adj, acc, sv); \
-    default: return elem_stage_t<T, 8>(c, *static_cast<const StageArgs<T> *>(args), stage, adj, acc, sv); \
+    case 1: return elem_stage_t<T, 1>(c, *static_cast<const StageArgs<T> *>(args), stage, adj, acc, sv, mat); \
+    case 2: return elem_stage_t<T, 2>(c, *static_cast<const StageArgs<T> *>(args), stage, adj, acc, sv, mat); \
+    case 3: return elem_stage_t<T, 3>(c, *static_cast<const StageArgs<T> *>(args), stage, adj, acc, sv, mat); \
+    case 4: return elem_stage_t<T, 4>(c, *static_cast<const StageArgs<T> *>(args), stage, adj, acc, sv, mat); \
+    case 5: return elem_stage_t<T, 5>(c, *static_cast<const StageArgs<T> *>(args), stage, adj, acc, sv, mat); \
+    case 6: return elem_stage_t<T, 6>(c, *static_cast<const StageArgs<T> *>(args), stage, adj, acc, sv, mat); \
+    case 7: return elem_stage_t<T, 7>(c, *static_cast<const StageArgs<T> *>(args), stage, adj, acc, sv, mat); \
+    default: return elem_stage_t<T, 8>(c, *static_cast<const StageArgs<T> *>(args), stage, adj, acc, sv, mat); \
     }
 
 // One matrix-free RK4 stage (element kernel + node kernel) on the stage
 // arguments of the CSR kernels; args points to a StageArgs of the context's precision.
-int elem_stage(hrn_ctx *c, const void *args, int stage, int adj, int acc, int sv)
+int elem_stage(hrn_ctx *c, const void *args, int stage, int adj, int acc, int sv, int mat)
 {
     if (c->precision == HRN_FP64) { HRN_ELEM_DISPATCH(double) }
     HRN_ELEM_DISPATCH(float)
 }
 
-// Variants 90-95: element slots (even) or atomic row sums (odd) with 1, 2 or 4
-// shots per thread; 2 needs an even shot count, 4 a multiple of 4 in FP32.
+// Variants 90-95 (stage inputs materialized by the previous stage) and 100-105
+// (rebuilt from x and kb): element slots (even) or atomic row sums (odd) with
+// 1, 2 or 4 shots per thread; 2 needs an even shot count, 4 a multiple of 4 in FP32.
 bool elem_variant_valid(const hrn_ctx *c, int v)
 {
-    if (v < 90 || v > 95) return false;
-    const int sv = 1 << ((v - 90) / 2);
+    const int b = v >= 100 ? 100 : 90;
+    if (v < b || v > b + 5) return false;
+    const int sv = 1 << ((v - b) / 2);
     if (c->nshot % sv != 0) return false;
     return sv < 4 || c->precision == HRN_FP32;
 }

@@ -174,7 +174,7 @@ int finalize_pattern_from_keys(hrn_ctx *c, const std::vector<uint64_t> &keys);
 int vec_reduce(hrn_ctx *c, int kind, int n, const double *x, const double *y, double *out);
 int elem_prepare(hrn_ctx *c);
 int elem_ready(hrn_ctx *c);
-int elem_stage(hrn_ctx *c, const void *stage_args, int stage, int adj, int acc, int shots_per_thread);
+int elem_stage(hrn_ctx *c, const void *stage_args, int stage, int adj, int acc, int shots_per_thread, int mat);
 bool elem_variant_valid(const hrn_ctx *c, int variant);
 int vec_axpby(hrn_ctx *c, int n, double a, const double *x, double b, const double *y, double *z);
 int set_error(hrn_ctx *c, int code, const std::string &msg);

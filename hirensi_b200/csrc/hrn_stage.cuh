@@ -101,6 +101,59 @@ struct StageArgs {
     T c, D, d6;                             // dt/2, dt, dt/6 (negated for the adjoint)
 };
 
+// Stage-input value of matrix TAG (0 = C, 1 = K, 2 = G) at row j, rebuilt from
+// x1, x2, x3 and the earlier kb with the fused multiply-adds the row owner uses,
+// e.g. km_3 = c*kb_2 + x3, kt_3 = c*km_2 + x2, h_3 = c*kt_2 + x1 (c = dt/2).
+template <typename T, int S, int STAGE, int TAG>
+__device__ __forceinline__ void gather(const StageArgs<T> &a, size_t j, T (&v)[S])
+{
+    const size_t o = j * S;
+    if constexpr (STAGE == 1) {
+        ldv<T, S>((TAG == 0 ? a.x3 : (TAG == 1 ? a.x2 : a.x1)) + o, v);
+    } else if constexpr (STAGE == 2) {
+        T p[S], q[S];
+        if constexpr (TAG == 0) { ldv<T, S>(a.kb1 + o, p); ldv<T, S>(a.x3 + o, q); }
+        else if constexpr (TAG == 1) { ldv<T, S>(a.x3 + o, p); ldv<T, S>(a.x2 + o, q); }
+        else { ldv<T, S>(a.x2 + o, p); ldv<T, S>(a.x1 + o, q); }
+#pragma unroll
+        for (int s = 0; s < S; ++s) v[s] = fmaT(a.c, p[s], q[s]);
+    } else if constexpr (STAGE == 3) {
+        if constexpr (TAG == 0) {
+            T p[S], q[S];
+            ldv<T, S>(a.kb2 + o, p); ldv<T, S>(a.x3 + o, q);
+#pragma unroll
+            for (int s = 0; s < S; ++s) v[s] = fmaT(a.c, p[s], q[s]);
+        } else if constexpr (TAG == 1) {
+            T k1[S], x3[S], x2[S];
+            ldv<T, S>(a.kb1 + o, k1); ldv<T, S>(a.x3 + o, x3); ldv<T, S>(a.x2 + o, x2);
+#pragma unroll
+            for (int s = 0; s < S; ++s) v[s] = fmaT(a.c, fmaT(a.c, k1[s], x3[s]), x2[s]);
+        } else {
+            T x3[S], x2[S], x1[S];
+            ldv<T, S>(a.x3 + o, x3); ldv<T, S>(a.x2 + o, x2); ldv<T, S>(a.x1 + o, x1);
+#pragma unroll
+            for (int s = 0; s < S; ++s) v[s] = fmaT(a.c, fmaT(a.c, x3[s], x2[s]), x1[s]);
+        }
+    } else {
+        if constexpr (TAG == 0) {
+            T p[S], q[S];
+            ldv<T, S>(a.kb3 + o, p); ldv<T, S>(a.x3 + o, q);
+#pragma unroll
+            for (int s = 0; s < S; ++s) v[s] = fmaT(a.D, p[s], q[s]);
+        } else if constexpr (TAG == 1) {
+            T k2[S], x3[S], x2[S];
+            ldv<T, S>(a.kb2 + o, k2); ldv<T, S>(a.x3 + o, x3); ldv<T, S>(a.x2 + o, x2);
+#pragma unroll
+            for (int s = 0; s < S; ++s) v[s] = fmaT(a.D, fmaT(a.c, k2[s], x3[s]), x2[s]);
+        } else {
+            T k1[S], x3[S], x2[S], x1[S];
+            ldv<T, S>(a.kb1 + o, k1); ldv<T, S>(a.x3 + o, x3); ldv<T, S>(a.x2 + o, x2); ldv<T, S>(a.x1 + o, x1);
+#pragma unroll
+            for (int s = 0; s < S; ++s) v[s] = fmaT(a.D, fmaT(a.c, fmaT(a.c, k1[s], x3[s]), x2[s]), x1[s]);
+        }
+    }
+}
+
 // Row epilogue: stage source, history (stage 1), kb or the next-stage inputs
 // (stages 1-3) or the RK4 update into the other state buffer (stage 4).
 template <typename T, int S, int STAGE, int MAT>

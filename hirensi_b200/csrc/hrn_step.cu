@@ -26,57 +26,6 @@
 namespace hrn {
 
 
-// Stage-input value of matrix TAG at column j (see the file comment).
-template <typename T, int S, int STAGE, int TAG>
-__device__ __forceinline__ void gather(const StageArgs<T> &a, size_t j, T (&v)[S])
-{
-    const size_t o = j * S;
-    if constexpr (STAGE == 1) {
-        ldv<T, S>((TAG == 0 ? a.x3 : (TAG == 1 ? a.x2 : a.x1)) + o, v);
-    } else if constexpr (STAGE == 2) {
-        T p[S], q[S];
-        if constexpr (TAG == 0) { ldv<T, S>(a.kb1 + o, p); ldv<T, S>(a.x3 + o, q); }
-        else if constexpr (TAG == 1) { ldv<T, S>(a.x3 + o, p); ldv<T, S>(a.x2 + o, q); }
-        else { ldv<T, S>(a.x2 + o, p); ldv<T, S>(a.x1 + o, q); }
-#pragma unroll
-        for (int s = 0; s < S; ++s) v[s] = fmaT(a.c, p[s], q[s]);
-    } else if constexpr (STAGE == 3) {
-        if constexpr (TAG == 0) {
-            T p[S], q[S];
-            ldv<T, S>(a.kb2 + o, p); ldv<T, S>(a.x3 + o, q);
-#pragma unroll
-            for (int s = 0; s < S; ++s) v[s] = fmaT(a.c, p[s], q[s]);
-        } else if constexpr (TAG == 1) {
-            T k1[S], x3[S], x2[S];
-            ldv<T, S>(a.kb1 + o, k1); ldv<T, S>(a.x3 + o, x3); ldv<T, S>(a.x2 + o, x2);
-#pragma unroll
-            for (int s = 0; s < S; ++s) v[s] = fmaT(a.c, fmaT(a.c, k1[s], x3[s]), x2[s]);
-        } else {
-            T x3[S], x2[S], x1[S];
-            ldv<T, S>(a.x3 + o, x3); ldv<T, S>(a.x2 + o, x2); ldv<T, S>(a.x1 + o, x1);
-#pragma unroll
-            for (int s = 0; s < S; ++s) v[s] = fmaT(a.c, fmaT(a.c, x3[s], x2[s]), x1[s]);
-        }
-    } else {
-        if constexpr (TAG == 0) {
-            T p[S], q[S];
-            ldv<T, S>(a.kb3 + o, p); ldv<T, S>(a.x3 + o, q);
-#pragma unroll
-            for (int s = 0; s < S; ++s) v[s] = fmaT(a.D, p[s], q[s]);
-        } else if constexpr (TAG == 1) {
-            T k2[S], x3[S], x2[S];
-            ldv<T, S>(a.kb2 + o, k2); ldv<T, S>(a.x3 + o, x3); ldv<T, S>(a.x2 + o, x2);
-#pragma unroll
-            for (int s = 0; s < S; ++s) v[s] = fmaT(a.D, fmaT(a.c, k2[s], x3[s]), x2[s]);
-        } else {
-            T k1[S], x3[S], x2[S], x1[S];
-            ldv<T, S>(a.kb1 + o, k1); ldv<T, S>(a.x3 + o, x3); ldv<T, S>(a.x2 + o, x2); ldv<T, S>(a.x1 + o, x1);
-#pragma unroll
-            for (int s = 0; s < S; ++s) v[s] = fmaT(a.D, fmaT(a.c, fmaT(a.c, k1[s], x3[s]), x2[s]), x1[s]);
-        }
-    }
-}
-
 // Stage input of the entry's matrix at column j: rebuilt from x and earlier kb
 // (MAT = 0), or read from the vectors the previous stage materialized (MAT = 1).
 template <typename T, int S, int STAGE, int MAT>
@@ -547,9 +496,10 @@ struct TileArgs {
 // tiled with bulk-copied matrix slabs (2); encoded lanes * 10 + mat + tiled,
 // chosen per operator by timing.
 constexpr int kVariants[10] = {40, 80, 160, 41, 81, 161, 42, 43, 82, 83};
-// 90-95: matrix-free element kernels, element slots (even) or atomic row sums
-// (odd), with 1 (90, 91), 2 (92, 93) or 4 (94, 95) shots per thread
-inline bool is_elem_variant(int v) { return v >= 90 && v <= 95; }
+// 90-95 / 100-105: matrix-free element kernels with the stage inputs
+// materialized / rebuilt from x and kb; element slots (even) or atomic row sums
+// (odd), with 1 (+0, +1), 2 (+2, +3) or 4 (+4, +5) shots per thread
+inline bool is_elem_variant(int v) { return (v >= 90 && v <= 95) || (v >= 100 && v <= 105); }
 
 template <typename T, int S, int STAGE, int G, int MAT>
 static void launch_tile(const StageArgs<T> &a, const TileArgs &ta, cudaStream_t st)
@@ -778,7 +728,8 @@ static void launch_step(hrn_ctx *c, StageArgs<T> a, T *X, T *Y, StageTimer *tm, 
         a.in_t = in; a.in_m = in + vn; a.in_h = in + 2 * vn;
         a.out_t = out; a.out_m = out + vn; a.out_h = out + 2 * vn;
         if (is_elem_variant(lanes)) {
-            elem_stage(c, &a, st, adj, (lanes - 90) % 2, 1 << ((lanes - 90) / 2));
+            const int b = lanes >= 100 ? 100 : 90;
+            elem_stage(c, &a, st, adj, (lanes - b) % 2, 1 << ((lanes - b) / 2), b == 90 ? 1 : 0);
         } else {
             switch (st) {
             case 1: launch_stage<T, S, 1>(a, lanes, c->stream, ta); break;
@@ -815,7 +766,7 @@ static int autotune_lanes(hrn_ctx *c, StageArgs<T> a, T *X, T *Y, const TileArgs
     std::vector<int> cand(kVariants, kVariants + 10);
     if (c->op_from_mesh) {
         if (int rc = elem_ready(c)) return rc;
-        for (int v = 90; v <= 95; ++v)
+        for (int v : {90, 91, 92, 93, 94, 95, 100, 101, 102, 103, 104, 105})
             if (elem_variant_valid(c, v)) cand.push_back(v);
     }
     cudaEvent_t e0, e1;

@@ -4,7 +4,8 @@ on the device from the mesh.
 Even variants (90, 92, 94) write each element's contribution to a slot and sum
 the slots of a row in ascending element order (reproducible run to run); odd
 variants (91, 93, 95) add the contributions atomically.  90/91 take one shot per
-thread, 92/93 two, 94/95 four (FP32 only).  Tolerances as in the CSR parity tests: FP64 1e-10
+thread, 92/93 two, 94/95 four (FP32 only); 100-105 are the same with the stage
+inputs rebuilt from x and kb instead of materialized by the previous stage.  Tolerances as in the CSR parity tests: FP64 1e-10
 relative L2 for histories, adjoint histories and gradients; FP32 1e-4 for
 histories and 1e-3 for gradients.
 """
@@ -45,7 +46,8 @@ def _oracle_adjoint(p, om, S, hist, dis):
     return padj, gl, gm
 
 
-@pytest.mark.parametrize("variant,nshot", [(90, 1), (91, 1), (90, 3), (91, 3), (92, 2), (93, 4)])
+@pytest.mark.parametrize("variant,nshot", [(90, 1), (91, 1), (90, 3), (91, 3), (92, 2), (93, 4),
+                                           (100, 1), (101, 3), (102, 2), (103, 4)])
 def test_matrix_free_fp64_matches_oracle(gpu_lib, variant, nshot):
     p = tiny(nshot=nshot, nstep=150)
     _, _, hist_t = oracle_forward(p, p["lam_t"], p["mu_t"])
@@ -67,7 +69,7 @@ def test_matrix_free_fp64_matches_oracle(gpu_lib, variant, nshot):
         assert rel_l2(gm, gm_ref) < TOL64
 
 
-@pytest.mark.parametrize("variant", [90, 91, 92, 93, 94, 95])
+@pytest.mark.parametrize("variant", [90, 91, 92, 93, 94, 95, 100, 101, 102, 103, 104, 105])
 def test_matrix_free_fp32_within_bars(gpu_lib, variant):
     p = tiny(nshot=4, nstep=150)
     _, _, hist_t = oracle_forward(p, p["lam_t"], p["mu_t"])
