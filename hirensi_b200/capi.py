@@ -40,6 +40,7 @@ SIGNATURES = {
     "hrn_get_traces": (C.c_int, [VP, PD]),
     "hrn_misfit": (C.c_int, [VP, PD, PD]),
     "hrn_misfit_noalloc": (C.c_int, [VP, VP, PD]),
+    "hrn_set_checkpointing": (C.c_int, [VP, C.c_int32]),
     "hrn_adjoint_gradient": (C.c_int, [VP, PD, C.c_int32, C.c_int32, PD, PD]),
     "hrn_get_adjoint_history": (C.c_int, [VP, C.c_int32, PD]),
     "hrn_set_stream": (C.c_int, [VP, VP]),

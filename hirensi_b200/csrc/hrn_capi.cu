@@ -268,6 +268,12 @@ static int upload_receivers(hrn_ctx *c)
     HRN_CUDA(c, cudaMemcpy(c->d_aslot_q.p, ql.data(), ql.size() * 4, cudaMemcpyHostToDevice));
     HRN_CUDA(c, cudaMemcpy(c->d_aslot_eq.p, seq.data(), seq.size() * 4, cudaMemcpyHostToDevice));
     HRN_CUDA(c, cudaMemcpy(c->d_eqdis_map.p, c->h_eqdis_map.data(), size_t(c->nrec3) * 4, cudaMemcpyHostToDevice));
+    std::vector<int32_t> iota(size_t(c->nrec3));
+    for (int q = 0; q < c->nrec3; ++q) iota[q] = q;
+    HRN_CUDA(c, c->d_eqdis.alloc(size_t(c->nrec3) * 4));
+    HRN_CUDA(c, c->d_iota.alloc(size_t(c->nrec3) * 4));
+    HRN_CUDA(c, cudaMemcpy(c->d_eqdis.p, c->h_eqdis.data(), size_t(c->nrec3) * 4, cudaMemcpyHostToDevice));
+    HRN_CUDA(c, cudaMemcpy(c->d_iota.p, iota.data(), size_t(c->nrec3) * 4, cudaMemcpyHostToDevice));
     return 0;
 }
 
@@ -277,7 +283,21 @@ static int ensure_state(hrn_ctx *c)
     HRN_CUDA(c, c->d_X.alloc(2 * 3 * size_t(c->neq) * S * eb));
     HRN_CUDA(c, c->d_KB.alloc(3 * size_t(c->neq) * S * eb));
     HRN_CUDA(c, c->d_MB.alloc(2 * 3 * size_t(c->neq) * S * eb));
-    HRN_CUDA(c, c->d_hist.alloc(std::max<size_t>(size_t(c->nstep + 1) * c->nstore * S * eb, 1)));
+    if (c->ckpt > 0) {
+        // forward states every ckpt steps, one segment of history, all receiver traces
+        c->d_hist.release();
+        const size_t nck = size_t(c->nstep / c->ckpt) + 1;
+        HRN_CUDA(c, c->d_ckpt.alloc(nck * 3 * size_t(c->neq) * S * eb));
+        HRN_CUDA(c, c->d_ckseg.alloc(std::max<size_t>(size_t(c->ckpt) * c->nstore * S * eb, 1)));
+        HRN_CUDA(c, c->d_traces.alloc(std::max<size_t>(size_t(c->nstep + 1) * c->nrec3 * S * eb, 1)));
+        HRN_CUDA(c, c->d_Xr.alloc(2 * 3 * size_t(c->neq) * S * eb));
+    } else {
+        c->d_ckpt.release();
+        c->d_ckseg.release();
+        c->d_traces.release();
+        c->d_Xr.release();
+        HRN_CUDA(c, c->d_hist.alloc(std::max<size_t>(size_t(c->nstep + 1) * c->nstore * S * eb, 1)));
+    }
     return 0;
 }
 
@@ -574,6 +594,7 @@ int hrn_get_history(hrn_ctx *c, int32_t shot, double *u_store)
 {
     if (!c || !u_store) return HRN_EARG;
     if (!c->have_forward) return set_error(c, HRN_ESTATE, "no forward history");
+    if (c->ckpt > 0) return set_error(c, HRN_ESTATE, "the forward history is not kept with checkpointing (receiver traces are)");
     if (shot < 0 || shot >= c->nshot) return set_error(c, HRN_EARG, "shot out of range");
     const size_t S = c->nshot, n = size_t(c->nstep + 1) * c->nstore;
     HRN_CUDA(c, cudaStreamSynchronize(c->stream));
@@ -616,9 +637,11 @@ int hrn_get_traces(hrn_ctx *c, double *traces)
     HRN_CUDA(c, cudaStreamSynchronize(c->stream));
     // one strided 2D copy per receiver pulls its S values at every step
     std::vector<char> buf(T1 * S * eb);
+    const RecView rv = rec_view(c);
     for (int q = 0; q < c->nrec3; ++q) {
-        const char *src = static_cast<const char *>(c->d_hist.p) + size_t(c->h_eqdis_map[q]) * S * eb;
-        HRN_CUDA(c, cudaMemcpy2D(buf.data(), S * eb, src, size_t(c->nstore) * S * eb, S * eb, T1, cudaMemcpyDeviceToHost));
+        const int pos = c->ckpt > 0 ? q : c->h_eqdis_map[q];
+        const char *src = static_cast<const char *>(rv.hist) + size_t(pos) * S * eb;
+        HRN_CUDA(c, cudaMemcpy2D(buf.data(), S * eb, src, size_t(rv.stride) * S * eb, S * eb, T1, cudaMemcpyDeviceToHost));
         for (size_t s = 0; s < S; ++s)
             for (size_t n = 0; n < T1; ++n) {
                 double v = eb == 8 ? reinterpret_cast<const double *>(buf.data())[n * S + s]
@@ -683,6 +706,16 @@ int hrn_get_variant(hrn_ctx *c, int32_t *forward, int32_t *adjoint)
     if (!c) return HRN_EARG;
     if (forward) *forward = c->lanes_f;
     if (adjoint) *adjoint = c->lanes_a;
+    return HRN_OK;
+}
+
+int hrn_set_checkpointing(hrn_ctx *c, int32_t interval)
+{
+    if (!c) return HRN_EARG;
+    if (interval < 0) return set_error(c, HRN_EARG, "checkpoint interval must be >= 0");
+    c->ckpt = interval;
+    c->have_forward = false;
+    c->have_phist = false;
     return HRN_OK;
 }
 

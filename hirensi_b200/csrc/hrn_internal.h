@@ -132,6 +132,14 @@ struct hrn_ctx {
     hrn::DevBuf d_mis_terms;      // [nshot][nstep+1] FP64
     hrn::DevBuf d_cost;           // [1 + nshot] FP64
 
+    // ---- checkpointing of the forward wavefield (0: keep the whole history)
+    int ckpt = 0;                 // steps between stored forward states
+    hrn::DevBuf d_ckpt;           // [nstep / ckpt + 1][3][neq][S] forward state at steps 0, ckpt, 2 ckpt, ...
+    hrn::DevBuf d_ckseg;          // [ckpt][nstore][S] history of the segment being recomputed
+    hrn::DevBuf d_traces;         // [nstep+1][nrec3][S] receiver displacements of every step
+    hrn::DevBuf d_Xr;             // [2][3][neq][S] state of the recomputed forward
+    hrn::DevBuf d_eqdis, d_iota;  // [nrec3] receiver equations; 0 .. nrec3-1
+
     // ---- state and histories
     hrn::DevBuf d_X;              // [2][3][neq][S]
     hrn::DevBuf d_KB;             // [3][neq][S]
@@ -164,6 +172,19 @@ struct hrn_ctx {
 
 // Kernel launchers implemented in the .cu files.
 namespace hrn {
+// Where the receiver displacements of every step live: the forward history
+// (rows = history positions) or, with checkpointing, the trace buffer (rows =
+// receivers).  Row q of step n: hist + (n * stride + map[q]) * S.
+struct RecView {
+    const void *hist;
+    int stride;
+    const int32_t *map;
+};
+inline RecView rec_view(const hrn_ctx *c)
+{
+    if (c->ckpt > 0) return RecView{c->d_traces.p, c->nrec3, c->d_iota.as<int32_t>()};
+    return RecView{c->d_hist.p, c->nstore, c->d_eqdis_map.as<int32_t>()};
+}
 int launch_scale_operator(hrn_ctx *c);
 int run_forward(hrn_ctx *c);
 int run_adjoint_gradient(hrn_ctx *c, int lambda_2mu, int keep_p);

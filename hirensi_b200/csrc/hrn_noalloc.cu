@@ -96,14 +96,15 @@ extern "C" int hrn_misfit_noalloc(hrn_ctx *c, const double *d_dis_meas, double *
     double *terms = scratch, *out = scratch + kNoAllocMaxTerms;
     const int th = 128, nb = int((nterms + th - 1) / th);
     if (c->nslot_a > 0) {
+        const RecView rv = rec_view(c);
         if (c->precision == HRN_FP64)
-            k_noalloc_terms<double><<<nb, th, 0, c->stream>>>(c->nshot, c->nstep, c->nstore, c->nrec3, c->nslot_a,
-                                                              c->d_aslot_ptr.as<int32_t>(), c->d_aslot_q.as<int32_t>(),
-                                                              c->d_eqdis_map.as<int32_t>(), c->d_hist.as<double>(), d_dis_meas, terms);
+            k_noalloc_terms<double><<<nb, th, 0, c->stream>>>(c->nshot, c->nstep, rv.stride, c->nrec3, c->nslot_a,
+                                                              c->d_aslot_ptr.as<int32_t>(), c->d_aslot_q.as<int32_t>(), rv.map,
+                                                              static_cast<const double *>(rv.hist), d_dis_meas, terms);
         else
-            k_noalloc_terms<float><<<nb, th, 0, c->stream>>>(c->nshot, c->nstep, c->nstore, c->nrec3, c->nslot_a,
-                                                             c->d_aslot_ptr.as<int32_t>(), c->d_aslot_q.as<int32_t>(),
-                                                             c->d_eqdis_map.as<int32_t>(), c->d_hist.as<float>(), d_dis_meas, terms);
+            k_noalloc_terms<float><<<nb, th, 0, c->stream>>>(c->nshot, c->nstep, rv.stride, c->nrec3, c->nslot_a,
+                                                             c->d_aslot_ptr.as<int32_t>(), c->d_aslot_q.as<int32_t>(), rv.map,
+                                                             static_cast<const float *>(rv.hist), d_dis_meas, terms);
         ++c->launches;
     } else {
         // no receivers: every term is zero (the scratch keeps the last call's contents)

@@ -295,6 +295,16 @@ __global__ void k_src_fwd(int nstep, int nslot, const int32_t *__restrict__ slot
 // Adjoint stage sources of step n (S4/Solver_PETSc_Explicit.F90:1269-1312):
 // k1 = iM r_n, k4 = iM r_{n-1}, k2 = k3 = (k1 + k4)/2 with
 // r_m = U_Store(EqDis_MAP, m) - Dis_meas(m, :) summed over duplicate equations.
+// Receiver displacements of one step (checkpointed forward): out[q][s] = x2[eqdis[q]][s].
+template <typename T, int S>
+__global__ void k_traces(int nrec3, const int32_t *__restrict__ eq, const T *__restrict__ x2, T *__restrict__ out)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nrec3 * S) return;
+    const int q = t / S, s = t % S;
+    out[t] = x2[size_t(eq[q]) * S + s];
+}
+
 template <typename T, int S>
 __global__ void k_src_adj(int n, int nstep, int nstore, int nrec3, int nslot, const int32_t *__restrict__ ptr,
                           const int32_t *__restrict__ qlist, const int32_t *__restrict__ slot_eq,
@@ -799,6 +809,31 @@ static int check_step_error(hrn_ctx *c)
     return 0;
 }
 
+// Stage arguments of the forward operator (CSR, forward sources, history rows).
+template <typename T, int S>
+static StageArgs<T> forward_args(hrn_ctx *c)
+{
+    StageArgs<T> a{};
+    a.n = c->neq;
+    a.rowptr = c->d_rowptr.as<int32_t>();
+    a.seg = c->d_seg.as<int2>();
+    a.colx = c->d_colx.as<uint32_t>();
+    a.val = c->d_fwd.as<T>();
+    a.slot = c->d_slot_f.as<int32_t>();
+    a.nslot = c->nslot_f;
+    a.store_pos = c->d_store_pos.as<int32_t>();
+    a.c = T(0.5 * c->dt);
+    a.D = T(c->dt);
+    a.d6 = T(c->dt / 6.0);
+    return a;
+}
+
+template <typename T, int S>
+static const T *forward_src(hrn_ctx *c, int n)
+{
+    return c->nslot_f ? c->d_srcv_f.as<T>() + size_t(n) * 4 * c->nslot_f * S : nullptr;
+}
+
 template <typename T, int S>
 static int forward_t(hrn_ctx *c)
 {
@@ -816,18 +851,7 @@ static int forward_t(hrn_ctx *c)
                                                                      c->d_im.as<double>(), c->d_srcv_f.as<T>()); ++c->launches;
         HRN_CUDA(c, cudaGetLastError());
     }
-    StageArgs<T> a{};
-    a.n = c->neq;
-    a.rowptr = c->d_rowptr.as<int32_t>();
-    a.seg = c->d_seg.as<int2>();
-    a.colx = c->d_colx.as<uint32_t>();
-    a.val = c->d_fwd.as<T>();
-    a.slot = c->d_slot_f.as<int32_t>();
-    a.nslot = c->nslot_f;
-    a.store_pos = c->d_store_pos.as<int32_t>();
-    a.c = T(0.5 * c->dt);
-    a.D = T(c->dt);
-    a.d6 = T(c->dt / 6.0);
+    StageArgs<T> a = forward_args<T, S>(c);
     TileArgs ta{c->d_tiles.as<int32_t>(), c->ntiles, std::min(c->ntiles, 2 * c->num_sms), c->d_step_err.as<int>()};
     if (c->lanes_f <= 0) {
         a.srcv = c->d_srcv_f.as<T>();
@@ -840,10 +864,24 @@ static int forward_t(hrn_ctx *c)
         if (int rc = elem_ready(c)) return rc;
     }
     StageTimer tm(c);
+    const int K = c->ckpt;
     for (int n = 0; n <= c->nstep; ++n) {
-        a.srcv = c->nslot_f ? c->d_srcv_f.as<T>() + size_t(n) * 4 * c->nslot_f * S : nullptr;
-        a.hist = c->d_hist.as<T>() + size_t(n) * c->nstore * S;
+        a.srcv = forward_src<T, S>(c, n);
         T *X = (n & 1) ? X1 : X0, *Y = (n & 1) ? X0 : X1;
+        if (K > 0) {
+            // checkpointed: the state every K steps and the receiver rows of every step
+            if (n % K == 0)
+                HRN_CUDA(c, cudaMemcpyAsync(c->d_ckpt.as<T>() + size_t(n / K) * 3 * vn, X, 3 * vn * sizeof(T),
+                                            cudaMemcpyDeviceToDevice, c->stream));
+            if (c->nrec3 > 0) {
+                k_traces<T, S><<<(c->nrec3 * S + 127) / 128, 128, 0, c->stream>>>(
+                    c->nrec3, c->d_eqdis.as<int32_t>(), X + vn, c->d_traces.as<T>() + size_t(n) * c->nrec3 * S);
+                ++c->launches;
+            }
+            a.hist = nullptr;
+        } else {
+            a.hist = c->d_hist.as<T>() + size_t(n) * c->nstore * S;
+        }
         launch_step<T, S>(c, a, X, Y, c->timing ? &tm : nullptr, c->lanes_f, ta, 0);
     }
     HRN_CUDA(c, cudaGetLastError());
@@ -907,12 +945,32 @@ static int adjoint_t(hrn_ctx *c, int lambda_2mu, int keep_p)
     StageTimer tm(c);
     double *gl = c->d_g.as<double>(), *gmu = gl + c->nj;
     const int gblocks = (c->nel_rd + kGradElems - 1) / kGradElems;
+    const RecView rv = rec_view(c);
+    const int K = c->ckpt;
+    StageArgs<T> af = forward_args<T, S>(c);
+    TileArgs taf{c->d_tiles.as<int32_t>(), c->ntiles, std::min(c->ntiles, 2 * c->num_sms), c->d_step_err.as<int>()};
     int it = 0;
     for (int n = c->nstep; n >= 1; --n, ++it) {
+        const int k0 = K > 0 ? (n / K) * K : 0;   // first step of n's checkpoint segment
+        if (K > 0 && (n == c->nstep || n % K == K - 1)) {
+            // recompute the forward history of steps k0 .. min(k0 + K - 1, nstep - 1) from the checkpoint
+            T *R0 = c->d_Xr.as<T>(), *R1 = R0 + 3 * vn;
+            HRN_CUDA(c, cudaMemcpyAsync(R0, c->d_ckpt.as<T>() + size_t(n / K) * 3 * vn, 3 * vn * sizeof(T),
+                                        cudaMemcpyDeviceToDevice, c->stream));
+            const int m1 = std::min(k0 + K - 1, c->nstep - 1);
+            for (int m = k0; m <= m1; ++m) {
+                af.srcv = forward_src<T, S>(c, m);
+                af.hist = c->d_ckseg.as<T>() + size_t(m - k0) * c->nstore * S;
+                T *Xm = ((m - k0) & 1) ? R1 : R0, *Ym = ((m - k0) & 1) ? R0 : R1;
+                launch_step<T, S>(c, af, Xm, Ym, c->timing ? &tm : nullptr, c->lanes_f, taf, 0);
+            }
+        }
+        const T *u_n = K > 0 ? c->d_ckseg.as<T>() + size_t(n - k0) * c->nstore * S
+                             : c->d_hist.as<T>() + size_t(n) * c->nstore * S;
         if (c->nslot_a > 0)
             k_src_adj<T, S><<<(c->nslot_a * S + 127) / 128, 128, 0, c->stream>>>(
-                n, c->nstep, c->nstore, c->nrec3, c->nslot_a, c->d_aslot_ptr.as<int32_t>(), c->d_aslot_q.as<int32_t>(),
-                c->d_aslot_eq.as<int32_t>(), c->d_eqdis_map.as<int32_t>(), c->d_hist.as<T>(), c->d_dis.as<double>(),
+                n, c->nstep, rv.stride, c->nrec3, c->nslot_a, c->d_aslot_ptr.as<int32_t>(), c->d_aslot_q.as<int32_t>(),
+                c->d_aslot_eq.as<int32_t>(), rv.map, static_cast<const T *>(rv.hist), c->d_dis.as<double>(),
                 c->d_im.as<double>(), c->d_srcv_a.as<T>()); ++c->launches;
         a.hist = keep_p ? c->d_phist.as<T>() + size_t(n) * c->nstore * S : nullptr;
         T *X = (it & 1) ? X1 : X0, *Y = (it & 1) ? X0 : X1;
@@ -920,7 +978,7 @@ static int adjoint_t(hrn_ctx *c, int lambda_2mu, int keep_p)
         if (n <= c->nstep - 1 && c->nel_rd > 0)
             k_gradient<T, S><<<gblocks, 128, 0, c->stream>>>(c->nel_rd, c->d_rd_store.as<int32_t>(), c->d_rd_elems.as<int32_t>(),
                                                              c->d_inod.as<int32_t>(), c->d_rd_geom.as<double>(),
-                                                             c->d_hist.as<T>() + size_t(n) * c->nstore * S, X + vn,
+                                                             u_n, X + vn,
                                                              c->d_store_eq.as<int32_t>(), gl, gmu, c->dt, lambda_2mu); ++c->launches;
     }
     HRN_CUDA(c, cudaGetLastError());
@@ -944,9 +1002,10 @@ template <typename T, int S>
 static int misfit_t(hrn_ctx *c, double *cost)
 {
     const int tot = (c->nstep + 1) * S;
-    k_misfit_terms<T, S><<<(tot + 127) / 128, 128, 0, c->stream>>>(c->nstep, c->nstore, c->nrec3, c->nslot_a,
+    const RecView rv = rec_view(c);
+    k_misfit_terms<T, S><<<(tot + 127) / 128, 128, 0, c->stream>>>(c->nstep, rv.stride, c->nrec3, c->nslot_a,
                                                                    c->d_aslot_ptr.as<int32_t>(), c->d_aslot_q.as<int32_t>(),
-                                                                   c->d_eqdis_map.as<int32_t>(), c->d_hist.as<T>(),
+                                                                   rv.map, static_cast<const T *>(rv.hist),
                                                                    c->d_dis.as<double>(), c->d_mis_terms.as<double>()); ++c->launches;
     k_misfit_sum<<<1, 1, 0, c->stream>>>(S, c->nstep, c->dt, c->d_mis_terms.as<double>(), c->d_cost.as<double>()); ++c->launches;
     HRN_CUDA(c, cudaGetLastError());

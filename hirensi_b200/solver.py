@@ -157,8 +157,17 @@ class Solver:
             d = self._dis(dis_meas)
             self._check(self._L.hrn_set_data(self.h, d.ctypes.data_as(C.c_void_p), 0))
 
+    def set_checkpointing(self, interval: int):
+        """0: keep the whole forward history; K > 0: keep the forward state every
+        K steps and recompute each segment's history during the adjoint."""
+        self._check(self._L.hrn_set_checkpointing(self.h, int(interval)))
+
     def set_variant(self, forward: int = 0, adjoint: int = 0):
-        """Force the stage-kernel variant (lanes*10 + materialized), 0 = autotune."""
+        """Force the stage-kernel variant, 0 = chosen by timing on first use.
+        CSR: lanes per row * 10 + stage inputs materialized (1) or rebuilt (0),
+        + 2 for the tiled kernel (40-43, 80-83, 160, 161).  Matrix-free (operator
+        assembled from the mesh): 90-95 materialized / 100-105 rebuilt inputs,
+        even = element slots, odd = atomic row sums, with 1, 2 or 4 shots per thread."""
         self._check(self._L.hrn_set_variant(self.h, int(forward), int(adjoint)))
 
     def variant(self):

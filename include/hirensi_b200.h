@@ -105,6 +105,17 @@ int hrn_set_data(hrn_ctx *ctx, const double *dis_meas, int32_t on_device);
 
 /* ---- time loops ------------------------------------------------------------ */
 
+/* Forward-wavefield checkpointing for the adjoint.  interval 0 (the default)
+ * keeps the whole history U_Store(NStore, 0:NSTEP) on the device, as the
+ * reference does.  interval K > 0 keeps instead the forward state every K steps
+ * and the receiver displacements of every step.  hrn_adjoint_gradient then
+ * recomputes the history of each K-step segment from its checkpoint before
+ * stepping the adjoint through it.  This costs one more forward pass and needs
+ * device memory for about (NSTEP/K) states + K history rows.  With
+ * checkpointing, hrn_get_history is unavailable; misfit, traces and gradient
+ * are the same. */
+int hrn_set_checkpointing(hrn_ctx *ctx, int32_t interval);
+
 /* Forward RK4 for all shots, EXPLICIT_RK4_PETSC_PML_3D (S4/Solver_PETSc_Explicit.F90:660-1117).
  * The history U_Store of every shot stays on the device. */
 int hrn_forward(hrn_ctx *ctx);
