@@ -50,6 +50,8 @@ def parse_args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fwi", action="store_true", help="skip the FWI time-to-misfit leg")
     ap.add_argument("--fwi-iters", type=int, default=10)
+    ap.add_argument("--profile-precision", choices=["fp64", "fp32"], default="fp64",
+                    help="stepping precision of the --profile-case run")
     ap.add_argument("--variant", type=int, default=0,
                     help="stage-kernel variant for forward and adjoint (0 = chosen by timing on first use)")
     return ap.parse_args()
@@ -160,7 +162,7 @@ def run_native(args, rank, world, local_rank):
     m = prob.mesh
     stream = torch.cuda.current_stream(dev)
 
-    def make_solver(precision):
+    def make_solver(precision, variant=True):
         s = Solver(precision, device=local_rank)
         s.set_stream(stream.cuda_stream)
         s.set_mesh(m, RHO)
@@ -168,15 +170,20 @@ def run_native(args, rank, world, local_rank):
         s.set_history(m.store_eq)
         s.set_shots(prob.nstep, prob.dt, prob.src_eq, prob.src_b, prob.ftab)
         s.set_receivers(prob.eqdis, prob.eqdis_map)
-        if args.variant:
+        if variant and args.variant:
             s.set_variant(args.variant, args.variant)
         return s
 
     # measured data: FP64 forward of the true model (set-up, untimed)
-    s64 = make_solver("fp64")
+    fp32_profile = args.profile_case and args.profile_precision == "fp32"
+    s64 = make_solver("fp64", variant=not fp32_profile)
     s64.assemble(prob.lam_true, prob.mu_true)
     s64.forward()
     dis = s64.traces()
+    if fp32_profile:
+        # profiler runs of the FP32 stepping: the value leg runs in FP32
+        s64.close()
+        s64 = make_solver("fp32")
     dis_dev = torch.from_numpy(dis).to(dev)
     lam_dev = torch.from_numpy(prob.lam0).to(dev)
     mu_dev = torch.from_numpy(prob.mu0).to(dev)
@@ -261,7 +268,8 @@ def run_native(args, rank, world, local_rank):
 
     result = {"metric": METRIC, "value": value / 1e9, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
               "ms_per_step": ms_val / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-              "dtype": "f64", "data": "synthetic (seeded layered model with a Gaussian anomaly; no dataset)"}
+              "dtype": "f32" if (args.profile_case and args.profile_precision == "fp32") else "f64",
+              "data": "synthetic (seeded layered model with a Gaussian anomaly; no dataset)"}
     nnz = [s64.operator_csr(w)[2].size for w in range(3)]
     result["config"] = {"workload": prob.name + f"_4shots_{prob.nstep}steps", "elements": m.nel, "nodes": m.nj,
                         "dof": prob.dof, "equations": m.neq, "nnz_CKG": nnz, "shots_per_gpu": prob.nshot,
