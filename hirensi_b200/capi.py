@@ -41,6 +41,9 @@ SIGNATURES = {
     "hrn_misfit": (C.c_int, [VP, PD, PD]),
     "hrn_misfit_noalloc": (C.c_int, [VP, VP, PD]),
     "hrn_set_checkpointing": (C.c_int, [VP, C.c_int32]),
+    "hrn_illumination": (C.c_int, [VP, VP]),
+    "hrn_cnn_conv3d_forward": (C.c_int, [C.c_int32] * 5 + [VP, VP, VP, C.c_int32, VP, VP]),
+    "hrn_cnn_conv3d_backward": (C.c_int, [C.c_int32] * 5 + [VP, VP, VP, C.c_int32, VP, VP, VP, VP, VP]),
     "hrn_adjoint_gradient": (C.c_int, [VP, PD, C.c_int32, C.c_int32, PD, PD]),
     "hrn_get_adjoint_history": (C.c_int, [VP, C.c_int32, PD]),
     "hrn_set_stream": (C.c_int, [VP, VP]),

@@ -240,6 +240,27 @@ int gradient_mass(hrn_ctx *c, double *mg)
 
 using namespace hrn;
 
+namespace hrn {
+// Source illumination of every stored node: the sum over steps, shots and the three
+// displacement components of u^2 in the forward history [nstep+1][nstore][S].
+template <typename T>
+__global__ void k_illumination(int nnode, int nstore, int nstep, int S, const T *__restrict__ hist, double *__restrict__ out)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= nnode) return;
+    double acc = 0.0;
+    for (int n = 0; n <= nstep; ++n) {
+        const T *h = hist + (size_t(n) * nstore + 3 * size_t(k)) * S;
+        for (int i = 0; i < 3 * S; ++i) {
+            const double v = double(h[i]);
+            acc = fma(v, v, acc);
+        }
+    }
+    out[k] = acc;
+}
+
+}  // namespace hrn
+
 extern "C" {
 
 int hrn_vec_dot(hrn_ctx *c, int32_t n, const double *x, const double *y, double *out)
@@ -293,6 +314,25 @@ int hrn_regularization_tv(hrn_ctx *c, const double *d_lambda, const double *d_mu
     if (!c || !d_lambda || !d_mu || !d_reg_lambda || !d_reg_mu || !cost_lambda || !cost_mu) return HRN_EARG;
     if (!c->have_mesh) return set_error(c, HRN_ESTATE, "no mesh: call hrn_set_mesh first");
     return regularization_tv(c, d_lambda, d_mu, d_reg_lambda, d_reg_mu, cost_lambda, cost_mu);
+}
+
+int hrn_illumination(hrn_ctx *c, double *d_out)
+{
+    if (!c || !d_out) return HRN_EARG;
+    if (!c->have_forward) return set_error(c, HRN_ESTATE, "no forward history: call hrn_forward first");
+    if (c->ckpt > 0) return set_error(c, HRN_ESTATE, "illumination needs the whole forward history (checkpointing is on)");
+    if (c->nstore % 3 != 0) return set_error(c, HRN_EARG, "history rows must come in x, y, z triples");
+    cudaSetDevice(c->device);
+    const int nnode = c->nstore / 3, th = 128;
+    if (c->precision == HRN_FP64)
+        k_illumination<double><<<(nnode + th - 1) / th, th, 0, c->stream>>>(nnode, c->nstore, c->nstep, c->nshot,
+                                                                          c->d_hist.as<double>(), d_out);
+    else
+        k_illumination<float><<<(nnode + th - 1) / th, th, 0, c->stream>>>(nnode, c->nstore, c->nstep, c->nshot,
+                                                                         c->d_hist.as<float>(), d_out);
+    ++c->launches;
+    HRN_CUDA(c, cudaGetLastError());
+    return HRN_OK;
 }
 
 int hrn_gradient_mass(hrn_ctx *c, double *d_mg)

@@ -46,9 +46,16 @@ class ArmijoFailure(RuntimeError):
 
 
 class FWI:
-    def __init__(self, backend, cfg: InversionConfig):
+    """preconditioner: optional object with ``direction(backend, g_l, g_m, lam, mu)``
+    returning a proposed update direction (``hirensi_b200.learned.LearnedPreconditioner``).
+    Each iteration tries it first with one Armijo test on the true misfit.  If the test
+    fails, the model is restored and the iteration takes the reference's L-BFGS path
+    unchanged."""
+
+    def __init__(self, backend, cfg: InversionConfig, preconditioner=None):
         self.b = backend
         self.cfg = cfg
+        self.pre = preconditioner
 
     def run(self, lam0, mu0, n_iter: int, target_reduction: float | None = None, log=None):
         b, cfg = self.b, self.cfg
@@ -141,11 +148,32 @@ class FWI:
                 a_l = a_l_sd
             if chk_m and cfg.search == "LBFGS":
                 a_m = a_m_sd
-            update(a_l, a_m, it)
-            J = b.forward(lam, mu)
+            learned = False
+            if self.pre is not None:
+                q_l, q_m = self.pre.direction(b, g_l, g_m, lam, mu)
+                gq_l, gq_m = b.dot(g_l, q_l), b.dot(g_m, q_m)
+                if gq_l < 0.0 and gq_m < 0.0:
+                    al = fac_l / b.norminf(q_l)
+                    am = fac_m / b.norminf(q_m)
+                    b.axpby(al, q_l, 1.0, lam_pre, lam)
+                    b.axpby(am, q_m, 1.0, mu_pre, mu)
+                    b.extend(lam)
+                    b.extend(mu)
+                    b.clip(lam, *cfg.bounds_lambda)
+                    b.clip(mu, *cfg.bounds_mu)
+                    J_try = b.forward(lam, mu)
+                    if J_try <= J_pre + cfg.armijo_c * (al * gq_l + am * gq_m):   # sufficient decrease (g.q < 0)
+                        learned, J, a_l, a_m = True, J_try, al, am
+            if learned:
+                count = 0
+                rec_extra = {"learned": True}
+            else:
+                rec_extra = {"learned": False} if self.pre is not None else {}
+                update(a_l, a_m, it)
+                J = b.forward(lam, mu)
             armijo = cfg.armijo_c * abs(a_m) * gp_m + cfg.armijo_c * abs(a_l) * gp_l
             count = 0
-            while J > J_pre + armijo:            # :737-896
+            while not learned and J > J_pre + armijo:            # :737-896
                 count += 1
                 if count == 3:
                     fac_l /= 6.0
@@ -161,7 +189,7 @@ class FWI:
                     raise ArmijoFailure(f"Armijo condition failure at iteration {it}")
             rec = dict(iter=it, misfit=J, cost=J + cost_rl + cost_rm, reg_lambda=cost_rl, reg_mu=cost_rm,
                        g_lambda=b.norm2(g_l), g_mu=b.norm2(g_m), armijo=count, alpha_lambda=a_l, alpha_mu=a_m,
-                       wall_s=time.perf_counter() - t0)
+                       wall_s=time.perf_counter() - t0, **rec_extra)
             hist.append(rec)
             if log:
                 log(rec)
@@ -276,3 +304,10 @@ class DeviceBackend:
     def gradient(self, g_l, g_m):
         self.s.adjoint_gradient(None, to_host=False)
         self.s.gradient_device(self._p(g_l), self._p(g_m))
+
+    def illumination(self):
+        """Source illumination of the stored nodes of the last forward (host array)."""
+        import ctypes as C
+        out = self.torch.zeros(self.s.nstore // 3, dtype=self.torch.float64, device=self.dev)
+        self._ck(self.L.hrn_illumination(self.h, C.c_void_p(self._p(out))))
+        return out.cpu().numpy()

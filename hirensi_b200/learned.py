@@ -1,0 +1,331 @@
+"""Learned gradient preconditioner of the inversion.
+
+A small 3-D CNN looks at the gradient, the source illumination and the current
+shear-wave speed on the regular-domain node lattice, and returns a positive
+diagonal scale D for each of the lambda and mu gradients.  The inversion tries
+the scaled steepest-descent direction -D * g first.  Its Armijo line search on
+the true misfit accepts it, or the iteration falls back to the plain L-BFGS
+direction (``hirensi_b200.inversion.FWI``).
+
+* Network: four 3x3x3 convolutions (4 -> 16 -> 16 -> 16 -> 2 channels, ReLU
+  between), BF16 weights and activations with FP32 accumulation, run by the
+  library's own kernels (hrn_cnn_conv3d_forward / _backward).  D = exp(clip(z, -4, 4)).
+* Loss of one sample: sum over lambda, mu of 1 - cos^2(D * q, dm), where q = -g
+  is the scaled gradient the inversion steps along and dm = m_true - m.  It is
+  scale-invariant, because the inversion caps the step length itself.
+* Data: seeded random layered models with an anomaly, whose gradients the
+  library computes.  Samples come from the starting model and from the iterates
+  of a short plain inversion (its accepted L-BFGS steps).
+* Training: Adam on FP32 master weights, gradients from the backward kernels.
+
+The voxel grid is the node lattice of the regular domain of a box mesh
+((2nx+1) x (2ny+1) x (2nz+1)): one voxel per stored node.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import dataclasses
+
+import numpy as np
+
+CH = (4, 16, 16, 16, 2)       # channels of the five activations
+ZCLIP = 4.0
+
+
+# ---------------------------------------------------------------------------
+# BF16 <-> FP32 on the host (round to nearest even, as __float2bfloat16_rn)
+
+def to_bf16_bits(a: np.ndarray) -> np.ndarray:
+    f = np.ascontiguousarray(a, dtype=np.float32)
+    b = f.view(np.uint32).astype(np.uint64)
+    r = (b + 0x7FFF + ((b >> 16) & 1)) >> 16
+    return r.astype(np.uint16)
+
+
+def from_bf16_bits(h: np.ndarray) -> np.ndarray:
+    return (np.asarray(h, dtype=np.uint32) << 16).view(np.float32)
+
+
+def round_bf16(a: np.ndarray) -> np.ndarray:
+    return from_bf16_bits(to_bf16_bits(a)).astype(np.float64)
+
+
+# ---------------------------------------------------------------------------
+# reference convolution (numpy, float64 on BF16-rounded inputs): the oracle of
+# the device kernels
+
+def _shift(x: np.ndarray, dz: int, dy: int, dx: int) -> np.ndarray:
+    """x[..., z + dz, y + dy, x + dx] with zeros outside."""
+    out = np.zeros_like(x)
+    nz, ny, nx = x.shape[-3:]
+
+    def sl(d, n):
+        return slice(max(0, -d), n - max(0, d)), slice(max(0, d), n - max(0, -d))
+
+    (oz, iz), (oy, iy), (ox, ix) = sl(dz, nz), sl(dy, ny), sl(dx, nx)
+    out[..., oz, oy, ox] = x[..., iz, iy, ix]
+    return out
+
+
+def conv_ref(x, w, b, relu):
+    """x [cin, nz, ny, nx], w [cout, cin, 27], b [cout] -> y [cout, nz, ny, nx]."""
+    cout = w.shape[0]
+    y = np.zeros((cout,) + x.shape[1:])
+    for k in range(27):
+        xs = _shift(x, k // 9 - 1, (k // 3) % 3 - 1, k % 3 - 1)
+        y += np.einsum("oc,czyx->ozyx", w[:, :, k], xs)
+    y += b[:, None, None, None]
+    return np.maximum(y, 0.0) if relu else y
+
+
+def conv_ref_backward(x, w, y, relu, gy):
+    gz = gy * (y > 0) if relu else gy
+    gx = np.zeros_like(x)
+    gw = np.zeros_like(w)
+    for k in range(27):
+        dz, dy, dx = k // 9 - 1, (k // 3) % 3 - 1, k % 3 - 1
+        xs = _shift(x, dz, dy, dx)
+        gw[:, :, k] = np.einsum("ozyx,czyx->oc", gz, xs)
+        gx += _shift(np.einsum("oc,ozyx->czyx", w[:, :, k], gz), -dz, -dy, -dx)
+    return gx, gw, gz.sum(axis=(1, 2, 3))
+
+
+# ---------------------------------------------------------------------------
+# lattice of the regular domain
+
+@dataclasses.dataclass
+class Lattice:
+    shape: tuple          # (nz, ny, nx) voxels
+    store_to_voxel: np.ndarray   # [nstore/3] voxel of each stored node (history order)
+    store_nodes: np.ndarray      # [nstore/3] node id of each stored node
+
+    @staticmethod
+    def of(mesh) -> "Lattice":
+        nodes = np.asarray(mesh.store_nodes)
+        x = mesh.xyz[nodes]
+        s = 0.5 * mesh.h
+        lo = x.min(axis=0)
+        idx = np.rint((x - lo) / s).astype(np.int64)
+        nx, ny, nz = (idx.max(axis=0) + 1).tolist()
+        vox = (idx[:, 2] * ny + idx[:, 1]) * nx + idx[:, 0]
+        if np.unique(vox).size != vox.size or vox.size != nx * ny * nz:
+            raise ValueError("the stored nodes do not fill a lattice")
+        return Lattice((nz, ny, nx), vox, nodes)
+
+    def to_grid(self, node_values: np.ndarray) -> np.ndarray:
+        g = np.zeros(int(np.prod(self.shape)))
+        g[self.store_to_voxel] = node_values[self.store_nodes]
+        return g.reshape(self.shape)
+
+    def from_grid(self, grid: np.ndarray, nj: int) -> np.ndarray:
+        out = np.zeros(nj)
+        out[self.store_nodes] = np.asarray(grid).reshape(-1)[self.store_to_voxel]
+        return out
+
+
+def features(lat: Lattice, g_l, g_m, illum_store, vs) -> np.ndarray:
+    """Input channels [4, nz, ny, nx]: the two gradients scaled to unit max, the log
+    illumination standardized, the shear-wave speed / 400."""
+    def unit(v):
+        m = np.abs(v).max()
+        return v / m if m > 0 else v
+
+    il = np.zeros(int(np.prod(lat.shape)))
+    il[lat.store_to_voxel] = np.log(np.asarray(illum_store) + 1e-300 + np.max(illum_store) * 1e-12)
+    il = (il - il.mean()) / (il.std() + 1e-12)
+    return np.stack([unit(lat.to_grid(g_l)), unit(lat.to_grid(g_m)), il.reshape(lat.shape), lat.to_grid(vs) / 400.0])
+
+
+def cosine_loss(a: np.ndarray, t: np.ndarray):
+    """L = 1 - cos^2(a, t) and dL/da."""
+    at = float(a.ravel() @ t.ravel())
+    aa = float(a.ravel() @ a.ravel())
+    tt = float(t.ravel() @ t.ravel())
+    if aa == 0.0 or tt == 0.0:
+        return 1.0, np.zeros_like(a)
+    L = 1.0 - at * at / (aa * tt)
+    grad = -2.0 * at / (aa * tt) * (t - (at / aa) * a)
+    return L, grad
+
+
+# ---------------------------------------------------------------------------
+# the network on the device kernels
+
+class Net:
+    def __init__(self, seed: int = 0, weights: dict | None = None):
+        rng = np.random.default_rng(seed)
+        self.w, self.b = [], []
+        for i in range(4):
+            cin, cout = CH[i], CH[i + 1]
+            std = np.sqrt(2.0 / (cin * 27)) * (0.1 if i == 3 else 1.0)
+            self.w.append(rng.standard_normal((cout, cin, 27)).astype(np.float32) * np.float32(std))
+            self.b.append(np.zeros(cout, dtype=np.float32))
+        if weights is not None:
+            self.w = [np.asarray(weights[f"w{i}"], dtype=np.float32) for i in range(4)]
+            self.b = [np.asarray(weights[f"b{i}"], dtype=np.float32) for i in range(4)]
+
+    def state(self) -> dict:
+        d = {f"w{i}": self.w[i] for i in range(4)}
+        d.update({f"b{i}": self.b[i] for i in range(4)})
+        return d
+
+    def save(self, path: str):
+        np.savez(path, **self.state())
+
+    @staticmethod
+    def load(path: str) -> "Net":
+        with np.load(path) as d:
+            return Net(weights={k: d[k] for k in d.files})
+
+
+class DeviceNet:
+    """Forward and backward passes of a Net through libhirensi_b200.so."""
+
+    def __init__(self, net: Net, shape: tuple, device=None):
+        import torch
+        from . import capi
+        self.torch = torch
+        self.L = capi.load()
+        self.net = net
+        self.shape = shape
+        self.dev = device or torch.device("cuda", torch.cuda.current_device())
+        self.stream = torch.cuda.current_stream(self.dev).cuda_stream
+        V = int(np.prod(shape))
+        self.V = V
+        self.act = [torch.zeros(c * V, dtype=torch.int16, device=self.dev) for c in CH]   # BF16 bits
+        self.sync_weights()
+
+    def _ck(self, rc):
+        if rc != 0:
+            raise RuntimeError(f"hirensi_b200 CNN kernel error {rc}")
+
+    def sync_weights(self):
+        t = self.torch
+        self.wd = [t.from_numpy(to_bf16_bits(w).view(np.int16)).to(self.dev) for w in self.net.w]
+        self.bd = [t.from_numpy(b).to(self.dev) for b in self.net.b]
+
+    def forward(self, x: np.ndarray) -> np.ndarray:
+        """x [4, nz, ny, nx] -> z [2, nz, ny, nx] (the network's last activation)."""
+        t = self.torch
+        nz, ny, nx = self.shape
+        self.act[0].copy_(t.from_numpy(to_bf16_bits(x).view(np.int16).ravel()))
+        for i in range(4):
+            self._ck(self.L.hrn_cnn_conv3d_forward(CH[i], CH[i + 1], nz, ny, nx, C.c_void_p(self.act[i].data_ptr()),
+                                                   C.c_void_p(self.wd[i].data_ptr()), C.c_void_p(self.bd[i].data_ptr()),
+                                                   int(i < 3), C.c_void_p(self.act[i + 1].data_ptr()), C.c_void_p(self.stream)))
+        z = self.act[4].cpu().numpy().view(np.uint16)
+        return from_bf16_bits(z).astype(np.float64).reshape((CH[4],) + self.shape)
+
+    def backward(self, gz: np.ndarray):
+        """Weight and bias gradients for dL/dz = gz (after a forward of the same input)."""
+        t = self.torch
+        nz, ny, nx = self.shape
+        gy = t.from_numpy(np.ascontiguousarray(gz, dtype=np.float32).ravel()).to(self.dev)
+        gws, gbs = [None] * 4, [None] * 4
+        for i in range(3, -1, -1):
+            gw = t.zeros(CH[i + 1] * CH[i] * 27, dtype=t.float32, device=self.dev)
+            gb = t.zeros(CH[i + 1], dtype=t.float32, device=self.dev)
+            gx = t.zeros(CH[i] * self.V, dtype=t.float32, device=self.dev) if i > 0 else None
+            self._ck(self.L.hrn_cnn_conv3d_backward(CH[i], CH[i + 1], nz, ny, nx, C.c_void_p(self.act[i].data_ptr()),
+                                                    C.c_void_p(self.wd[i].data_ptr()), C.c_void_p(self.act[i + 1].data_ptr()),
+                                                    int(i < 3), C.c_void_p(gy.data_ptr()),
+                                                    C.c_void_p(gx.data_ptr() if gx is not None else 0),
+                                                    C.c_void_p(gw.data_ptr()), C.c_void_p(gb.data_ptr()), C.c_void_p(self.stream)))
+            gws[i] = gw.cpu().numpy().reshape(CH[i + 1], CH[i], 27)
+            gbs[i] = gb.cpu().numpy()
+            gy = gx
+        return gws, gbs
+
+
+def scale_from_z(z: np.ndarray) -> np.ndarray:
+    return np.exp(np.clip(z, -ZCLIP, ZCLIP))
+
+
+def sample_loss(dnet: DeviceNet, x, q, dm):
+    """Loss of one sample and its gradients.  q, dm: [2, nz, ny, nx]."""
+    z = dnet.forward(x)
+    D = scale_from_z(z)
+    L = 0.0
+    gz = np.zeros_like(z)
+    for c in range(2):
+        a = D[c] * q[c]
+        Lc, ga = cosine_loss(a, dm[c])
+        L += Lc
+        inside = np.abs(z[c]) < ZCLIP
+        gz[c] = ga * a * inside          # d a / d z = a inside the clip
+    gws, gbs = dnet.backward(gz)
+    return L, gws, gbs
+
+
+class Adam:
+    def __init__(self, params, lr=1e-3, b1=0.9, b2=0.999, eps=1e-8):
+        self.p, self.lr, self.b1, self.b2, self.eps = params, lr, b1, b2, eps
+        self.m = [np.zeros_like(x) for x in params]
+        self.v = [np.zeros_like(x) for x in params]
+        self.t = 0
+
+    def step(self, grads):
+        self.t += 1
+        for i, (p, g) in enumerate(zip(self.p, grads)):
+            self.m[i] = self.b1 * self.m[i] + (1 - self.b1) * g
+            self.v[i] = self.b2 * self.v[i] + (1 - self.b2) * g * g
+            mh = self.m[i] / (1 - self.b1 ** self.t)
+            vh = self.v[i] / (1 - self.b2 ** self.t)
+            p -= (self.lr * mh / (np.sqrt(vh) + self.eps)).astype(p.dtype)
+
+
+def train(dnet: DeviceNet, samples, epochs: int = 40, lr: float = 2e-3, log=None):
+    """samples: list of (x, q, dm).  Full-batch Adam; returns the loss history."""
+    net = dnet.net
+    opt = Adam(net.w + net.b, lr=lr)
+    hist = []
+    for ep in range(epochs):
+        tot = 0.0
+        gw = [np.zeros_like(w) for w in net.w]
+        gb = [np.zeros_like(b) for b in net.b]
+        for x, q, dm in samples:
+            L, gws, gbs = sample_loss(dnet, x, q, dm)
+            tot += L
+            for i in range(4):
+                gw[i] += gws[i] / len(samples)
+                gb[i] += gbs[i] / len(samples)
+        opt.step(gw + gb)
+        dnet.sync_weights()
+        hist.append(tot / len(samples))
+        if log:
+            log(ep, hist[-1])
+    return hist
+
+
+def evaluate(dnet: DeviceNet, samples) -> tuple[float, float]:
+    """Mean loss of the network and of the unscaled direction (D = 1) on samples."""
+    ln, l1 = 0.0, 0.0
+    for x, q, dm in samples:
+        D = scale_from_z(dnet.forward(x))
+        for c in range(2):
+            ln += cosine_loss(D[c] * q[c], dm[c])[0]
+            l1 += cosine_loss(q[c], dm[c])[0]
+    return ln / len(samples), l1 / len(samples)
+
+
+class LearnedPreconditioner:
+    """Proposal hook of FWI: scaled steepest-descent direction from the network."""
+
+    def __init__(self, dnet: DeviceNet, mesh, rho: float):
+        self.dnet = dnet
+        self.lat = Lattice.of(mesh)
+        self.mesh = mesh
+        self.rho = rho
+
+    def direction(self, backend, g_l, g_m, lam, mu):
+        """p = -D * g (host round trip of the small grids); returns device/host vectors
+        of the backend."""
+        gl, gm = backend.host(g_l), backend.host(g_m)
+        il = backend.illumination()
+        vs = np.sqrt(np.maximum(backend.host(mu), 0.0) / self.rho)
+        x = features(self.lat, gl, gm, il, vs)
+        D = scale_from_z(self.dnet.forward(x))
+        nj = self.mesh.nj
+        pl = -self.lat.from_grid(D[0], nj) * gl
+        pm = -self.lat.from_grid(D[1], nj) * gm
+        return backend.vec(pl), backend.vec(pm)

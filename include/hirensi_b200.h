@@ -213,6 +213,29 @@ int hrn_get_variant(hrn_ctx *ctx, int32_t *forward, int32_t *adjoint);
 /* Number of kernels this context has launched since it was created. */
 int hrn_launch_count(hrn_ctx *ctx, int64_t *n);
 
+/* ---- learned gradient preconditioner ---------------------------------------
+ * No counterpart in the reference.  The inversion can ask a small 3-D CNN for a
+ * positive diagonal scale of the gradient; the line search on the true misfit
+ * accepts the scaled direction or falls back to L-BFGS. */
+
+/* Source illumination of every stored node: sum over steps, shots and x, y, z of
+ * u^2 from the forward history.  d_out: device array [nstore / 3], in the order of
+ * the history rows (needs the whole history, i.e. no checkpointing). */
+int hrn_illumination(hrn_ctx *ctx, double *d_out);
+
+/* 3x3x3 convolution with zero padding on a [channel][nz][ny][nx] grid, BF16 x, w
+ * and y, FP32 bias and accumulation: y = act(b + w * x), act = ReLU when relu != 0.
+ * w is [cout][cin][27] (tap k = 9 dz + 3 dy + dx).  At most 16 channels in and out.
+ * All pointers are device pointers; stream is a cudaStream_t or NULL. */
+int hrn_cnn_conv3d_forward(int32_t cin, int32_t cout, int32_t nz, int32_t ny, int32_t nx, const void *x,
+                           const void *w, const float *bias, int32_t relu, void *y, void *stream);
+/* Gradients of that layer from gy = dL/dy (FP32): gx = dL/dx (FP32, skipped when
+ * NULL), gw = dL/dw [cout][cin][27] and gb = dL/db [cout] (FP32, overwritten).
+ * y is the forward output (for the ReLU mask). */
+int hrn_cnn_conv3d_backward(int32_t cin, int32_t cout, int32_t nz, int32_t ny, int32_t nx, const void *x,
+                            const void *w, const void *y, int32_t relu, const float *gy, float *gx, float *gw,
+                            float *gb, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

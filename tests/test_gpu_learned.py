@@ -1,0 +1,87 @@
+"""Device kernels of the learned preconditioner against the host oracle: the BF16
+3-D convolution forward and backward (FP32 accumulation), the source illumination
+of the forward history, and a few training steps lowering the loss."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from hirensi_b200 import learned as Lr
+from problems import RHO, tiny
+
+pytestmark = pytest.mark.gpu
+
+
+def _bits(t, a):
+    return t.from_numpy(Lr.to_bf16_bits(a).view(np.int16).ravel()).cuda()
+
+
+@pytest.mark.parametrize("cin,cout,shape,relu", [(4, 16, (5, 7, 9), 1), (16, 16, (6, 5, 8), 1), (16, 2, (4, 6, 5), 0)])
+def test_conv3d_kernels_match_oracle(gpu_lib, cin, cout, shape, relu):
+    import torch
+    rng = np.random.default_rng(cin * 100 + cout)
+    x = Lr.round_bf16(rng.standard_normal((cin,) + shape))
+    w = Lr.round_bf16(rng.standard_normal((cout, cin, 27)) * 0.2)
+    b = (rng.standard_normal(cout) * 0.1).astype(np.float32).astype(np.float64)
+    V = int(np.prod(shape))
+    xd, wd = _bits(torch, x), _bits(torch, w)
+    bd = torch.from_numpy(b.astype(np.float32)).cuda()
+    yd = torch.zeros(cout * V, dtype=torch.int16, device="cuda")
+    nz, ny, nx = shape
+    rc = gpu_lib.hrn_cnn_conv3d_forward(cin, cout, nz, ny, nx, C.c_void_p(xd.data_ptr()), C.c_void_p(wd.data_ptr()),
+                                        C.c_void_p(bd.data_ptr()), relu, C.c_void_p(yd.data_ptr()), None)
+    assert rc == 0
+    y = Lr.from_bf16_bits(yd.cpu().numpy().view(np.uint16)).astype(np.float64).reshape((cout,) + shape)
+    yr = Lr.conv_ref(x, w, b, relu)
+    # BF16 output: within one rounding of the FP64 result
+    assert np.all(np.abs(y - yr) <= 2.0 ** -7 * np.abs(yr) + 1e-6)
+    gy = rng.standard_normal(y.shape)
+    gyd = torch.from_numpy(gy.astype(np.float32).ravel()).cuda()
+    gx = torch.zeros(cin * V, dtype=torch.float32, device="cuda")
+    gw = torch.zeros(cout * cin * 27, dtype=torch.float32, device="cuda")
+    gb = torch.zeros(cout, dtype=torch.float32, device="cuda")
+    rc = gpu_lib.hrn_cnn_conv3d_backward(cin, cout, nz, ny, nx, C.c_void_p(xd.data_ptr()), C.c_void_p(wd.data_ptr()),
+                                         C.c_void_p(yd.data_ptr()), relu, C.c_void_p(gyd.data_ptr()),
+                                         C.c_void_p(gx.data_ptr()), C.c_void_p(gw.data_ptr()), C.c_void_p(gb.data_ptr()), None)
+    assert rc == 0
+    gxr, gwr, gbr = Lr.conv_ref_backward(x, w, y, relu, gy.astype(np.float32).astype(np.float64))
+    rel = lambda a, r: np.linalg.norm(a.ravel() - r.ravel()) / np.linalg.norm(r.ravel())
+    assert rel(gx.cpu().numpy(), gxr) < 1e-5
+    assert rel(gw.cpu().numpy(), gwr) < 1e-5
+    assert rel(gb.cpu().numpy(), gbr) < 1e-5
+    # invalid sizes are refused without a launch
+    assert gpu_lib.hrn_cnn_conv3d_forward(17, cout, nz, ny, nx, C.c_void_p(xd.data_ptr()), C.c_void_p(wd.data_ptr()),
+                                          C.c_void_p(bd.data_ptr()), relu, C.c_void_p(yd.data_ptr()), None) == 1
+
+
+def test_illumination_matches_history(gpu_lib):
+    import torch
+    from hirensi_b200.solver import Solver
+    p = tiny(nshot=2, nstep=40)
+    with Solver("fp64") as s:
+        s.set_mesh(p["mesh"], RHO)
+        s.assemble(p["lam"], p["mu"])
+        s.set_history(p["mesh"].store_eq)
+        s.set_shots(p["nstep"], p["dt"], p["src_eq"], p["src_b"], p["ftab"])
+        s.set_receivers(p["eqdis"], p["eqdis_map"])
+        s.forward()
+        out = torch.zeros(s.nstore // 3, dtype=torch.float64, device="cuda")
+        assert gpu_lib.hrn_illumination(s.h, C.c_void_p(out.data_ptr())) == 0
+        ref = sum((s.history(k) ** 2).reshape(p["nstep"] + 1, -1, 3).sum(axis=(0, 2)) for k in range(2))
+    got = out.cpu().numpy()
+    assert ref.max() > 0
+    assert np.linalg.norm(got - ref) <= 1e-12 * np.linalg.norm(ref)
+
+
+def test_training_steps_lower_the_loss(gpu_lib):
+    rng = np.random.default_rng(3)
+    shape = (5, 7, 9)
+    dnet = Lr.DeviceNet(Lr.Net(seed=1), shape)
+    samples = []
+    for _ in range(3):
+        x = rng.standard_normal((4,) + shape)
+        q = rng.standard_normal((2,) + shape)
+        dm = q * np.exp(0.5 * x[2:4])          # a target reachable by a positive scale
+        samples.append((x, q, dm))
+    hist = Lr.train(dnet, samples, epochs=25, lr=1e-2)
+    assert hist[-1] < hist[0]
