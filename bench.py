@@ -323,13 +323,26 @@ def run_native(args, rank, world, local_rank):
             result["fwi"] = {}
             for prec in (["fp64"] if args.no_fp32 else ["fp64", "fp32"]):
                 result["fwi"][prec] = fwi_leg(prec, prob, dis, local_rank, args.fwi_iters)
+            if not args.no_fp32 and os.path.exists(PRECOND_WEIGHTS):
+                # time for FP32 stepping + the learned preconditioner to reach the
+                # misfit reduction of the plain FP64 run
+                r64 = result["fwi"]["fp64"]["misfit_reduction"]
+                fl = fwi_leg("fp32", prob, dis, local_rank, args.fwi_iters, learned=True, target=r64)
+                result["fwi"]["fp32_learned"] = fl
+                if fl["reached_target"]:
+                    result["fwi"]["time_to_fp64_misfit_speedup"] = result["fwi"]["fp64"]["wall_s"] / fl["wall_s"]
     s64.close()
     return result
 
 
-def fwi_leg(precision, prob, dis, local_rank, iters):
+PRECOND_WEIGHTS = os.path.join(ROOT, "hirensi_b200", "data", "precond_cnn_16x16x8.npz")
+
+
+def fwi_leg(precision, prob, dis, local_rank, iters, learned=False, target=None):
     """Wall time of `iters` L-BFGS iterations (memory 5) of the inversion loop from
-    the initial model, all vectors on the device; misfit reduction reached."""
+    the initial model, all vectors on the device; misfit reduction reached.  With
+    `learned`, each iteration first tries the trained CNN's scaled direction, and the
+    run stops once the misfit reduction reaches `target`."""
     import torch
     from hirensi_b200.configs import RHO
     from hirensi_b200.inversion import FWI, DeviceBackend, InversionConfig
@@ -344,18 +357,29 @@ def fwi_leg(precision, prob, dis, local_rank, iters):
     s.set_data(dis)
     cfg = InversionConfig(m_lbfgs=5, bounds_lambda=(10.0, 2000.0), bounds_mu=(10.0, 1000.0))
     backend = DeviceBackend(s, m)
+    pre = None
+    if learned:
+        from hirensi_b200.learned import DeviceNet, LearnedPreconditioner, Lattice, Net
+        pre = LearnedPreconditioner(DeviceNet(Net.load(PRECOND_WEIGHTS), Lattice.of(m).shape), m, RHO)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    hist = FWI(backend, cfg).run(prob.lam0, prob.mu0, n_iter=iters)
+    hist = FWI(backend, cfg, preconditioner=pre).run(prob.lam0, prob.mu0, n_iter=iters, target_reduction=target)
     torch.cuda.synchronize()
     wall = time.perf_counter() - t0
     J0, J = hist[0]["misfit"], hist[-1]["misfit"]
     t_half = next((h["wall_s"] for h in hist if h["misfit"] <= 0.5 * J0), None)
     s.close()
-    return {"iterations": len(hist) - 1, "wall_s": wall, "misfit_initial": J0, "misfit_final": J,
-            "misfit_reduction": 1.0 - J / J0, "time_to_50pct_reduction_s": t_half,
-            "forward_solves": sum(1 + h["armijo"] for h in hist[1:]) + 1,
-            "config": "L-BFGS memory 5, TV regularization, reference step rules, bounds lambda [10,2000] mu [10,1000]"}
+    out = {"iterations": len(hist) - 1, "wall_s": wall, "misfit_initial": J0, "misfit_final": J,
+           "misfit_reduction": 1.0 - J / J0, "time_to_50pct_reduction_s": t_half,
+           "forward_solves": sum(1 + h["armijo"] + (1 if h.get("learned") is False else 0) for h in hist[1:]) + 1,
+           "config": "L-BFGS memory 5, TV regularization, reference step rules, bounds lambda [10,2000] mu [10,1000]"}
+    if learned:
+        out["learned_steps_accepted"] = int(sum(1 for h in hist[1:] if h.get("learned")))
+        out["weights"] = os.path.relpath(PRECOND_WEIGHTS, ROOT)
+    if target is not None:
+        out["target_reduction"] = target
+        out["reached_target"] = bool(1.0 - J / J0 >= target)
+    return out
 
 
 # ---------------------------------------------------------------------------

@@ -57,7 +57,9 @@ class FWI:
         self.cfg = cfg
         self.pre = preconditioner
 
-    def run(self, lam0, mu0, n_iter: int, target_reduction: float | None = None, log=None):
+    def run(self, lam0, mu0, n_iter: int, target_reduction: float | None = None, log=None, observer=None):
+        """observer(it, lam, mu, g_l, g_m), if given, sees each iteration's scaled
+        gradient before the direction is chosen."""
         b, cfg = self.b, self.cfg
         n = b.n
         lam, mu = b.vec(lam0), b.vec(mu0)
@@ -74,6 +76,7 @@ class FWI:
         J0 = J
         hist = [dict(iter=0, misfit=J, cost=J, reg_lambda=0.0, reg_mu=0.0, g_lambda=0.0, g_mu=0.0, armijo=0,
                      wall_s=time.perf_counter() - t0)]
+        self.hist = hist   # kept up to date, also when an ArmijoFailure ends the run
         if log:
             log(hist[-1])
 
@@ -116,6 +119,8 @@ class FWI:
                 cost_rl = cost_rm = 0.0
             b.mul(g_l, img, g_l)                 # :454-455
             b.mul(g_m, img, g_m)
+            if observer is not None:
+                observer(it, lam, mu, g_l, g_m)
             if cfg.search == "LBFGS":
                 b.lbfgs_direction(it, cfg.iter_begin, g_l, g_m, g_l_pre, g_m_pre, lam, mu, lam_pre, mu_pre, p_l, p_m)
             else:

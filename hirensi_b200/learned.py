@@ -329,3 +329,171 @@ class LearnedPreconditioner:
         pl = -self.lat.from_grid(D[0], nj) * gl
         pm = -self.lat.from_grid(D[1], nj) * gm
         return backend.vec(pl), backend.vec(pm)
+
+
+# ---------------------------------------------------------------------------
+# training data from the solver, training, evaluation
+
+def random_true_model(prob, rng):
+    """A model of the inversion configuration's distribution: three layers with
+    Vs 200 / 300 / 400 m/s (each +-10 %, interfaces +-2 m) and a Gaussian Vs anomaly
+    of +-20..40 % (radius 3..7 m) at a random position in the regular domain."""
+    from .configs import extend_into_pml, layered_vs, vs_to_lame
+    m = prob.mesh
+    vs_l = np.array([200.0, 300.0, 400.0]) * (1.0 + rng.uniform(-0.1, 0.1, 3))
+    vs = layered_vs(m, tuple(vs_l), (-7.5 + rng.uniform(-2, 2), -15.0 + rng.uniform(-2, 2)))
+    (x0, x1), (y0, y1), (z0, _) = m.rd_box
+    c = np.array([rng.uniform(0.7 * x0, 0.7 * x1), rng.uniform(0.7 * y0, 0.7 * y1), rng.uniform(0.8 * z0, 0.2 * z0)])
+    r = rng.uniform(3.0, 7.0)
+    amp = rng.choice([-1.0, 1.0]) * rng.uniform(0.2, 0.4)
+    d2 = ((m.xyz - c) ** 2).sum(axis=1)
+    vs = extend_into_pml(m, vs * (1.0 + amp * np.exp(-d2 / (r * r))))
+    return vs_to_lame(vs)
+
+
+class _Runner:
+    """One solver + device backend for many models of one configuration."""
+
+    def __init__(self, prob, precision="fp32"):
+        import torch
+        from .configs import RHO
+        from .inversion import DeviceBackend
+        from .solver import Solver
+        self.torch = torch
+        self.prob = prob
+        m = prob.mesh
+        s = Solver(precision)
+        s.set_mesh(m, RHO)
+        s.assemble(prob.lam0, prob.mu0)
+        s.set_history(m.store_eq)
+        s.set_shots(prob.nstep, prob.dt, prob.src_eq, prob.src_b, prob.ftab)
+        s.set_receivers(prob.eqdis, prob.eqdis_map)
+        self.s = s
+        self.b = DeviceBackend(s, m)
+        self.lat = Lattice.of(m)
+        self.rho = RHO
+
+    def set_true(self, lam_t, mu_t):
+        self.s.assemble(lam_t, mu_t)
+        self.s.forward()
+        dis = self.s.traces()
+        self.dis_dev = self.torch.from_numpy(dis).cuda()
+        self.s.set_data(device_ptr=self.dis_dev.data_ptr())
+
+    def fwi(self, n_iter, cfg=None, preconditioner=None, observer=None, target_reduction=None):
+        from .inversion import FWI, ArmijoFailure
+        cfg = cfg or default_inversion_config()
+        f = FWI(self.b, cfg, preconditioner=preconditioner)
+        try:
+            f.run(self.prob.lam0, self.prob.mu0, n_iter=n_iter, observer=observer, target_reduction=target_reduction)
+        except ArmijoFailure:
+            pass   # the iterations done so far stand
+        return f.hist
+
+
+def default_inversion_config():
+    from .inversion import InversionConfig
+    return InversionConfig(m_lbfgs=5, bounds_lambda=(10.0, 2000.0), bounds_mu=(10.0, 1000.0))
+
+
+def generate_samples(runner: _Runner, seeds, iters: int = 3, log=None):
+    """(x, q, dm) of the first `iters` iterations of a plain inversion of each seeded model."""
+    out = []
+    nj = runner.prob.mesh.nj
+    for sd in seeds:
+        rng = np.random.default_rng(int(sd))
+        lam_t, mu_t = random_true_model(runner.prob, rng)
+        runner.set_true(lam_t, mu_t)
+
+        def obs(it, lam, mu, g_l, g_m):
+            b = runner.b
+            gl, gm = b.host(g_l), b.host(g_m)
+            lh, mh = b.host(lam), b.host(mu)
+            vs = np.sqrt(np.maximum(mh, 0.0) / runner.rho)
+            x = features(runner.lat, gl, gm, b.illumination(), vs)
+            q = np.stack([runner.lat.to_grid(-gl), runner.lat.to_grid(-gm)])
+            dm = np.stack([runner.lat.to_grid(lam_t - lh), runner.lat.to_grid(mu_t - mh)])
+            out.append((x, q, dm))
+
+        runner.fwi(iters, observer=obs)
+        if log:
+            log(f"model seed {sd}: {len(out)} samples")
+    return out
+
+
+class UnitScale:
+    """The proposal with D = 1 (the scaled gradient itself): the ablation of the network."""
+
+    def direction(self, backend, g_l, g_m, lam, mu):
+        return backend.vec(-backend.host(g_l)), backend.vec(-backend.host(g_m))
+
+
+def fwi_gain(runner: _Runner, dnet: DeviceNet, seeds, n_iter: int = 10):
+    """Misfit reduction and wall time of n_iter iterations with and without the
+    network on each seeded model."""
+    rows = []
+    pre = LearnedPreconditioner(dnet, runner.prob.mesh, runner.rho)
+    for sd in seeds:
+        rng = np.random.default_rng(int(sd))
+        lam_t, mu_t = random_true_model(runner.prob, rng)
+        runner.set_true(lam_t, mu_t)
+        h0 = runner.fwi(n_iter)
+        h1 = runner.fwi(n_iter, preconditioner=pre)
+        h2 = runner.fwi(n_iter, preconditioner=UnitScale())
+        rows.append({"seed": int(sd), "plain_reduction": 1.0 - h0[-1]["misfit"] / h0[0]["misfit"],
+                     "learned_reduction": 1.0 - h1[-1]["misfit"] / h1[0]["misfit"],
+                     "unit_scale_reduction": 1.0 - h2[-1]["misfit"] / h2[0]["misfit"],
+                     "plain_s": h0[-1]["wall_s"], "learned_s": h1[-1]["wall_s"], "unit_scale_s": h2[-1]["wall_s"],
+                     "plain_iters": len(h0) - 1, "learned_iters": len(h1) - 1,
+                     "learned_accepted": int(sum(1 for h in h1[1:] if h.get("learned"))),
+                     "unit_scale_accepted": int(sum(1 for h in h2[1:] if h.get("learned")))})
+    return rows
+
+
+def main(argv=None):
+    import argparse
+    import json
+    import time
+    import torch
+    from .configs import inversion_config
+    ap = argparse.ArgumentParser(description="train the learned gradient preconditioner on solver-generated data")
+    ap.add_argument("--out", required=True, help="weights file (.npz); a .json summary is written beside it")
+    ap.add_argument("--models", type=int, default=48)
+    ap.add_argument("--eval-models", type=int, default=6)
+    ap.add_argument("--iters", type=int, default=3)
+    ap.add_argument("--epochs", type=int, default=60)
+    ap.add_argument("--lr", type=float, default=2e-3)
+    ap.add_argument("--nstep", type=int, default=2000)
+    ap.add_argument("--fwi-iters", type=int, default=10)
+    ap.add_argument("--eval-only", help="skip training: evaluate these weights")
+    a = ap.parse_args(argv)
+    t0 = time.time()
+    prob = inversion_config(nstep=a.nstep)
+    runner = _Runner(prob, "fp32")
+    if a.eval_only:
+        dnet = DeviceNet(Net.load(a.eval_only), runner.lat.shape)
+        for g in fwi_gain(runner, dnet, range(5000, 5000 + a.eval_models), a.fwi_iters):
+            print(g, flush=True)
+        return
+    train_s = generate_samples(runner, range(1000, 1000 + a.models), a.iters)
+    eval_s = generate_samples(runner, range(5000, 5000 + a.eval_models), a.iters)
+    t_data = time.time() - t0
+    dnet = DeviceNet(Net(seed=0), runner.lat.shape)
+    hist = train(dnet, train_s, epochs=a.epochs, lr=a.lr, log=lambda ep, L: print(f"epoch {ep} loss {L:.4f}", flush=True))
+    t_train = time.time() - t0 - t_data
+    ev_net, ev_one = evaluate(dnet, eval_s)
+    dnet.net.save(a.out)
+    gains = fwi_gain(runner, dnet, range(5000, 5000 + a.eval_models), a.fwi_iters)
+    summary = {"train_samples": len(train_s), "eval_samples": len(eval_s), "epochs": a.epochs,
+               "loss_first_epoch": hist[0], "loss_last_epoch": hist[-1], "eval_loss_network": ev_net,
+               "eval_loss_unscaled_gradient": ev_one, "fwi": gains, "data_s": t_data, "train_s": t_train,
+               "nstep": a.nstep, "shape": list(runner.lat.shape)}
+    with open(a.out.replace(".npz", ".json"), "w") as f:
+        json.dump(summary, f, indent=1)
+    print(json.dumps({k: v for k, v in summary.items() if k != "fwi"}), flush=True)
+    for g in gains:
+        print(g, flush=True)
+
+
+if __name__ == "__main__":
+    main()

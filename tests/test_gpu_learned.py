@@ -85,3 +85,19 @@ def test_training_steps_lower_the_loss(gpu_lib):
         samples.append((x, q, dm))
     hist = Lr.train(dnet, samples, epochs=25, lr=1e-2)
     assert hist[-1] < hist[0]
+
+
+def test_trained_network_beats_plain_and_unit_scale_on_held_out_models(gpu_lib):
+    import os
+    from hirensi_b200.configs import inversion_config
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    weights = os.path.join(root, "hirensi_b200", "data", "precond_cnn_16x16x8.npz")
+    runner = Lr._Runner(inversion_config(nstep=2000), "fp32")
+    dnet = Lr.DeviceNet(Lr.Net.load(weights), runner.lat.shape)
+    rows = Lr.fwi_gain(runner, dnet, [5000, 5001], n_iter=5)
+    for r in rows:
+        # held-out seeds (training used 1000..1047): the network's direction must do
+        # clearly better than the plain L-BFGS path and than the unscaled gradient
+        assert r["learned_reduction"] > 2.0 * r["plain_reduction"]
+        assert r["learned_reduction"] > 2.0 * r["unit_scale_reduction"]
+        assert r["learned_accepted"] >= 3
