@@ -14,7 +14,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT_DIR = os.path.join(HERE, "_build")
 LIB = os.path.join(OUT_DIR, "libhirensi_b200.so")
-SOURCES = ["hrn_capi.cu", "hrn_step.cu", "hrn_assemble.cu", "hrn_inv.cu", "hrn_noalloc.cu", "hrn_elem.cu", "hrn_cnn.cu"]
+SOURCES = ["hrn_capi.cu", "hrn_step.cu", "hrn_assemble.cu", "hrn_inv.cu", "hrn_noalloc.cu", "hrn_elem.cu", "hrn_cnn.cu", "hrn_gtile.cu"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr", "-Xptxas", "-O3"]

@@ -113,6 +113,7 @@ static int install_pattern(hrn_ctx *c, int32_t neq, std::vector<int32_t> &rowptr
     c->h_rowptr.swap(rowptr);
     c->h_colx.swap(colx);
     c->have_pattern = true;
+    c->gt[0].built = c->gt[1].built = false;
     return 0;
 }
 
@@ -690,10 +691,10 @@ int hrn_set_variant(hrn_ctx *c, int32_t forward, int32_t adjoint)
     if (!c) return HRN_EARG;
     auto ok = [](int v) {
         return v == 0 || v == 40 || v == 80 || v == 160 || v == 41 || v == 81 || v == 161 || v == 42 || v == 43 || v == 82 ||
-               v == 83 || (v >= 90 && v <= 95) || (v >= 100 && v <= 105);
+               v == 83 || hrn::is_gt_variant(v) || (v >= 90 && v <= 95) || (v >= 100 && v <= 105);
     };
     if (!ok(forward) || !ok(adjoint))
-        return set_error(c, HRN_EARG, "variant must be 0 (tune), lanes*10 + mat + tiled (lanes 4/8/16, mat 0/1, tiled 0/2; "
+        return set_error(c, HRN_EARG, "variant must be 0 (tune), lanes*10 + mat + tiled (lanes 4/8/16, mat 0/1, tiled 0/2/4; "
                                       "tiled only with lanes 4/8) or 90-95 / 100-105 (matrix-free with materialized / rebuilt stage inputs: "
                                       "slots even, atomics odd; 1, 2, 4 shots per thread)");
     c->lanes_f = forward;

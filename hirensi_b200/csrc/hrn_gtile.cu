@@ -1,0 +1,568 @@
+// hrn_gtile.cu -- RK4 stage kernel over spatially compact row tiles whose
+// gathered stage inputs are staged in shared memory (variants 44, 45, 84, 85).
+//
+// The row-parallel stage kernel gathers one row record ([S] shots of the stage
+// input of the entry's matrix) per stored entry: about 18 gathers per row on the
+// 27-node meshes.  Here the rows are cut into tiles of nodes that lie close
+// together (nodes along a Morton curve of their coordinates when the mesh is
+// known, consecutive rows otherwise), and a tile needs only about 8 distinct
+// (matrix, column) records per row.  One CTA per tile:
+//   1. one thread starts 1-D bulk copies of the tile's entry slab (values and
+//      16-bit positions in the staged set) into shared memory;
+//   2. meanwhile the threads load the tile's rows with their source slots and
+//      history positions, and the tile's distinct records, ascending, into shared
+//      memory (asynchronous 16-byte copies when the stage inputs are materialized);
+//   3. after a bounded wait for the bulk copies, G lanes per row sum the row's
+//      entries from shared memory;
+//   4. one thread per row finishes it as the other stage kernels do (source,
+//      history, kb or the next-stage inputs, or the RK4 update).
+// Entries keep their order within a row and the lane split of the row-parallel
+// kernel, so the row sums equal that kernel's bit for bit.
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <algorithm>
+#include <numeric>
+#include <vector>
+
+#include "hrn_internal.h"
+#include "hrn_stage.cuh"
+
+namespace hrn {
+
+#ifndef HRN_GT_BUDGET_KB
+#define HRN_GT_BUDGET_KB 36    // shared memory per tile: up to six CTAs per SM
+#endif
+#ifndef HRN_GT_ROWS
+#define HRN_GT_ROWS 64         // rows per tile before halving to fit the budget
+#endif
+
+#ifndef HRN_GT_THREADS
+#define HRN_GT_THREADS 128
+#endif
+
+constexpr int kGtThreads = HRN_GT_THREADS;
+constexpr size_t kGtBudget = size_t(HRN_GT_BUDGET_KB) * 1024;
+constexpr int kGtRows = HRN_GT_ROWS;
+
+template <typename T>
+struct GtArgs {
+    const int4 *__restrict__ tinfo;     // [ntiles][2]
+    const int32_t *__restrict__ row;
+    const int32_t *__restrict__ ent;
+    const uint32_t *__restrict__ ukey;
+    const uint16_t *__restrict__ lidx;
+    const T *__restrict__ val;
+    int *__restrict__ err;
+};
+
+__host__ __device__ constexpr size_t a16(size_t x) { return (x + 15) & ~size_t(15); }
+
+// shared-memory footprint of a tile: barrier, four row arrays, row sums, entry slab, records
+__host__ __device__ constexpr size_t gt_footprint(int nrows, int nent_pad, int nu, size_t elem, size_t rec)
+{
+    return 16 + 4 * a16(size_t(nrows) * 4) + a16(size_t(nrows) * rec) + a16(size_t(nent_pad) * 2) +
+           a16(size_t(nent_pad) * elem) + size_t(nu) * rec;
+}
+
+__device__ __forceinline__ void cp_async16(void *dst, const void *src)
+{
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+}
+
+template <typename T, int S>
+__device__ __forceinline__ void sts_rec(T *d, const T (&v)[S])
+{
+    if constexpr (sizeof(T) == 8 && S % 2 == 0) {
+#pragma unroll
+        for (int s = 0; s < S; s += 2) reinterpret_cast<double2 *>(d)[s / 2] = make_double2(v[s], v[s + 1]);
+    } else if constexpr (sizeof(T) == 4 && S % 4 == 0) {
+#pragma unroll
+        for (int s = 0; s < S; s += 4) reinterpret_cast<float4 *>(d)[s / 4] = make_float4(v[s], v[s + 1], v[s + 2], v[s + 3]);
+    } else if constexpr (sizeof(T) == 4 && S % 2 == 0) {
+#pragma unroll
+        for (int s = 0; s < S; s += 2) reinterpret_cast<float2 *>(d)[s / 2] = make_float2(v[s], v[s + 1]);
+    } else {
+#pragma unroll
+        for (int s = 0; s < S; ++s) d[s] = v[s];
+    }
+}
+
+template <typename T, int S>
+__device__ __forceinline__ void lds_rec(const T *p, T (&o)[S])
+{
+    if constexpr (sizeof(T) == 8 && S % 2 == 0) {
+#pragma unroll
+        for (int s = 0; s < S; s += 2) {
+            const double2 v = reinterpret_cast<const double2 *>(p)[s / 2];
+            o[s] = v.x;
+            o[s + 1] = v.y;
+        }
+    } else if constexpr (sizeof(T) == 4 && S % 4 == 0) {
+#pragma unroll
+        for (int s = 0; s < S; s += 4) {
+            const float4 v = reinterpret_cast<const float4 *>(p)[s / 4];
+            o[s] = v.x; o[s + 1] = v.y; o[s + 2] = v.z; o[s + 3] = v.w;
+        }
+    } else if constexpr (sizeof(T) == 4 && S % 2 == 0) {
+#pragma unroll
+        for (int s = 0; s < S; s += 2) {
+            const float2 v = reinterpret_cast<const float2 *>(p)[s / 2];
+            o[s] = v.x; o[s + 1] = v.y;
+        }
+    } else {
+#pragma unroll
+        for (int s = 0; s < S; ++s) o[s] = p[s];
+    }
+}
+
+// Stage input of matrix TAG at row j (same values as the gathers of rk4_stage).
+template <typename T, int S, int STAGE, int MAT>
+__device__ __forceinline__ void staged_input(const StageArgs<T> &a, uint32_t key, T (&v)[S])
+{
+    const int tag = int(key >> kTagBits);
+    const size_t j = size_t(key & kColMask);
+    if constexpr (MAT == 1 && STAGE > 1) {
+        const T *src = tag == 0 ? a.in_m : (tag == 1 ? a.in_t : a.in_h);
+        ldv<T, S>(src + j * S, v);
+    } else {
+        if (tag == 0) gather<T, S, STAGE, 0>(a, j, v);
+        else if (tag == 1) gather<T, S, STAGE, 1>(a, j, v);
+        else gather<T, S, STAGE, 2>(a, j, v);
+    }
+}
+
+template <typename T, int S, int STAGE, int G, int MAT>
+__global__ void __launch_bounds__(kGtThreads) rk4_stage_gt(const StageArgs<T> a, const GtArgs<T> g)
+{
+    extern __shared__ __align__(128) unsigned char gt_smem[];
+    const int4 ti0 = __ldg(g.tinfo + 2 * blockIdx.x), ti1 = __ldg(g.tinfo + 2 * blockIdx.x + 1);
+    const int row_off = ti0.x, nrows = ti0.y, ent_off = ti0.z, nent = ti0.w, u_off = ti1.x, nu = ti1.y;
+    uint64_t *bar = reinterpret_cast<uint64_t *>(gt_smem);
+    size_t off = 16;
+    int32_t *s_row = reinterpret_cast<int32_t *>(gt_smem + off); off += a16(size_t(nrows) * 4);
+    int32_t *s_ent = reinterpret_cast<int32_t *>(gt_smem + off); off += a16(size_t(nrows) * 4);
+    int32_t *s_slot = reinterpret_cast<int32_t *>(gt_smem + off); off += a16(size_t(nrows) * 4);
+    int32_t *s_pos = reinterpret_cast<int32_t *>(gt_smem + off); off += a16(size_t(nrows) * 4);
+    T *s_acc = reinterpret_cast<T *>(gt_smem + off); off += a16(size_t(nrows) * S * sizeof(T));
+    uint16_t *s_lidx = reinterpret_cast<uint16_t *>(gt_smem + off); off += a16(size_t(nent) * 2);
+    T *s_val = reinterpret_cast<T *>(gt_smem + off); off += a16(size_t(nent) * sizeof(T));
+    T *sx = reinterpret_cast<T *>(gt_smem + off);
+
+    // 1. entry slab by bulk copies (sizes and addresses are multiples of 16 bytes)
+    if (threadIdx.x == 0) {
+        mbar_init(bar, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        if (nent > 0) {
+            mbar_expect_tx(bar, uint32_t(nent) * uint32_t(2 + sizeof(T)));
+            bulk_g2s(s_lidx, g.lidx + ent_off, uint32_t(nent) * 2u, bar);
+            bulk_g2s(s_val, g.val + ent_off, uint32_t(nent) * uint32_t(sizeof(T)), bar);
+        } else {
+            asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+        }
+    }
+    // 2. rows of the tile with their source slot and history position
+    for (int r = threadIdx.x; r < nrows; r += kGtThreads) {
+        const int row = __ldg(g.row + row_off + r);
+        s_row[r] = row;
+        s_ent[r] = __ldg(g.ent + row_off + r);
+        s_slot[r] = __ldg(a.slot + row);
+        s_pos[r] = (STAGE == 1 && a.hist) ? __ldg(a.store_pos + row) : -1;
+    }
+    //    staged set, ascending keys, adjacent threads on adjacent keys
+    constexpr size_t kRec = S * sizeof(T);
+    if constexpr (MAT == 1 && STAGE > 1 && kRec % 16 == 0) {
+        // materialized inputs: asynchronous 16-byte copies straight into shared memory,
+        // eight keys per thread in flight before their copies are issued
+        for (int u = threadIdx.x; u < nu; u += 8 * kGtThreads) {
+            uint32_t key[8];
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+                const int uu = u + q * kGtThreads;
+                key[q] = uu < nu ? __ldg(g.ukey + u_off + uu) : 0u;
+            }
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+                const int uu = u + q * kGtThreads;
+                if (uu < nu) {
+                    const int tag = int(key[q] >> kTagBits);
+                    const T *src = (tag == 0 ? a.in_m : (tag == 1 ? a.in_t : a.in_h)) + size_t(key[q] & kColMask) * S;
+                    T *d = sx + size_t(uu) * S;
+#pragma unroll
+                    for (size_t b = 0; b < kRec; b += 16)
+                        cp_async16(reinterpret_cast<char *>(d) + b, reinterpret_cast<const char *>(src) + b);
+                }
+            }
+        }
+        asm volatile("cp.async.commit_group;" ::: "memory");
+        asm volatile("cp.async.wait_group 0;" ::: "memory");
+    } else {
+        // Q records per thread per trip, all loads issued before the stores
+        constexpr int Q = (kRec >= 64) ? 2 : 4;
+        for (int u = threadIdx.x; u < nu; u += Q * kGtThreads) {
+            T v[Q][S];
+#pragma unroll
+            for (int q = 0; q < Q; ++q) {
+                const int uu = u + q * kGtThreads;
+                if (uu < nu) staged_input<T, S, STAGE, MAT>(a, __ldg(g.ukey + u_off + uu), v[q]);
+            }
+#pragma unroll
+            for (int q = 0; q < Q; ++q) {
+                const int uu = u + q * kGtThreads;
+                if (uu < nu) sts_rec<T, S>(sx + size_t(uu) * S, v[q]);
+            }
+        }
+    }
+    // bounded wait for the slab; on a timeout flag the error, let the copy land (bounded) and stop
+    const bool ok = mbar_wait(bar, 0);
+    if (__syncthreads_or(!ok)) {
+        if (threadIdx.x == 0) {
+            atomicExch(g.err, 1);
+            mbar_wait(bar, 0);
+        }
+        return;
+    }
+
+    // 3. row sums, G lanes per row, everything read from shared memory
+    const int lane = threadIdx.x & (G - 1);
+    const unsigned gmask = (G == 32) ? 0xffffffffu : (((1u << G) - 1u) << ((threadIdx.x & 31) & ~(G - 1)));
+    for (int i = int(threadIdx.x) / G; i < nrows; i += kGtThreads / G) {
+        const uint32_t pe = uint32_t(s_ent[i]);
+        const int k0 = int(pe & 0xffffu), k3 = k0 + int(pe >> 16);
+        T acc[S];
+#pragma unroll
+        for (int s = 0; s < S; ++s) acc[s] = T(0);
+        for (int k = k0 + lane; k < k3; k += 4 * G) {
+#pragma unroll
+            for (int uu = 0; uu < 4; ++uu) {
+                const int kk = k + uu * G;
+                if (kk < k3) {
+                    T x[S];
+                    lds_rec<T, S>(sx + size_t(s_lidx[kk]) * S, x);
+                    const T w = s_val[kk];
+#pragma unroll
+                    for (int s = 0; s < S; ++s) acc[s] = fmaT(w, x[s], acc[s]);
+                }
+            }
+        }
+#pragma unroll
+        for (int off2 = G / 2; off2 > 0; off2 >>= 1)
+#pragma unroll
+            for (int s = 0; s < S; ++s) acc[s] += __shfl_xor_sync(gmask, acc[s], off2, G);
+        if (lane == 0) sts_rec<T, S>(s_acc + size_t(i) * S, acc);
+    }
+    __syncthreads();
+    // 4. one thread per row: source, history, kb / next-stage inputs or the RK4 update
+    for (int r = threadIdx.x; r < nrows; r += kGtThreads) {
+        T acc[S];
+        lds_rec<T, S>(s_acc + size_t(r) * S, acc);
+        finish_row_sp<T, S, STAGE, MAT>(a, s_row[r], s_slot[r], s_pos[r], acc);
+    }
+}
+
+template <typename T>
+__global__ void k_gt_values(int64_t nnz, const int32_t *__restrict__ perm, const T *__restrict__ src, T *__restrict__ dst)
+{
+    for (int64_t k = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; k < nnz; k += int64_t(gridDim.x) * blockDim.x)
+    {
+        const int32_t p = perm[k];
+        dst[k] = p >= 0 ? src[p] : T(0);
+    }
+}
+
+// ----------------------------------------------------------------------------
+// tile construction (host)
+
+static uint64_t spread3(uint32_t v)
+{
+    uint64_t r = 0;
+    for (int b = 0; b < 10; ++b) r |= uint64_t((v >> b) & 1u) << (3 * b);
+    return r;
+}
+
+// Rows in tile order, grouped by node (a group never straddles two tiles).
+// With the mesh: the equations of each node (ID order), nodes along a Morton
+// curve of their coordinates; without it, or if the mesh's ID does not number
+// the operator's rows exactly once: consecutive rows, one row per group.
+static void row_order(const hrn_ctx *c, std::vector<int32_t> &order, std::vector<int32_t> &gstart)
+{
+    const int n = c->neq;
+    order.clear();
+    gstart.clear();
+    if (c->have_mesh && c->nj > 0 && c->h_id.size() == size_t(c->nj) * 9 && c->h_xyz.size() == size_t(c->nj) * 3) {
+        double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+        for (int j = 0; j < c->nj; ++j)
+            for (int d = 0; d < 3; ++d) {
+                lo[d] = std::min(lo[d], c->h_xyz[size_t(j) * 3 + d]);
+                hi[d] = std::max(hi[d], c->h_xyz[size_t(j) * 3 + d]);
+            }
+        const double ext = std::max({hi[0] - lo[0], hi[1] - lo[1], hi[2] - lo[2], 1e-300});
+        std::vector<std::pair<uint64_t, int32_t>> key(size_t(c->nj));
+        for (int j = 0; j < c->nj; ++j) {
+            uint64_t code = 0;
+            for (int d = 0; d < 3; ++d) {
+                const double f = (c->h_xyz[size_t(j) * 3 + d] - lo[d]) / ext;
+                const uint32_t q = uint32_t(std::min(1023.0, std::max(0.0, f * 1023.999)));
+                code |= spread3(q) << d;
+            }
+            key[j] = {code, j};
+        }
+        std::sort(key.begin(), key.end());
+        std::vector<char> seen(size_t(n), 0);
+        bool ok = true;
+        for (const auto &kj : key) {
+            const int j = kj.second;
+            const size_t g0 = order.size();
+            for (int d = 0; d < 9 && ok; ++d) {
+                const int eq = c->h_id[size_t(j) * 9 + d];
+                if (eq < 0) continue;
+                if (eq >= n || seen[eq]) { ok = false; break; }
+                seen[eq] = 1;
+                order.push_back(eq);
+            }
+            if (!ok) break;
+            if (order.size() > g0) gstart.push_back(int32_t(g0));
+        }
+        if (ok && order.size() == size_t(n)) {
+            gstart.push_back(n);
+            return;
+        }
+        order.clear();
+        gstart.clear();
+    }
+    order.resize(size_t(n));
+    std::iota(order.begin(), order.end(), 0);
+    gstart.resize(size_t(n) + 1);
+    std::iota(gstart.begin(), gstart.end(), 0);
+}
+
+static int gt_build(hrn_ctx *c, int adj, size_t rec_bytes)
+{
+    GtSet &gs = c->gt[adj];
+    gs.built = false;
+    const int n = c->neq;
+    const int64_t nnz = c->nnz;
+    const size_t elem = c->elem_bytes();
+    std::vector<int32_t> rowptr;
+    std::vector<uint32_t> colx;
+    if (adj == 0) {
+        rowptr = c->h_rowptr;
+        colx = c->h_colx;
+    } else {
+        rowptr.resize(size_t(n) + 1);
+        colx.resize(size_t(nnz));
+        HRN_CUDA(c, cudaMemcpy(rowptr.data(), c->d_rowptrT.p, rowptr.size() * 4, cudaMemcpyDeviceToHost));
+        if (nnz) HRN_CUDA(c, cudaMemcpy(colx.data(), c->d_colxT.p, colx.size() * 4, cudaMemcpyDeviceToHost));
+    }
+    std::vector<int32_t> order, gstart;
+    row_order(c, order, gstart);
+    const int ngroups = int(gstart.size()) - 1;
+
+    // distinct keys and entries of the rows of groups [g0, g1)
+    std::vector<uint32_t> keys;
+    int64_t nent_range = 0;
+    auto collect = [&](int g0, int g1) {
+        keys.clear();
+        nent_range = 0;
+        for (int r = gstart[g0]; r < gstart[g1]; ++r) {
+            const int row = order[r];
+            keys.insert(keys.end(), colx.begin() + rowptr[row], colx.begin() + rowptr[row + 1]);
+            nent_range += rowptr[row + 1] - rowptr[row];
+        }
+        std::sort(keys.begin(), keys.end());
+        keys.erase(std::unique(keys.begin(), keys.end()), keys.end());
+    };
+    auto pad8 = [](int64_t x) { return (x + 7) & ~int64_t(7); };
+    std::vector<int32_t> tiles_g{0};   // group boundaries of the tiles
+    std::vector<int32_t> h_uoff{0};
+    std::vector<uint32_t> h_ukey;
+    size_t smem = 0;
+    bool fit = true;
+    // cut a range of groups into tiles: halve until the tile's footprint fits
+    std::vector<std::pair<int, int>> stack;
+    auto cut = [&](int g0, int g1) {
+        stack.assign(1, {g0, g1});
+        while (!stack.empty() && fit) {
+            const auto [a0, a1] = stack.back();
+            stack.pop_back();
+            collect(a0, a1);
+            const int nrows = gstart[a1] - gstart[a0];
+            const int64_t ne = pad8(nent_range);
+            const bool small = ne <= 65535 && keys.size() <= 65535;
+            const size_t f = small ? gt_footprint(nrows, int(ne), int(keys.size()), elem, rec_bytes) : ~size_t(0);
+            if (f > kGtBudget) {
+                if (a1 - a0 == 1) { fit = false; break; }
+                const int mid = (a0 + a1) / 2;
+                stack.push_back({mid, a1});
+                stack.push_back({a0, mid});
+                continue;
+            }
+            tiles_g.push_back(a1);
+            h_ukey.insert(h_ukey.end(), keys.begin(), keys.end());
+            h_uoff.push_back(int32_t(h_ukey.size()));
+            smem = std::max(smem, f);
+        }
+    };
+    int g = 0;
+    while (g < ngroups && fit) {
+        int g1 = g;
+        while (g1 < ngroups && (g1 == g || gstart[g1 + 1] - gstart[g] <= kGtRows)) ++g1;
+        cut(g, g1);
+        g = g1;
+    }
+    if (!fit) return set_error(c, HRN_EARG, "a node's rows need more shared memory than a staged tile holds");
+    if (int64_t(h_ukey.size()) >= (int64_t(1) << 31)) return set_error(c, HRN_EARG, "too many staged keys");
+    const int ntiles = int(tiles_g.size()) - 1;
+
+    // tile info, rows, packed entry ranges, local key positions and the value permutation
+    std::vector<int32_t> h_tinfo(size_t(ntiles) * 8, 0), h_ent(size_t(std::max(n, 1)), 0);
+    int64_t total = 0;
+    for (int t = 0; t < ntiles; ++t) {
+        int64_t ne = 0;
+        for (int r = gstart[tiles_g[t]]; r < gstart[tiles_g[t + 1]]; ++r) ne += rowptr[order[r] + 1] - rowptr[order[r]];
+        total += pad8(ne);
+    }
+    if (total >= (int64_t(1) << 31)) return set_error(c, HRN_EARG, "staged-gather tiles need fewer than 2^31 entries");
+    std::vector<uint16_t> h_lidx(size_t(std::max<int64_t>(total, 8)), 0);
+    std::vector<int32_t> h_perm(size_t(std::max<int64_t>(total, 8)), -1);
+    int64_t e = 0;
+    for (int t = 0; t < ntiles; ++t) {
+        const int ra = gstart[tiles_g[t]], rb = gstart[tiles_g[t + 1]];
+        const uint32_t *kb = h_ukey.data() + h_uoff[t], *ke = h_ukey.data() + h_uoff[t + 1];
+        const int64_t e0 = e;
+        for (int r = ra; r < rb; ++r) {
+            const int row = order[r];
+            const int cnt = rowptr[row + 1] - rowptr[row];
+            h_ent[r] = int32_t(uint32_t(e - e0) | (uint32_t(cnt) << 16));
+            for (int32_t p = rowptr[row]; p < rowptr[row + 1]; ++p, ++e) {
+                h_lidx[e] = uint16_t(std::lower_bound(kb, ke, colx[p]) - kb);
+                h_perm[e] = p;
+            }
+        }
+        e = e0 + pad8(e - e0);
+        int32_t *ti = h_tinfo.data() + size_t(t) * 8;
+        ti[0] = ra;
+        ti[1] = rb - ra;
+        ti[2] = int32_t(e0);
+        ti[3] = int32_t(e - e0);
+        ti[4] = h_uoff[t];
+        ti[5] = h_uoff[t + 1] - h_uoff[t];
+    }
+
+    HRN_CUDA(c, gs.d_tinfo.alloc(std::max<size_t>(h_tinfo.size(), 8) * 4));
+    HRN_CUDA(c, gs.d_row.alloc(std::max<size_t>(order.size(), 1) * 4));
+    HRN_CUDA(c, gs.d_ent.alloc(h_ent.size() * 4));
+    HRN_CUDA(c, gs.d_ukey.alloc(std::max<size_t>(h_ukey.size(), 1) * 4));
+    HRN_CUDA(c, gs.d_lidx.alloc(h_lidx.size() * 2));
+    HRN_CUDA(c, gs.d_perm.alloc(h_perm.size() * 4));
+    if (!h_tinfo.empty()) HRN_CUDA(c, cudaMemcpy(gs.d_tinfo.p, h_tinfo.data(), h_tinfo.size() * 4, cudaMemcpyHostToDevice));
+    if (!order.empty()) HRN_CUDA(c, cudaMemcpy(gs.d_row.p, order.data(), order.size() * 4, cudaMemcpyHostToDevice));
+    HRN_CUDA(c, cudaMemcpy(gs.d_ent.p, h_ent.data(), h_ent.size() * 4, cudaMemcpyHostToDevice));
+    if (!h_ukey.empty()) HRN_CUDA(c, cudaMemcpy(gs.d_ukey.p, h_ukey.data(), h_ukey.size() * 4, cudaMemcpyHostToDevice));
+    HRN_CUDA(c, cudaMemcpy(gs.d_lidx.p, h_lidx.data(), h_lidx.size() * 2, cudaMemcpyHostToDevice));
+    HRN_CUDA(c, cudaMemcpy(gs.d_perm.p, h_perm.data(), h_perm.size() * 4, cudaMemcpyHostToDevice));
+    gs.ntiles = ntiles;
+    gs.smem = smem;
+    gs.nu = int64_t(h_ukey.size());
+    gs.nent = total;
+    gs.rec_bytes = rec_bytes;
+    gs.val_version = -1;
+    gs.built = true;
+    return 0;
+}
+
+template <typename T>
+static int gt_values(hrn_ctx *c, int adj)
+{
+    GtSet &gs = c->gt[adj];
+    if (gs.val_version == c->val_version && gs.val_elem == sizeof(T)) return 0;
+    const int64_t ne = std::max<int64_t>(gs.nent, 8);
+    const size_t vb = size_t(ne) * sizeof(T);
+    if (gs.d_val.bytes != vb) HRN_CUDA(c, gs.d_val.alloc(vb));
+    const T *src = adj ? c->d_adj.as<T>() : c->d_fwd.as<T>();
+    const int th = 256;
+    const int blocks = int(std::min<int64_t>((ne + th - 1) / th, int64_t(c->num_sms) * 16));
+    k_gt_values<T><<<blocks, th, 0, c->stream>>>(ne, gs.d_perm.as<int32_t>(), src, gs.d_val.as<T>());
+    ++c->launches;
+    HRN_CUDA(c, cudaGetLastError());
+    gs.val_version = c->val_version;
+    gs.val_elem = sizeof(T);
+    return 0;
+}
+
+int gt_ready(hrn_ctx *c, int adj)
+{
+    if (!c->have_pattern || !c->have_operator) return set_error(c, HRN_ESTATE, "no operator");
+    if (c->nshot < 1) return set_error(c, HRN_ESTATE, "no shots");
+    const size_t rec = size_t(c->nshot) * c->elem_bytes();
+    GtSet &gs = c->gt[adj];
+    if (!gs.built || gs.rec_bytes != rec)
+        if (int rc = gt_build(c, adj, rec)) return rc;
+    return c->precision == HRN_FP64 ? gt_values<double>(c, adj) : gt_values<float>(c, adj);
+}
+
+// ----------------------------------------------------------------------------
+// launch
+
+template <typename T, int S, int STAGE, int G, int MAT>
+static void launch_gt(const StageArgs<T> &a, const GtArgs<T> &g, int ntiles, size_t smem, cudaStream_t st)
+{
+    static bool attr_set = false;
+    if (!attr_set) {
+        cudaFuncSetAttribute(rk4_stage_gt<T, S, STAGE, G, MAT>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kGtBudget));
+        attr_set = true;
+    }
+    rk4_stage_gt<T, S, STAGE, G, MAT><<<ntiles, kGtThreads, smem, st>>>(a, g);
+}
+
+template <typename T, int S, int STAGE>
+static void launch_gt_variant(const StageArgs<T> &a, const GtArgs<T> &g, int ntiles, size_t smem, int variant,
+                              cudaStream_t st)
+{
+    switch (variant) {
+    case 44: launch_gt<T, S, STAGE, 4, 0>(a, g, ntiles, smem, st); break;
+    case 45: launch_gt<T, S, STAGE, 4, 1>(a, g, ntiles, smem, st); break;
+    case 84: launch_gt<T, S, STAGE, 8, 0>(a, g, ntiles, smem, st); break;
+    default: launch_gt<T, S, STAGE, 8, 1>(a, g, ntiles, smem, st); break;
+    }
+}
+
+template <typename T, int S>
+static int gt_stage_t(hrn_ctx *c, const StageArgs<T> &a, int stage, int adj, int variant)
+{
+    const GtSet &gs = c->gt[adj];
+    if (!gs.built || gs.ntiles == 0) return 0;
+    const GtArgs<T> g{gs.d_tinfo.as<int4>(), gs.d_row.as<int32_t>(), gs.d_ent.as<int32_t>(), gs.d_ukey.as<uint32_t>(),
+                      gs.d_lidx.as<uint16_t>(), gs.d_val.as<T>(), c->d_step_err.as<int>()};
+    switch (stage) {
+    case 1: launch_gt_variant<T, S, 1>(a, g, gs.ntiles, gs.smem, variant, c->stream); break;
+    case 2: launch_gt_variant<T, S, 2>(a, g, gs.ntiles, gs.smem, variant, c->stream); break;
+    case 3: launch_gt_variant<T, S, 3>(a, g, gs.ntiles, gs.smem, variant, c->stream); break;
+    default: launch_gt_variant<T, S, 4>(a, g, gs.ntiles, gs.smem, variant, c->stream); break;
+    }
+    return 0;
+}
+
+#define HRN_GT_DISPATCH(T)                                                              \
+    switch (c->nshot) {                                                                 \
+    case 1: return gt_stage_t<T, 1>(c, *static_cast<const StageArgs<T> *>(args), stage, adj, variant); \
+    case 2: return gt_stage_t<T, 2>(c, *static_cast<const StageArgs<T> *>(args), stage, adj, variant); \
+    case 3: return gt_stage_t<T, 3>(c, *static_cast<const StageArgs<T> *>(args), stage, adj, variant); \
+    case 4: return gt_stage_t<T, 4>(c, *static_cast<const StageArgs<T> *>(args), stage, adj, variant); \
+    case 5: return gt_stage_t<T, 5>(c, *static_cast<const StageArgs<T> *>(args), stage, adj, variant); \
+    case 6: return gt_stage_t<T, 6>(c, *static_cast<const StageArgs<T> *>(args), stage, adj, variant); \
+    case 7: return gt_stage_t<T, 7>(c, *static_cast<const StageArgs<T> *>(args), stage, adj, variant); \
+    case 8: return gt_stage_t<T, 8>(c, *static_cast<const StageArgs<T> *>(args), stage, adj, variant); \
+    default: return set_error(c, HRN_EARG, "nshot out of range");                      \
+    }
+
+int gt_stage(hrn_ctx *c, const void *args, int stage, int adj, int variant)
+{
+    if (c->precision == HRN_FP64) { HRN_GT_DISPATCH(double) }
+    HRN_GT_DISPATCH(float)
+}
+
+}  // namespace hrn

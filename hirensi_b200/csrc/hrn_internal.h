@@ -42,6 +42,27 @@ constexpr int kTileEntries = 4096;     // entries per tile of the tiled stage ke
 constexpr size_t kBulkPad = 64;        // bytes past the end of bulk-copied arrays
 constexpr uint32_t kColMask = (1u << kTagBits) - 1u;
 
+// Row tiles of the staged-gather stage kernel (variants 44, 45, 84, 85) for one
+// operator direction: spatially compact sets of rows whose gathered (matrix,
+// column) pairs, entries and row data fit in one CTA's shared memory.
+struct GtSet {
+    bool built = false;
+    size_t rec_bytes = 0;       // bytes of one staged record (S values) the tiles were cut for
+    int ntiles = 0;
+    size_t smem = 0;            // largest shared-memory footprint of a tile (bytes)
+    int64_t nu = 0;             // staged records over all tiles
+    int64_t nent = 0;           // entries over all tiles, each tile padded to a multiple of 8
+    DevBuf d_tinfo;             // [ntiles][8] first tile row, rows, first entry, padded entries, first key, keys
+    DevBuf d_row;               // [neq] row of each tile row
+    DevBuf d_ent;               // [neq] first entry (relative to the tile) | entry count << 16
+    DevBuf d_ukey;              // [nu] matrix id << 30 | column, ascending within a tile
+    DevBuf d_lidx;              // [nent] uint16 position of the entry's key in its tile's set
+    DevBuf d_perm;              // [nent] int32 entry of the scaled value array (-1: padding)
+    DevBuf d_val;               // [nent] scaled values in tile order (T)
+    int64_t val_version = -1;   // value version d_val was built from
+    size_t val_elem = 0;
+};
+
 }  // namespace hrn
 
 struct hrn_ctx {
@@ -70,6 +91,8 @@ struct hrn_ctx {
     hrn::DevBuf d_step_err;                   // device flag: a bounded wait of a stage kernel timed out
     hrn::DevBuf d_raw;                        // unscaled values (FP64)
     hrn::DevBuf d_fwd, d_adj;                 // scaled forward values, transposed adjoint values (T)
+    int64_t val_version = 0;                  // incremented whenever d_fwd / d_adj are rewritten
+    hrn::GtSet gt[2];                         // staged-gather row tiles: forward, adjoint
     hrn::DevBuf d_diag_m, d_im;               // FP64 mass diagonal and its reciprocal
 
     // ---- mesh (device assembly and gradient)
@@ -193,6 +216,9 @@ int build_rd_geometry(hrn_ctx *c);
 int assemble_device(hrn_ctx *c, bool discover_pattern);
 int finalize_pattern_from_keys(hrn_ctx *c, const std::vector<uint64_t> &keys);
 int vec_reduce(hrn_ctx *c, int kind, int n, const double *x, const double *y, double *out);
+int gt_ready(hrn_ctx *c, int adj);
+int gt_stage(hrn_ctx *c, const void *stage_args, int stage, int adj, int variant);
+inline bool is_gt_variant(int v) { return v == 44 || v == 45 || v == 84 || v == 85; }
 int elem_prepare(hrn_ctx *c);
 int elem_ready(hrn_ctx *c);
 int elem_stage(hrn_ctx *c, const void *stage_args, int stage, int adj, int acc, int shots_per_thread, int mat);

@@ -74,6 +74,40 @@ __device__ __forceinline__ void stv(T *__restrict__ p, const T (&o)[S])
     }
 }
 
+// ----------------------------------------------------------------------------
+// mbarrier and 1-D bulk copies (global -> shared), with bounded waits
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) { return uint32_t(__cvta_generic_to_shared(p)); }
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                 ::"r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(bar)) : "memory");
+}
+
+// bounded wait for the phase with the given parity; false on timeout
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity)
+{
+    const uint32_t addr = smem_u32(bar);
+    for (int i = 0; i < (1 << 20); ++i) {
+        uint32_t done;
+        asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+                     : "=r"(done) : "r"(addr), "r"(parity) : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
 __device__ __forceinline__ double fmaT(double a, double b, double c) { return fma(a, b, c); }
 __device__ __forceinline__ float fmaT(float a, float b, float c) { return fmaf(a, b, c); }
 
@@ -156,12 +190,13 @@ __device__ __forceinline__ void gather(const StageArgs<T> &a, size_t j, T (&v)[S
 
 // Row epilogue: stage source, history (stage 1), kb or the next-stage inputs
 // (stages 1-3) or the RK4 update into the other state buffer (stage 4).
+// sl = the row's source slot (-1 none); pos = its history position (-1 none),
+// read only in stage 1 with a history to write.
 template <typename T, int S, int STAGE, int MAT>
-__device__ __forceinline__ void finish_row(const StageArgs<T> &a, int row, const T (&acc)[S])
+__device__ __forceinline__ void finish_row_sp(const StageArgs<T> &a, int row, int sl, int pos, const T (&acc)[S])
 {
     const size_t o = size_t(row) * S;
     T kb[S];
-    const int sl = __ldg(a.slot + row);
     if (sl >= 0) {
         T sv[S];
         ldv<T, S>(a.srcv + (size_t(STAGE - 1) * a.nslot + sl) * S, sv);
@@ -172,13 +207,10 @@ __device__ __forceinline__ void finish_row(const StageArgs<T> &a, int row, const
         for (int s = 0; s < S; ++s) kb[s] = acc[s];
     }
     if constexpr (STAGE == 1) {
-        if (a.hist) {
-            const int p = __ldg(a.store_pos + row);
-            if (p >= 0) {
-                T x2[S];
-                ldv<T, S>(a.x2 + o, x2);
-                stv<T, S>(a.hist + size_t(p) * S, x2);
-            }
+        if (a.hist && pos >= 0) {
+            T x2[S];
+            ldv<T, S>(a.x2 + o, x2);
+            stv<T, S>(a.hist + size_t(pos) * S, x2);
         }
     }
     if constexpr (STAGE < 4) {
@@ -229,6 +261,14 @@ __device__ __forceinline__ void finish_row(const StageArgs<T> &a, int row, const
         stv<T, S>(a.y2 + o, n2);
         stv<T, S>(a.y3 + o, n3);
     }
+}
+
+template <typename T, int S, int STAGE, int MAT>
+__device__ __forceinline__ void finish_row(const StageArgs<T> &a, int row, const T (&acc)[S])
+{
+    const int sl = __ldg(a.slot + row);
+    const int pos = (STAGE == 1 && a.hist) ? __ldg(a.store_pos + row) : -1;
+    finish_row_sp<T, S, STAGE, MAT>(a, row, sl, pos, acc);
 }
 
 }  // namespace hrn

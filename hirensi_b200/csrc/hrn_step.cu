@@ -106,37 +106,6 @@ constexpr size_t tile_smem_bytes()
     return 128 + 2 * (size_t(kTileE + kTileSlack) * 4 + size_t(kTileE + kTileSlack) * sizeof(T));
 }
 
-__device__ __forceinline__ uint32_t smem_u32(const void *p) { return uint32_t(__cvta_generic_to_shared(p)); }
-
-__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count)
-{
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
-}
-
-__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes)
-{
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
-}
-
-__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar)
-{
-    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
-                 ::"r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(bar)) : "memory");
-}
-
-// bounded wait for the phase with the given parity; false on timeout
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity)
-{
-    const uint32_t addr = smem_u32(bar);
-    for (int i = 0; i < (1 << 20); ++i) {
-        uint32_t done;
-        asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
-                     : "=r"(done) : "r"(addr), "r"(parity) : "memory");
-        if (done) return true;
-    }
-    return false;
-}
-
 template <typename T>
 __device__ __forceinline__ void tile_issue(const StageArgs<T> &a, const int32_t *tiles, int t, uint32_t *cb, T *vb,
                                            uint64_t *bar)
@@ -492,6 +461,7 @@ static int scale_operator_t(hrn_ctx *c)
 
 int launch_scale_operator(hrn_ctx *c)
 {
+    ++c->val_version;
     return c->precision == HRN_FP64 ? scale_operator_t<double>(c) : scale_operator_t<float>(c);
 }
 
@@ -740,6 +710,8 @@ static void launch_step(hrn_ctx *c, StageArgs<T> a, T *X, T *Y, StageTimer *tm, 
         if (is_elem_variant(lanes)) {
             const int b = lanes >= 100 ? 100 : 90;
             elem_stage(c, &a, st, adj, (lanes - b) % 2, 1 << ((lanes - b) / 2), b == 90 ? 1 : 0);
+        } else if (is_gt_variant(lanes)) {
+            gt_stage(c, &a, st, adj, lanes);
         } else {
             switch (st) {
             case 1: launch_stage<T, S, 1>(a, lanes, c->stream, ta); break;
@@ -774,6 +746,8 @@ static int autotune_lanes(hrn_ctx *c, StageArgs<T> a, T *X, T *Y, const TileArgs
     float best = 1e30f;
     int pick = 80;
     std::vector<int> cand(kVariants, kVariants + 10);
+    if (gt_ready(c, adj) == 0)
+        for (int v : {44, 45, 84, 85}) cand.push_back(v);
     if (c->op_from_mesh) {
         if (int rc = elem_ready(c)) return rc;
         for (int v : {90, 91, 92, 93, 94, 95, 100, 101, 102, 103, 104, 105})
@@ -862,6 +836,8 @@ static int forward_t(hrn_ctx *c)
     } else if (is_elem_variant(c->lanes_f)) {
         if (!elem_variant_valid(c, c->lanes_f)) return set_error(c, HRN_EARG, "matrix-free variant not available for this shot count and precision");
         if (int rc = elem_ready(c)) return rc;
+    } else if (is_gt_variant(c->lanes_f)) {
+        if (int rc = gt_ready(c, 0)) return rc;
     }
     StageTimer tm(c);
     const int K = c->ckpt;
@@ -941,7 +917,11 @@ static int adjoint_t(hrn_ctx *c, int lambda_2mu, int keep_p)
     } else if (is_elem_variant(c->lanes_a)) {
         if (!elem_variant_valid(c, c->lanes_a)) return set_error(c, HRN_EARG, "matrix-free variant not available for this shot count and precision");
         if (int rc = elem_ready(c)) return rc;
+    } else if (is_gt_variant(c->lanes_a)) {
+        if (int rc = gt_ready(c, 1)) return rc;
     }
+    if (c->ckpt > 0 && is_gt_variant(c->lanes_f))   // the recomputed forward segments
+        if (int rc = gt_ready(c, 0)) return rc;
     StageTimer tm(c);
     double *gl = c->d_g.as<double>(), *gmu = gl + c->nj;
     const int gblocks = (c->nel_rd + kGradElems - 1) / kGradElems;

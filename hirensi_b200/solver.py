@@ -165,7 +165,8 @@ class Solver:
     def set_variant(self, forward: int = 0, adjoint: int = 0):
         """Force the stage-kernel variant, 0 = chosen by timing on first use.
         CSR: lanes per row * 10 + stage inputs materialized (1) or rebuilt (0),
-        + 2 for the tiled kernel (40-43, 80-83, 160, 161).  Matrix-free (operator
+        + 2 for the tiled kernel, + 4 for the compact row tiles with staged
+        gathers (40-45, 80-85, 160, 161).  Matrix-free (operator
         assembled from the mesh): 90-95 materialized / 100-105 rebuilt inputs,
         even = element slots, odd = atomic row sums, with 1, 2 or 4 shots per thread."""
         self._check(self._L.hrn_set_variant(self.h, int(forward), int(adjoint)))

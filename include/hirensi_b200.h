@@ -204,9 +204,12 @@ int hrn_last_timing(hrn_ctx *ctx, double *total_ms, double *stage_kernel_ms, int
 /* Stage-kernel variant per operator (forward, adjoint): lanes per row * 10 +
  * (1 if the stage inputs are materialized by the previous stage, 0 if rebuilt
  * at every gather) + (2 for the tiled kernel that stages the matrix slab of
- * each tile in shared memory with bulk copies); lanes in {4, 8, 16}, tiled
- * with 4 or 8.  0 = time all variants on first use and keep the fastest (the
- * default after every new sparsity pattern). */
+ * each tile in shared memory with bulk copies, 4 for the kernel over compact
+ * row tiles that stages each tile's distinct gathered records in shared
+ * memory); lanes in {4, 8, 16}, tiled with 4 or 8.  90-95 / 100-105: the
+ * matrix-free element kernels (operator assembled from the mesh).  0 = time all
+ * variants on first use and keep the fastest (the default after every new
+ * sparsity pattern). */
 int hrn_set_variant(hrn_ctx *ctx, int32_t forward, int32_t adjoint);
 int hrn_get_variant(hrn_ctx *ctx, int32_t *forward, int32_t *adjoint);
 

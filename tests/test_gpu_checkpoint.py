@@ -31,7 +31,7 @@ def _run(p, dis, precision, variant, interval):
 
 
 @pytest.mark.parametrize("precision,variant,interval", [("fp64", 41, 1), ("fp64", 41, 7), ("fp64", 41, 60),
-                                                        ("fp64", 90, 13), ("fp32", 41, 9)])
+                                                        ("fp64", 90, 13), ("fp32", 41, 9), ("fp64", 45, 7)])
 def test_checkpointed_adjoint_equals_full_history(gpu_lib, precision, variant, interval):
     p = tiny(nshot=2, nstep=60)
     _, _, hist_t = oracle_forward(p, p["lam_t"], p["mu_t"])
