@@ -54,6 +54,7 @@ SIGNATURES = {
     "hrn_get_gradient_device": (C.c_int, [VP, VP, VP]),
     "hrn_launch_count": (C.c_int, [VP, PI64]),
     "hrn_set_variant": (C.c_int, [VP, C.c_int32, C.c_int32]),
+    "hrn_set_shot_records": (C.c_int, [VP, VP, VP]),
     "hrn_get_variant": (C.c_int, [VP, PI, PI]),
     "hrn_vec_dot": (C.c_int, [VP, C.c_int32, VP, VP, PD]),
     "hrn_vec_norm": (C.c_int, [VP, C.c_int32, VP, C.c_int32, PD]),

@@ -560,6 +560,8 @@ int hrn_set_shots(hrn_ctx *c, int32_t nshot, int32_t nstep, double dt, int32_t n
     c->h_src_eq.assign(src_eq, src_eq + nsrc);
     c->h_src_b.assign(src_b, src_b + size_t(nsrc) * nshot);
     c->h_ftab.assign(ftab, ftab + size_t(nshot) * (nstep + 1) * 3);
+    c->h_shot_nstep.clear();
+    c->h_rec_mask.clear();
     c->have_data = false;
     for (double v : c->h_ftab)
         if (!std::isfinite(v)) return set_error(c, HRN_ENAN, "non-finite time function sample");
@@ -578,8 +580,43 @@ int hrn_set_receivers(hrn_ctx *c, int32_t nrec3, const int32_t *eqdis, const int
     c->nrec3 = nrec3;
     c->h_eqdis.assign(eqdis, eqdis + nrec3);
     c->h_eqdis_map.assign(eqdis_map, eqdis_map + nrec3);
+    c->h_rec_mask.clear();
     cudaSetDevice(c->device);
     return upload_receivers(c);
+}
+
+int hrn_set_shot_records(hrn_ctx *c, const int32_t *nstep_shot, const uint8_t *rec_mask)
+{
+    if (!c) return HRN_EARG;
+    if (c->nshot < 1) return set_error(c, HRN_ESTATE, "call hrn_set_shots first");
+    cudaSetDevice(c->device);
+    c->h_shot_nstep.clear();
+    c->h_rec_mask.clear();
+    if (nstep_shot) {
+        bool uneven = false;
+        for (int s = 0; s < c->nshot; ++s) {
+            if (nstep_shot[s] < 1 || nstep_shot[s] > c->nstep)
+                return set_error(c, HRN_EARG, "a shot's record length must be 1..nstep of hrn_set_shots");
+            uneven |= nstep_shot[s] != c->nstep;
+        }
+        if (uneven) {
+            c->h_shot_nstep.assign(nstep_shot, nstep_shot + c->nshot);
+            HRN_CUDA(c, c->d_shot_nstep.alloc(size_t(c->nshot) * 4));
+            HRN_CUDA(c, cudaMemcpy(c->d_shot_nstep.p, c->h_shot_nstep.data(), size_t(c->nshot) * 4, cudaMemcpyHostToDevice));
+        }
+    }
+    if (rec_mask && c->nrec3 > 0) {
+        const size_t nm = size_t(c->nshot) * c->nrec3;
+        bool all = true;
+        for (size_t i = 0; i < nm; ++i) all &= rec_mask[i] != 0;
+        if (!all) {
+            c->h_rec_mask.resize(nm);
+            for (size_t i = 0; i < nm; ++i) c->h_rec_mask[i] = rec_mask[i] ? 1 : 0;
+            HRN_CUDA(c, c->d_rec_mask.alloc(nm));
+            HRN_CUDA(c, cudaMemcpy(c->d_rec_mask.p, c->h_rec_mask.data(), nm, cudaMemcpyHostToDevice));
+        }
+    }
+    return HRN_OK;
 }
 
 int hrn_forward(hrn_ctx *c)

@@ -152,6 +152,12 @@ struct hrn_ctx {
     hrn::DevBuf d_eqdis_map;
     hrn::DevBuf d_srcv_a;         // [4][nslot_a][S]
     hrn::DevBuf d_dis;            // [nshot][nrec3][nstep+1] FP64
+    // uneven shots: per-shot record length and receiver selection (empty = all shots
+    // nstep long with every receiver)
+    std::vector<int32_t> h_shot_nstep;
+    std::vector<uint8_t> h_rec_mask;
+    hrn::DevBuf d_shot_nstep;     // [nshot] int32, or unset
+    hrn::DevBuf d_rec_mask;       // [nshot][nrec3] uint8, or unset
     hrn::DevBuf d_mis_terms;      // [nshot][nstep+1] FP64
     hrn::DevBuf d_cost;           // [1 + nshot] FP64
 
@@ -207,6 +213,16 @@ inline RecView rec_view(const hrn_ctx *c)
 {
     if (c->ckpt > 0) return RecView{c->d_traces.p, c->nrec3, c->d_iota.as<int32_t>()};
     return RecView{c->d_hist.p, c->nstore, c->d_eqdis_map.as<int32_t>()};
+}
+// Per-shot record lengths and receiver masks on the device, or null when the
+// batch is even.
+inline const int32_t *shot_nstep_ptr(const hrn_ctx *c)
+{
+    return c->h_shot_nstep.empty() ? nullptr : c->d_shot_nstep.as<int32_t>();
+}
+inline const uint8_t *rec_mask_ptr(const hrn_ctx *c)
+{
+    return c->h_rec_mask.empty() ? nullptr : c->d_rec_mask.as<uint8_t>();
 }
 int launch_scale_operator(hrn_ctx *c);
 int run_forward(hrn_ctx *c);

@@ -29,16 +29,19 @@ static __device__ __align__(256) double g_noalloc_scratch[kNoAllocMaxTerms + 1 +
 template <typename T>
 __global__ void k_noalloc_terms(int nshot, int nstep, int nstore, int nrec3, int nslot, const int32_t *__restrict__ ptr,
                                 const int32_t *__restrict__ qlist, const int32_t *__restrict__ emap, const T *__restrict__ hist,
-                                const double *__restrict__ dis, double *__restrict__ terms)
+                                const double *__restrict__ dis, double *__restrict__ terms,
+                                const int32_t *__restrict__ shot_nstep, const uint8_t *__restrict__ mask)
 {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= (nstep + 1) * nshot) return;
     const int s = t % nshot, n = t / nshot;
     double d = 0.0;
-    for (int sl = 0; sl < nslot; ++sl) {
+    // uneven shots: nothing past the shot's record length, masked receivers skipped
+    for (int sl = 0; sl < nslot && !(shot_nstep && n > shot_nstep[s]); ++sl) {
         double r = 0.0;
         for (int k = ptr[sl]; k < ptr[sl + 1]; ++k) {
             const int q = qlist[k];
+            if (mask && !mask[size_t(s) * nrec3 + q]) continue;
             r += double(hist[(size_t(n) * nstore + emap[q]) * nshot + s]) - dis[(size_t(s) * nrec3 + q) * (nstep + 1) + n];
         }
         d += r * r;
@@ -100,11 +103,13 @@ extern "C" int hrn_misfit_noalloc(hrn_ctx *c, const double *d_dis_meas, double *
         if (c->precision == HRN_FP64)
             k_noalloc_terms<double><<<nb, th, 0, c->stream>>>(c->nshot, c->nstep, rv.stride, c->nrec3, c->nslot_a,
                                                               c->d_aslot_ptr.as<int32_t>(), c->d_aslot_q.as<int32_t>(), rv.map,
-                                                              static_cast<const double *>(rv.hist), d_dis_meas, terms);
+                                                              static_cast<const double *>(rv.hist), d_dis_meas, terms,
+                                                              shot_nstep_ptr(c), rec_mask_ptr(c));
         else
             k_noalloc_terms<float><<<nb, th, 0, c->stream>>>(c->nshot, c->nstep, rv.stride, c->nrec3, c->nslot_a,
                                                              c->d_aslot_ptr.as<int32_t>(), c->d_aslot_q.as<int32_t>(), rv.map,
-                                                             static_cast<const float *>(rv.hist), d_dis_meas, terms);
+                                                             static_cast<const float *>(rv.hist), d_dis_meas, terms,
+                                                             shot_nstep_ptr(c), rec_mask_ptr(c));
         ++c->launches;
     } else {
         // no receivers: every term is zero (the scratch keeps the last call's contents)

@@ -274,18 +274,29 @@ __global__ void k_traces(int nrec3, const int32_t *__restrict__ eq, const T *__r
     out[t] = x2[size_t(eq[q]) * S + s];
 }
 
+// Uneven shots (shot_nstep / mask not null): shot s records steps 0..shot_nstep[s]
+// at the receivers q with mask[s][q] != 0.  Its adjoint starts at its own last
+// step: for n > shot_nstep[s] every source of the shot is zero, so its state stays
+// exactly zero until then and the batch reproduces the shot run alone.
 template <typename T, int S>
 __global__ void k_src_adj(int n, int nstep, int nstore, int nrec3, int nslot, const int32_t *__restrict__ ptr,
                           const int32_t *__restrict__ qlist, const int32_t *__restrict__ slot_eq,
                           const int32_t *__restrict__ emap, const T *__restrict__ hist,
-                          const double *__restrict__ dis, const double *__restrict__ im, T *__restrict__ srcv)
+                          const double *__restrict__ dis, const double *__restrict__ im, T *__restrict__ srcv,
+                          const int32_t *__restrict__ shot_nstep, const uint8_t *__restrict__ mask)
 {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= nslot * S) return;
     const int s = t % S, sl = t / S;
+    if (shot_nstep && n > shot_nstep[s]) {
+#pragma unroll
+        for (int k = 0; k < 4; ++k) srcv[(k * size_t(nslot) + sl) * S + s] = T(0);
+        return;
+    }
     double r1 = 0.0, r4 = 0.0;
     for (int k = ptr[sl]; k < ptr[sl + 1]; ++k) {
         const int q = qlist[k];
+        if (mask && !mask[size_t(s) * nrec3 + q]) continue;
         const size_t pos = size_t(emap[q]) * S + s;
         const double *d = dis + (size_t(s) * nrec3 + q) * (nstep + 1);
         r1 += double(hist[size_t(n) * nstore * S + pos]) - d[n];
@@ -397,19 +408,23 @@ __global__ void __launch_bounds__(128) k_gradient(int nel_rd, const int32_t *__r
 // ----------------------------------------------------------------------------
 // misfit (Compute_Misfit, S4/Solver_PETSc_Inverse.F90:591-657)
 
+// Uneven shots: the terms of a shot past its record length are zero, and masked
+// receivers do not enter it (see k_src_adj).
 template <typename T, int S>
 __global__ void k_misfit_terms(int nstep, int nstore, int nrec3, int nslot, const int32_t *__restrict__ ptr,
                                const int32_t *__restrict__ qlist, const int32_t *__restrict__ emap,
-                               const T *__restrict__ hist, const double *__restrict__ dis, double *__restrict__ terms)
+                               const T *__restrict__ hist, const double *__restrict__ dis, double *__restrict__ terms,
+                               const int32_t *__restrict__ shot_nstep, const uint8_t *__restrict__ mask)
 {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= (nstep + 1) * S) return;
     const int s = t % S, n = t / S;
     double d = 0.0;
-    for (int sl = 0; sl < nslot; ++sl) {
+    for (int sl = 0; sl < nslot && !(shot_nstep && n > shot_nstep[s]); ++sl) {
         double r = 0.0;
         for (int k = ptr[sl]; k < ptr[sl + 1]; ++k) {
             const int q = qlist[k];
+            if (mask && !mask[size_t(s) * nrec3 + q]) continue;
             r += double(hist[(size_t(n) * nstore + emap[q]) * S + s]) - dis[(size_t(s) * nrec3 + q) * (nstep + 1) + n];
         }
         d += r * r;
@@ -951,7 +966,7 @@ static int adjoint_t(hrn_ctx *c, int lambda_2mu, int keep_p)
             k_src_adj<T, S><<<(c->nslot_a * S + 127) / 128, 128, 0, c->stream>>>(
                 n, c->nstep, rv.stride, c->nrec3, c->nslot_a, c->d_aslot_ptr.as<int32_t>(), c->d_aslot_q.as<int32_t>(),
                 c->d_aslot_eq.as<int32_t>(), rv.map, static_cast<const T *>(rv.hist), c->d_dis.as<double>(),
-                c->d_im.as<double>(), c->d_srcv_a.as<T>()); ++c->launches;
+                c->d_im.as<double>(), c->d_srcv_a.as<T>(), shot_nstep_ptr(c), rec_mask_ptr(c)); ++c->launches;
         a.hist = keep_p ? c->d_phist.as<T>() + size_t(n) * c->nstore * S : nullptr;
         T *X = (it & 1) ? X1 : X0, *Y = (it & 1) ? X0 : X1;
         launch_step<T, S>(c, a, X, Y, c->timing ? &tm : nullptr, c->lanes_a, ta, 1);
@@ -986,7 +1001,8 @@ static int misfit_t(hrn_ctx *c, double *cost)
     k_misfit_terms<T, S><<<(tot + 127) / 128, 128, 0, c->stream>>>(c->nstep, rv.stride, c->nrec3, c->nslot_a,
                                                                    c->d_aslot_ptr.as<int32_t>(), c->d_aslot_q.as<int32_t>(),
                                                                    rv.map, static_cast<const T *>(rv.hist),
-                                                                   c->d_dis.as<double>(), c->d_mis_terms.as<double>()); ++c->launches;
+                                                                   c->d_dis.as<double>(), c->d_mis_terms.as<double>(),
+                                                                   shot_nstep_ptr(c), rec_mask_ptr(c)); ++c->launches;
     k_misfit_sum<<<1, 1, 0, c->stream>>>(S, c->nstep, c->dt, c->d_mis_terms.as<double>(), c->d_cost.as<double>()); ++c->launches;
     HRN_CUDA(c, cudaGetLastError());
     std::vector<double> h(size_t(1 + S));

@@ -149,6 +149,21 @@ class Solver:
         self._check(self._L.hrn_set_receivers(self.h, e.size, iptr(e), iptr(m)))
         self.nrec3 = e.size
 
+    def set_shot_records(self, nstep_shot=None, rec_mask=None):
+        """Uneven shots: record length of each shot (<= nstep of set_shots) and
+        rec_mask [nshot, nrec3] of the receivers each shot records (None = all)."""
+        ns = None if nstep_shot is None else i32(nstep_shot)
+        if ns is not None and ns.size != self.nshot:
+            raise ValueError("nstep_shot must have one entry per shot")
+        mk = None
+        if rec_mask is not None:
+            mk = np.ascontiguousarray(np.asarray(rec_mask, dtype=np.uint8))
+            if mk.shape != (self.nshot, self.nrec3):
+                raise ValueError("rec_mask must be [nshot, nrec3]")
+        self._check(self._L.hrn_set_shot_records(self.h, ns.ctypes.data if ns is not None else None,
+                                                 mk.ctypes.data if mk is not None else None))
+        self._keep_records = (ns, mk)
+
     def set_data(self, dis_meas=None, device_ptr: int | None = None):
         """Keep the measured data [nshot, nrec3, nstep+1] on the device (host array or device pointer)."""
         if device_ptr is not None:

@@ -97,6 +97,19 @@ int hrn_set_shots(hrn_ctx *ctx, int32_t nshot, int32_t nstep, double dt,
  * positions in the history), S4/IO_Parallel_Inversion.F90:116-133. */
 int hrn_set_receivers(hrn_ctx *ctx, int32_t nrec3, const int32_t *eqdis, const int32_t *eqdis_map);
 
+/* Shots of uneven record length and receiver count advanced in one batch.  The
+ * reference runs one source per solve, with its own NSTEP and EqDis
+ * (S4/Solver_PETSc_Explicit.F90:660-1405, S4/Solver_PETSc_Inverse.F90:591-657); here
+ * shot s records steps 0..nstep_shot[s] (1 <= nstep_shot[s] <= nstep of
+ * hrn_set_shots), and receiver entry q of hrn_set_receivers belongs to it when
+ * rec_mask[s * nrec3 + q] != 0.  Its misfit counts steps 1..nstep_shot[s] and its
+ * receivers only, and its adjoint starts at its own last step, so every shot's
+ * misfit, traces and gradient share equal those of the shot solved alone.  The
+ * batch still steps nstep times, and the forward history past a shot's length is
+ * computed but unused.  NULL leaves all shots at nstep / every receiver.  Reset by
+ * hrn_set_shots (both) and hrn_set_receivers (the mask). */
+int hrn_set_shot_records(hrn_ctx *ctx, const int32_t *nstep_shot, const uint8_t *rec_mask);
+
 /* Measured data Dis_meas of every shot, kept on the device for hrn_misfit and
  * hrn_adjoint_gradient called with dis_meas = NULL (on_device: dis_meas is a
  * device pointer).  Replaces the measured-data read of
