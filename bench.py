@@ -54,6 +54,8 @@ def parse_args():
                     help="stepping precision of the --profile-case run")
     ap.add_argument("--variant", type=int, default=0,
                     help="stage-kernel variant for forward and adjoint (0 = chosen by timing on first use)")
+    ap.add_argument("--no-graphs", action="store_true",
+                    help="launch every kernel directly instead of replaying the captured time loops")
     return ap.parse_args()
 
 
@@ -67,6 +69,18 @@ def measured_peaks():
         return float(d["hbm_gbs"]), "measured"
     except Exception:
         return 6650.0, "fallback"
+
+
+def stage_kernel_name(variant: int):
+    """Kernel of a stage variant (FP64, 4 shots) and the committed ncu summary holding
+    its DRAM traffic per launch."""
+    if variant in (44, 45, 84, 85):
+        return "rk4_stage_gt<double,4>", "rk4_stage_gt_fp64_inversion.md"
+    if variant in (42, 43, 82, 83):
+        return "rk4_stage_tile<double,4>", None
+    if 90 <= variant <= 105:
+        return "k_elem<double,4> + k_node<double,4>", None
+    return "rk4_stage<double,4>", "rk4_stage_fp64_inversion.md"
 
 
 def profile_traffic(name: str):
@@ -172,6 +186,7 @@ def run_native(args, rank, world, local_rank):
         s.set_receivers(prob.eqdis, prob.eqdis_map)
         if variant and args.variant:
             s.set_variant(args.variant, args.variant)
+        s.set_graphs(not args.no_graphs)
         return s
 
     # measured data: FP64 forward of the true model (set-up, untimed)
@@ -279,18 +294,20 @@ def run_native(args, rank, world, local_rank):
     result["gpu_launches"] = int(launches)
     result["config"]["stage_variant_fwd_adj"] = list(s64.variant())
 
-    # roofline of the dominant kernel (fused RK4 stage)
+    # roofline of the dominant kernel (fused RK4 stage, the variant the tuner chose)
     peak, peak_kind = measured_peaks()
     bytes_launch = stage_bytes(sum(nnz), m.neq, prob.nshot, 8)
     achieved = bytes_launch / (stage_avg_ms * 1e-3) / 1e9
-    traffic = profile_traffic("rk4_stage_fp64_inversion.md")
-    result["roofline"] = {"bound": "hbm", "kernel": "rk4_stage<double,4>", "achieved": achieved, "peak": peak,
+    kname, kprofile = stage_kernel_name(s64.variant()[0])
+    traffic = profile_traffic(kprofile) if kprofile else None
+    result["roofline"] = {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": peak,
                           "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
                           "bytes_per_launch": bytes_launch, "avg_launch_us": stage_avg_ms * 1e3,
                           "launches_timed": int(stage_n), "stage_share_of_step": stage_ms / ms_roof,
                           "traffic": traffic}
     result["clocks"] = clocks
 
+    tuned = {"fp64": s64.variant()}   # the FWI legs reuse the variants tuned here
     if not args.profile_case:
         # e2e leg: host buffers through the C ABI, copies inside the timed region
         ms_e2e, _, _ = timed(step_e2e, s64, K, min(W, 1))
@@ -308,6 +325,7 @@ def run_native(args, rank, world, local_rank):
             tr32 = s32.traces()
             g32 = g_dev.clone()
             ms32e, _, _ = timed(step_e2e, s32, K, min(W, 1))
+            tuned["fp32"] = s32.variant()
 
             def rel(a, b):
                 return float(np.linalg.norm(a - b) / np.linalg.norm(b))
@@ -322,12 +340,13 @@ def run_native(args, rank, world, local_rank):
         if not args.no_fwi and world == 1:
             result["fwi"] = {}
             for prec in (["fp64"] if args.no_fp32 else ["fp64", "fp32"]):
-                result["fwi"][prec] = fwi_leg(prec, prob, dis, local_rank, args.fwi_iters)
+                result["fwi"][prec] = fwi_leg(prec, prob, dis, local_rank, args.fwi_iters, variant=tuned.get(prec))
             if not args.no_fp32 and os.path.exists(PRECOND_WEIGHTS):
                 # time for FP32 stepping + the learned preconditioner to reach the
                 # misfit reduction of the plain FP64 run
                 r64 = result["fwi"]["fp64"]["misfit_reduction"]
-                fl = fwi_leg("fp32", prob, dis, local_rank, args.fwi_iters, learned=True, target=r64)
+                fl = fwi_leg("fp32", prob, dis, local_rank, args.fwi_iters, learned=True, target=r64,
+                             variant=tuned.get("fp32"))
                 result["fwi"]["fp32_learned"] = fl
                 if fl["reached_target"]:
                     result["fwi"]["time_to_fp64_misfit_speedup"] = result["fwi"]["fp64"]["wall_s"] / fl["wall_s"]
@@ -338,11 +357,12 @@ def run_native(args, rank, world, local_rank):
 PRECOND_WEIGHTS = os.path.join(ROOT, "hirensi_b200", "data", "precond_cnn_16x16x8.npz")
 
 
-def fwi_leg(precision, prob, dis, local_rank, iters, learned=False, target=None):
+def fwi_leg(precision, prob, dis, local_rank, iters, learned=False, target=None, variant=None):
     """Wall time of `iters` L-BFGS iterations (memory 5) of the inversion loop from
     the initial model, all vectors on the device; misfit reduction reached.  With
     `learned`, each iteration first tries the trained CNN's scaled direction, and the
-    run stops once the misfit reduction reaches `target`."""
+    run stops once the misfit reduction reaches `target`.  `variant` = the (forward,
+    adjoint) stage variants tuned earlier on the same operator, reused here."""
     import torch
     from hirensi_b200.configs import RHO
     from hirensi_b200.inversion import FWI, DeviceBackend, InversionConfig
@@ -355,6 +375,8 @@ def fwi_leg(precision, prob, dis, local_rank, iters, learned=False, target=None)
     s.set_shots(prob.nstep, prob.dt, prob.src_eq, prob.src_b, prob.ftab)
     s.set_receivers(prob.eqdis, prob.eqdis_map)
     s.set_data(dis)
+    if variant:
+        s.set_variant(*variant)
     cfg = InversionConfig(m_lbfgs=5, bounds_lambda=(10.0, 2000.0), bounds_mu=(10.0, 1000.0))
     backend = DeviceBackend(s, m)
     pre = None

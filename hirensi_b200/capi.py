@@ -55,6 +55,8 @@ SIGNATURES = {
     "hrn_launch_count": (C.c_int, [VP, PI64]),
     "hrn_set_variant": (C.c_int, [VP, C.c_int32, C.c_int32]),
     "hrn_set_shot_records": (C.c_int, [VP, VP, VP]),
+    "hrn_set_graphs": (C.c_int, [VP, C.c_int32]),
+    "hrn_graph_stats": (C.c_int, [VP, VP, VP]),
     "hrn_get_variant": (C.c_int, [VP, PI, PI]),
     "hrn_vec_dot": (C.c_int, [VP, C.c_int32, VP, VP, PD]),
     "hrn_vec_norm": (C.c_int, [VP, C.c_int32, VP, C.c_int32, PD]),

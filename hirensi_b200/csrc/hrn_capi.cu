@@ -372,7 +372,28 @@ const char *hrn_last_error(const hrn_ctx *c) { return c ? c->err.c_str() : "null
 int hrn_set_stream(hrn_ctx *c, void *stream)
 {
     if (!c) return HRN_EARG;
+    ++c->epoch;
     c->stream = stream ? static_cast<cudaStream_t>(stream) : c->own_stream;
+    return HRN_OK;
+}
+
+int hrn_set_graphs(hrn_ctx *c, int32_t enable)
+{
+    if (!c) return HRN_EARG;
+    c->graphs = enable != 0;
+    if (!c->graphs) {
+        cudaSetDevice(c->device);
+        c->gfwd.reset();
+        c->gadj.reset();
+    }
+    return HRN_OK;
+}
+
+int hrn_graph_stats(hrn_ctx *c, int64_t *captures, int64_t *replays)
+{
+    if (!c) return HRN_EARG;
+    if (captures) *captures = c->graph_captures;
+    if (replays) *replays = c->graph_replays;
     return HRN_OK;
 }
 
@@ -401,6 +422,7 @@ int hrn_set_operator_csr(hrn_ctx *c, int32_t neq, const int32_t *c_ia, const int
                          const int32_t *g_ja, const double *g_a, const double *diag_m)
 {
     if (!c) return HRN_EARG;
+    ++c->epoch;
     if (neq <= 0 || !c_ia || !k_ia || !g_ia || !diag_m) return set_error(c, HRN_EARG, "bad operator arguments");
     if (c->have_mesh && neq != c->neq) return set_error(c, HRN_EARG, "neq differs from the mesh");
     cudaSetDevice(c->device);
@@ -431,6 +453,7 @@ int hrn_set_mesh(hrn_ctx *c, int32_t nj, int32_t nel, int32_t neq, const double 
                  const int32_t *mtel, const int32_t *id, const double *rho_el, const double *pml_param)
 {
     if (!c) return HRN_EARG;
+    ++c->epoch;
     if (nj <= 0 || nel <= 0 || neq <= 0 || !xyz || !inod || !mtel || !id || !rho_el || !pml_param)
         return set_error(c, HRN_EARG, "bad mesh arguments");
     if (c->have_pattern && neq != c->neq) return set_error(c, HRN_EARG, "neq differs from the operator");
@@ -538,6 +561,7 @@ int hrn_get_diag_m(hrn_ctx *c, double *diag_m)
 int hrn_set_history(hrn_ctx *c, int32_t nstore, const int32_t *store_eq)
 {
     if (!c) return HRN_EARG;
+    ++c->epoch;
     if (nstore <= 0 || !store_eq) return set_error(c, HRN_EARG, "bad history arguments");
     c->nstore = nstore;
     c->h_store_eq.assign(store_eq, store_eq + nstore);
@@ -551,6 +575,7 @@ int hrn_set_shots(hrn_ctx *c, int32_t nshot, int32_t nstep, double dt, int32_t n
                   const double *src_b, const double *ftab)
 {
     if (!c) return HRN_EARG;
+    ++c->epoch;
     if (nshot < 1 || nshot > HRN_MAX_SHOTS) return set_error(c, HRN_EARG, "nshot must be 1..HRN_MAX_SHOTS");
     if (nstep < 1 || !(dt > 0.0) || nsrc < 0 || (nsrc > 0 && (!src_eq || !src_b)) || !ftab)
         return set_error(c, HRN_EARG, "bad shot arguments");
@@ -576,6 +601,7 @@ int hrn_set_shots(hrn_ctx *c, int32_t nshot, int32_t nstep, double dt, int32_t n
 int hrn_set_receivers(hrn_ctx *c, int32_t nrec3, const int32_t *eqdis, const int32_t *eqdis_map)
 {
     if (!c) return HRN_EARG;
+    ++c->epoch;
     if (nrec3 < 0 || (nrec3 > 0 && (!eqdis || !eqdis_map))) return set_error(c, HRN_EARG, "bad receiver arguments");
     c->nrec3 = nrec3;
     c->h_eqdis.assign(eqdis, eqdis + nrec3);
@@ -588,6 +614,7 @@ int hrn_set_receivers(hrn_ctx *c, int32_t nrec3, const int32_t *eqdis, const int
 int hrn_set_shot_records(hrn_ctx *c, const int32_t *nstep_shot, const uint8_t *rec_mask)
 {
     if (!c) return HRN_EARG;
+    ++c->epoch;
     if (c->nshot < 1) return set_error(c, HRN_ESTATE, "call hrn_set_shots first");
     cudaSetDevice(c->device);
     c->h_shot_nstep.clear();
@@ -726,6 +753,7 @@ int hrn_get_gradient_device(hrn_ctx *c, double *d_g_lambda, double *d_g_mu)
 int hrn_set_variant(hrn_ctx *c, int32_t forward, int32_t adjoint)
 {
     if (!c) return HRN_EARG;
+    ++c->epoch;
     auto ok = [](int v) {
         return v == 0 || v == 40 || v == 80 || v == 160 || v == 41 || v == 81 || v == 161 || v == 42 || v == 43 || v == 82 ||
                v == 83 || hrn::is_gt_variant(v) || (v >= 90 && v <= 95) || (v >= 100 && v <= 105);
@@ -750,6 +778,7 @@ int hrn_get_variant(hrn_ctx *c, int32_t *forward, int32_t *adjoint)
 int hrn_set_checkpointing(hrn_ctx *c, int32_t interval)
 {
     if (!c) return HRN_EARG;
+    ++c->epoch;
     if (interval < 0) return set_error(c, HRN_EARG, "checkpoint interval must be >= 0");
     c->ckpt = interval;
     c->have_forward = false;

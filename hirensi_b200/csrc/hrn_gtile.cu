@@ -361,26 +361,67 @@ static int gt_build(hrn_ctx *c, int adj, size_t rec_bytes)
     row_order(c, order, gstart);
     const int ngroups = int(gstart.size()) - 1;
 
-    // distinct keys and entries of the rows of groups [g0, g1)
-    std::vector<uint32_t> keys;
-    int64_t nent_range = 0;
-    auto collect = [&](int g0, int g1) {
-        keys.clear();
-        nent_range = 0;
+    // Distinct keys of a range of groups, counted with a per-key mark of the last
+    // range that saw it (no clearing between ranges).  Key index = matrix * n + column.
+    auto kidx = [n](uint32_t key) { return size_t(key >> kTagBits) * size_t(n) + size_t(key & kColMask); };
+    std::vector<int32_t> mark(size_t(3) * n, -1), pos(size_t(3) * n, 0);
+    int range_id = 0;
+    auto count = [&](int g0, int g1, int64_t &nent, int &nu) {
+        ++range_id;
+        nent = 0;
+        nu = 0;
         for (int r = gstart[g0]; r < gstart[g1]; ++r) {
             const int row = order[r];
-            keys.insert(keys.end(), colx.begin() + rowptr[row], colx.begin() + rowptr[row + 1]);
-            nent_range += rowptr[row + 1] - rowptr[row];
+            for (int32_t p = rowptr[row]; p < rowptr[row + 1]; ++p) {
+                const size_t k = kidx(colx[p]);
+                if (mark[k] != range_id) {
+                    mark[k] = range_id;
+                    ++nu;
+                }
+            }
+            nent += rowptr[row + 1] - rowptr[row];
         }
-        std::sort(keys.begin(), keys.end());
-        keys.erase(std::unique(keys.begin(), keys.end()), keys.end());
     };
     auto pad8 = [](int64_t x) { return (x + 7) & ~int64_t(7); };
-    std::vector<int32_t> tiles_g{0};   // group boundaries of the tiles
-    std::vector<int32_t> h_uoff{0};
+    std::vector<int32_t> h_tinfo, h_ent(size_t(std::max(n, 1)), 0);
     std::vector<uint32_t> h_ukey;
+    std::vector<uint16_t> h_lidx;
+    std::vector<int32_t> h_perm;
+    std::vector<uint32_t> keys;
     size_t smem = 0;
     bool fit = true;
+    // accept groups [g0, g1) as a tile: its ascending keys, rows, entries and slab padding
+    auto emit = [&](int g0, int g1) {
+        ++range_id;
+        keys.clear();
+        for (int r = gstart[g0]; r < gstart[g1]; ++r)
+            for (int32_t p = rowptr[order[r]]; p < rowptr[order[r] + 1]; ++p) {
+                const size_t k = kidx(colx[p]);
+                if (mark[k] != range_id) {
+                    mark[k] = range_id;
+                    keys.push_back(colx[p]);
+                }
+            }
+        std::sort(keys.begin(), keys.end());
+        for (size_t q = 0; q < keys.size(); ++q) pos[kidx(keys[q])] = int32_t(q);
+        const int64_t e0 = int64_t(h_lidx.size());
+        for (int r = gstart[g0]; r < gstart[g1]; ++r) {
+            const int row = order[r];
+            const int cnt = rowptr[row + 1] - rowptr[row];
+            h_ent[r] = int32_t(uint32_t(int64_t(h_lidx.size()) - e0) | (uint32_t(cnt) << 16));
+            for (int32_t p = rowptr[row]; p < rowptr[row + 1]; ++p) {
+                h_lidx.push_back(uint16_t(pos[kidx(colx[p])]));
+                h_perm.push_back(p);
+            }
+        }
+        const int64_t ne = int64_t(h_lidx.size()) - e0;
+        h_lidx.resize(size_t(e0 + pad8(ne)), 0);
+        h_perm.resize(size_t(e0 + pad8(ne)), -1);
+        const int32_t ti[8] = {gstart[g0], gstart[g1] - gstart[g0], int32_t(e0), int32_t(pad8(ne)),
+                               int32_t(h_ukey.size()), int32_t(keys.size()), 0, 0};
+        h_tinfo.insert(h_tinfo.end(), ti, ti + 8);
+        h_ukey.insert(h_ukey.end(), keys.begin(), keys.end());
+    };
     // cut a range of groups into tiles: halve until the tile's footprint fits
     std::vector<std::pair<int, int>> stack;
     auto cut = [&](int g0, int g1) {
@@ -388,11 +429,13 @@ static int gt_build(hrn_ctx *c, int adj, size_t rec_bytes)
         while (!stack.empty() && fit) {
             const auto [a0, a1] = stack.back();
             stack.pop_back();
-            collect(a0, a1);
+            int64_t nent = 0;
+            int nu = 0;
+            count(a0, a1, nent, nu);
             const int nrows = gstart[a1] - gstart[a0];
-            const int64_t ne = pad8(nent_range);
-            const bool small = ne <= 65535 && keys.size() <= 65535;
-            const size_t f = small ? gt_footprint(nrows, int(ne), int(keys.size()), elem, rec_bytes) : ~size_t(0);
+            const int64_t ne = pad8(nent);
+            const bool small = ne <= 65535 && nu <= 65535;
+            const size_t f = small ? gt_footprint(nrows, int(ne), nu, elem, rec_bytes) : ~size_t(0);
             if (f > kGtBudget) {
                 if (a1 - a0 == 1) { fit = false; break; }
                 const int mid = (a0 + a1) / 2;
@@ -400,9 +443,7 @@ static int gt_build(hrn_ctx *c, int adj, size_t rec_bytes)
                 stack.push_back({a0, mid});
                 continue;
             }
-            tiles_g.push_back(a1);
-            h_ukey.insert(h_ukey.end(), keys.begin(), keys.end());
-            h_uoff.push_back(int32_t(h_ukey.size()));
+            emit(a0, a1);
             smem = std::max(smem, f);
         }
     };
@@ -414,42 +455,13 @@ static int gt_build(hrn_ctx *c, int adj, size_t rec_bytes)
         g = g1;
     }
     if (!fit) return set_error(c, HRN_EARG, "a node's rows need more shared memory than a staged tile holds");
-    if (int64_t(h_ukey.size()) >= (int64_t(1) << 31)) return set_error(c, HRN_EARG, "too many staged keys");
-    const int ntiles = int(tiles_g.size()) - 1;
-
-    // tile info, rows, packed entry ranges, local key positions and the value permutation
-    std::vector<int32_t> h_tinfo(size_t(ntiles) * 8, 0), h_ent(size_t(std::max(n, 1)), 0);
-    int64_t total = 0;
-    for (int t = 0; t < ntiles; ++t) {
-        int64_t ne = 0;
-        for (int r = gstart[tiles_g[t]]; r < gstart[tiles_g[t + 1]]; ++r) ne += rowptr[order[r] + 1] - rowptr[order[r]];
-        total += pad8(ne);
-    }
-    if (total >= (int64_t(1) << 31)) return set_error(c, HRN_EARG, "staged-gather tiles need fewer than 2^31 entries");
-    std::vector<uint16_t> h_lidx(size_t(std::max<int64_t>(total, 8)), 0);
-    std::vector<int32_t> h_perm(size_t(std::max<int64_t>(total, 8)), -1);
-    int64_t e = 0;
-    for (int t = 0; t < ntiles; ++t) {
-        const int ra = gstart[tiles_g[t]], rb = gstart[tiles_g[t + 1]];
-        const uint32_t *kb = h_ukey.data() + h_uoff[t], *ke = h_ukey.data() + h_uoff[t + 1];
-        const int64_t e0 = e;
-        for (int r = ra; r < rb; ++r) {
-            const int row = order[r];
-            const int cnt = rowptr[row + 1] - rowptr[row];
-            h_ent[r] = int32_t(uint32_t(e - e0) | (uint32_t(cnt) << 16));
-            for (int32_t p = rowptr[row]; p < rowptr[row + 1]; ++p, ++e) {
-                h_lidx[e] = uint16_t(std::lower_bound(kb, ke, colx[p]) - kb);
-                h_perm[e] = p;
-            }
-        }
-        e = e0 + pad8(e - e0);
-        int32_t *ti = h_tinfo.data() + size_t(t) * 8;
-        ti[0] = ra;
-        ti[1] = rb - ra;
-        ti[2] = int32_t(e0);
-        ti[3] = int32_t(e - e0);
-        ti[4] = h_uoff[t];
-        ti[5] = h_uoff[t + 1] - h_uoff[t];
+    if (int64_t(h_ukey.size()) >= (int64_t(1) << 31) || int64_t(h_lidx.size()) >= (int64_t(1) << 31))
+        return set_error(c, HRN_EARG, "staged-gather tiles need fewer than 2^31 entries and keys");
+    const int ntiles = int(h_tinfo.size() / 8);
+    const int64_t total = int64_t(h_lidx.size());
+    if (h_lidx.size() < 8) {
+        h_lidx.resize(8, 0);
+        h_perm.resize(8, -1);
     }
 
     HRN_CUDA(c, gs.d_tinfo.alloc(std::max<size_t>(h_tinfo.size(), 8) * 4));

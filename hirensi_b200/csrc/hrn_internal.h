@@ -5,12 +5,21 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <atomic>
 #include <string>
 #include <vector>
 
 #include "../../include/hirensi_b200.h"
 
 namespace hrn {
+
+// Incremented by every device allocation or release of a DevBuf, so that a
+// captured graph can tell whether any buffer it names may have moved.
+inline std::atomic<uint64_t> &alloc_generation()
+{
+    static std::atomic<uint64_t> g{0};
+    return g;
+}
 
 // Owning device buffer (cudaMalloc / cudaFree).
 struct DevBuf {
@@ -21,7 +30,10 @@ struct DevBuf {
     DevBuf &operator=(const DevBuf &) = delete;
     ~DevBuf() { release(); }
     void release() {
-        if (p) cudaFree(p);
+        if (p) {
+            cudaFree(p);
+            alloc_generation()++;
+        }
         p = nullptr;
         bytes = 0;
     }
@@ -30,6 +42,7 @@ struct DevBuf {
         release();
         if (n == 0) return cudaSuccess;
         cudaError_t e = cudaMalloc(&p, n);
+        alloc_generation()++;
         if (e == cudaSuccess) bytes = n;
         else p = nullptr;
         return e;
@@ -41,6 +54,22 @@ constexpr int kTagBits = 30;
 constexpr int kTileEntries = 4096;     // entries per tile of the tiled stage kernel
 constexpr size_t kBulkPad = 64;        // bytes past the end of bulk-copied arrays
 constexpr uint32_t kColMask = (1u << kTagBits) - 1u;
+
+// One time loop (every launch of a forward or adjoint call) captured as a CUDA
+// graph and replayed while its signature -- allocation generation, settings
+// epoch, variant and flags -- is unchanged.
+struct LoopGraph {
+    cudaGraphExec_t exec = nullptr;
+    uint64_t sig[6] = {0, 0, 0, 0, 0, 0};
+    int64_t launches = 0;      // kernels launched by one replay
+    void reset() {
+        if (exec) cudaGraphExecDestroy(exec);
+        exec = nullptr;
+        for (auto &v : sig) v = 0;
+        launches = 0;
+    }
+    ~LoopGraph() { reset(); }
+};
 
 // Row tiles of the staged-gather stage kernel (variants 44, 45, 84, 85) for one
 // operator direction: spatially compact sets of rows whose gathered (matrix,
@@ -182,10 +211,17 @@ struct hrn_ctx {
 
     // ---- inversion (model update)
     hrn::DevBuf d_red;            // reduction partials
+    hrn::DevBuf d_tv_part;        // per-block partial sums of the TV regularization
     int lbfgs_m = 0;
     hrn::DevBuf d_lbfgs;          // [4][M][nj] Ys_l, Ys_m, Ss_l, Ss_m, then 6 scratch vectors [nj]
     hrn::DevBuf d_restrict;       // [nj] restriction to the regular domain (1 / 0)
     std::vector<double> lbfgs_rho, lbfgs_alpha;
+
+    // ---- CUDA graphs of the time loops (on unless disabled or timing per launch)
+    bool graphs = true;
+    uint64_t epoch = 1;            // incremented by every setting change
+    hrn::LoopGraph gfwd, gadj;
+    int64_t graph_captures = 0, graph_replays = 0;
 
     // ---- timing
     int64_t launches = 0;          // kernels launched by this context (cumulative)

@@ -207,7 +207,7 @@ int regularization_tv(hrn_ctx *c, const double *lam, const double *mu, double *r
     HRN_CUDA(c, cudaMemsetAsync(reg_l, 0, size_t(c->nj) * 8, c->stream));
     HRN_CUDA(c, cudaMemsetAsync(reg_m, 0, size_t(c->nj) * 8, c->stream));
     const int th = 256, nb = std::max((c->nel_rd * 27 + th - 1) / th, 1);
-    DevBuf part;
+    DevBuf &part = c->d_tv_part;   // kept, so that repeated calls allocate nothing
     HRN_CUDA(c, part.alloc(size_t(2) * nb * 8));
     k_tv<<<nb, th, 0, c->stream>>>(c->nel_rd, c->d_rd_elems.as<int32_t>(), c->d_inod.as<int32_t>(), c->d_rd_geom.as<double>(),
                                    lam, mu, reg_l, reg_m, part.as<double>());

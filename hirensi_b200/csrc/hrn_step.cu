@@ -823,60 +823,147 @@ static const T *forward_src(hrn_ctx *c, int n)
     return c->nslot_f ? c->d_srcv_f.as<T>() + size_t(n) * 4 * c->nslot_f * S : nullptr;
 }
 
+// ----------------------------------------------------------------------------
+// CUDA graphs of the time loops.  A call's stream work (memsets, source tables,
+// every stage, history, trace and gradient launch of all steps) is captured once
+// and replayed while nothing it names can have changed: the allocation
+// generation (every DevBuf allocation or release), the settings epoch (every
+// setter), the variant and the call's flags.  Values in the buffers -- the
+// scaled operator after a reassembly, the data, the time functions -- may
+// change between replays.  Host work (autotuning, table builds, allocations)
+// stays outside the capture.
+
+static bool graph_usable(const hrn_ctx *c)
+{
+    return c->graphs && !c->timing && c->stream != nullptr && c->stream != cudaStreamLegacy;
+}
+
+// Capture body(c) on the context's stream into g (replacing an older graph).
+// Returns false, with the stream usable and no error pending, if capture or
+// instantiation fails; the caller then runs the body directly.
+template <typename F>
+static bool graph_capture(hrn_ctx *c, LoopGraph &g, const uint64_t (&sig)[6], F body)
+{
+    g.reset();
+    const int64_t l0 = c->launches;
+    if (cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    const int rc = body();
+    cudaGraph_t graph = nullptr;
+    const cudaError_t ec = cudaStreamEndCapture(c->stream, &graph);
+    const int64_t captured = c->launches - l0;
+    c->launches = l0;
+    bool ok = rc == 0 && ec == cudaSuccess && graph != nullptr;
+    if (ok) ok = cudaGraphInstantiate(&g.exec, graph, 0) == cudaSuccess;
+    if (graph) cudaGraphDestroy(graph);
+    if (!ok) {
+        cudaGetLastError();
+        g.reset();
+        return false;
+    }
+    for (int k = 0; k < 6; ++k) g.sig[k] = sig[k];
+    g.launches = captured;
+    return true;
+}
+
+// Run body(c) through the graph g when possible, directly otherwise.
+template <typename F>
+static int run_loop(hrn_ctx *c, LoopGraph &g, const uint64_t (&sig)[6], F body)
+{
+    if (graph_usable(c)) {
+        bool same = g.exec != nullptr;
+        for (int k = 0; k < 6 && same; ++k) same = g.sig[k] == sig[k];
+        if (!same && graph_capture(c, g, sig, body)) {
+            same = true;
+            ++c->graph_captures;
+        }
+        if (same) {
+            HRN_CUDA(c, cudaGraphLaunch(g.exec, c->stream));
+            c->launches += g.launches;
+            ++c->graph_replays;
+            return 0;
+        }
+    }
+    return body();
+}
+
 template <typename T, int S>
 static int forward_t(hrn_ctx *c)
 {
     const size_t vn = size_t(c->neq) * S;
     T *X0 = c->d_X.as<T>(), *X1 = X0 + 3 * vn;
-    cudaEvent_t t0, t1;
-    cudaEventCreate(&t0);
-    cudaEventCreate(&t1);
-    cudaEventRecord(t0, c->stream);
-    HRN_CUDA(c, cudaMemsetAsync(X0, 0, 3 * vn * sizeof(T), c->stream));
-    if (c->nslot_f > 0) {
-        const int64_t tot = int64_t(c->nstep + 1) * c->nslot_f * S;
-        k_src_fwd<T, S><<<blocks_for(tot, 256), 256, 0, c->stream>>>(c->nstep, c->nslot_f, c->d_fslot_eq.as<int32_t>(),
-                                                                     c->d_fsrc_b.as<double>(), c->d_ftab.as<double>(),
-                                                                     c->d_im.as<double>(), c->d_srcv_f.as<T>()); ++c->launches;
-        HRN_CUDA(c, cudaGetLastError());
-    }
     StageArgs<T> a = forward_args<T, S>(c);
     TileArgs ta{c->d_tiles.as<int32_t>(), c->ntiles, std::min(c->ntiles, 2 * c->num_sms), c->d_step_err.as<int>()};
+    // variant choice and its tables: host work, before any capture
     if (c->lanes_f <= 0) {
+        // first use: the source table, then time the variants on the zero state
+        HRN_CUDA(c, cudaMemsetAsync(X0, 0, 3 * vn * sizeof(T), c->stream));
+        if (c->nslot_f > 0) {
+            const int64_t tot = int64_t(c->nstep + 1) * c->nslot_f * S;
+            k_src_fwd<T, S><<<blocks_for(tot, 256), 256, 0, c->stream>>>(c->nstep, c->nslot_f, c->d_fslot_eq.as<int32_t>(),
+                                                                         c->d_fsrc_b.as<double>(), c->d_ftab.as<double>(),
+                                                                         c->d_im.as<double>(), c->d_srcv_f.as<T>()); ++c->launches;
+            HRN_CUDA(c, cudaGetLastError());
+        }
         a.srcv = c->d_srcv_f.as<T>();
         const int r = autotune_lanes<T, S>(c, a, X0, X1, ta, 0);
         if (r < 40) return r;
         c->lanes_f = r;
-        HRN_CUDA(c, cudaMemsetAsync(X0, 0, 3 * vn * sizeof(T), c->stream));
-    } else if (is_elem_variant(c->lanes_f)) {
+    }
+    if (is_elem_variant(c->lanes_f)) {
         if (!elem_variant_valid(c, c->lanes_f)) return set_error(c, HRN_EARG, "matrix-free variant not available for this shot count and precision");
         if (int rc = elem_ready(c)) return rc;
     } else if (is_gt_variant(c->lanes_f)) {
         if (int rc = gt_ready(c, 0)) return rc;
     }
+    cudaEvent_t t0, t1;
+    cudaEventCreate(&t0);
+    cudaEventCreate(&t1);
+    cudaEventRecord(t0, c->stream);
     StageTimer tm(c);
-    const int K = c->ckpt;
-    for (int n = 0; n <= c->nstep; ++n) {
-        a.srcv = forward_src<T, S>(c, n);
-        T *X = (n & 1) ? X1 : X0, *Y = (n & 1) ? X0 : X1;
-        if (K > 0) {
-            // checkpointed: the state every K steps and the receiver rows of every step
-            if (n % K == 0)
-                HRN_CUDA(c, cudaMemcpyAsync(c->d_ckpt.as<T>() + size_t(n / K) * 3 * vn, X, 3 * vn * sizeof(T),
-                                            cudaMemcpyDeviceToDevice, c->stream));
-            if (c->nrec3 > 0) {
-                k_traces<T, S><<<(c->nrec3 * S + 127) / 128, 128, 0, c->stream>>>(
-                    c->nrec3, c->d_eqdis.as<int32_t>(), X + vn, c->d_traces.as<T>() + size_t(n) * c->nrec3 * S);
-                ++c->launches;
-            }
-            a.hist = nullptr;
-        } else {
-            a.hist = c->d_hist.as<T>() + size_t(n) * c->nstore * S;
+    // stream work only: memsets, source table, every step
+    auto body = [&]() -> int {
+        HRN_CUDA(c, cudaMemsetAsync(X0, 0, 3 * vn * sizeof(T), c->stream));
+        if (c->nslot_f > 0) {
+            const int64_t tot = int64_t(c->nstep + 1) * c->nslot_f * S;
+            k_src_fwd<T, S><<<blocks_for(tot, 256), 256, 0, c->stream>>>(c->nstep, c->nslot_f, c->d_fslot_eq.as<int32_t>(),
+                                                                         c->d_fsrc_b.as<double>(), c->d_ftab.as<double>(),
+                                                                         c->d_im.as<double>(), c->d_srcv_f.as<T>()); ++c->launches;
+            HRN_CUDA(c, cudaGetLastError());
         }
-        launch_step<T, S>(c, a, X, Y, c->timing ? &tm : nullptr, c->lanes_f, ta, 0);
-    }
-    HRN_CUDA(c, cudaGetLastError());
+        const int K = c->ckpt;
+        for (int n = 0; n <= c->nstep; ++n) {
+            a.srcv = forward_src<T, S>(c, n);
+            T *X = (n & 1) ? X1 : X0, *Y = (n & 1) ? X0 : X1;
+            if (K > 0) {
+                // checkpointed: the state every K steps and the receiver rows of every step
+                if (n % K == 0)
+                    HRN_CUDA(c, cudaMemcpyAsync(c->d_ckpt.as<T>() + size_t(n / K) * 3 * vn, X, 3 * vn * sizeof(T),
+                                                cudaMemcpyDeviceToDevice, c->stream));
+                if (c->nrec3 > 0) {
+                    k_traces<T, S><<<(c->nrec3 * S + 127) / 128, 128, 0, c->stream>>>(
+                        c->nrec3, c->d_eqdis.as<int32_t>(), X + vn, c->d_traces.as<T>() + size_t(n) * c->nrec3 * S);
+                    ++c->launches;
+                }
+                a.hist = nullptr;
+            } else {
+                a.hist = c->d_hist.as<T>() + size_t(n) * c->nstore * S;
+            }
+            launch_step<T, S>(c, a, X, Y, c->timing ? &tm : nullptr, c->lanes_f, ta, 0);
+        }
+        HRN_CUDA(c, cudaGetLastError());
+        return 0;
+    };
+    const uint64_t sig[6] = {alloc_generation().load(), c->epoch, uint64_t(c->lanes_f), 0, 0, uintptr_t(c->stream)};
+    const int rc = run_loop(c, c->gfwd, sig, body);
     cudaEventRecord(t1, c->stream);
+    if (rc) {
+        cudaEventDestroy(t0);
+        cudaEventDestroy(t1);
+        return rc;
+    }
     HRN_CUDA(c, cudaEventSynchronize(t1));
     float ms = 0.f;
     cudaEventElapsedTime(&ms, t0, t1);
@@ -887,7 +974,7 @@ static int forward_t(hrn_ctx *c)
     c->last_stage_launches = c->timing ? int64_t(tm.used / 2) : 0;
     c->acc_stage_ms += c->last_stage_ms;
     c->acc_stage_launches += c->last_stage_launches;
-    if (int rc = check_step_error(c)) return rc;
+    if (int rc2 = check_step_error(c)) return rc2;
     c->have_forward = true;
     c->have_phist = false;
     return 0;
@@ -899,17 +986,7 @@ static int adjoint_t(hrn_ctx *c, int lambda_2mu, int keep_p)
     if (int rc = build_rd_store(c)) return rc;
     const size_t vn = size_t(c->neq) * S;
     T *X0 = c->d_X.as<T>(), *X1 = X0 + 3 * vn;
-    cudaEvent_t t0, t1;
-    cudaEventCreate(&t0);
-    cudaEventCreate(&t1);
-    cudaEventRecord(t0, c->stream);
-    HRN_CUDA(c, cudaMemsetAsync(X0, 0, 3 * vn * sizeof(T), c->stream));
-    HRN_CUDA(c, cudaMemsetAsync(c->d_g.p, 0, size_t(2) * c->nj * 8, c->stream));
-    if (keep_p) {
-        const size_t hb = size_t(c->nstep + 1) * c->nstore * S * sizeof(T);
-        HRN_CUDA(c, c->d_phist.alloc(hb));
-        HRN_CUDA(c, cudaMemsetAsync(c->d_phist.p, 0, hb, c->stream));
-    }
+    if (keep_p) HRN_CUDA(c, c->d_phist.alloc(size_t(c->nstep + 1) * c->nstore * S * sizeof(T)));
     StageArgs<T> a{};
     a.n = c->neq;
     a.rowptr = c->d_rowptrT.as<int32_t>();
@@ -924,12 +1001,14 @@ static int adjoint_t(hrn_ctx *c, int lambda_2mu, int keep_p)
     a.D = T(-c->dt);
     a.d6 = T(-c->dt / 6.0);
     TileArgs ta{c->d_tilesT.as<int32_t>(), c->ntilesT, std::min(c->ntilesT, 2 * c->num_sms), c->d_step_err.as<int>()};
+    // variant choice and its tables: host work, before any capture
     if (c->lanes_a <= 0) {
+        HRN_CUDA(c, cudaMemsetAsync(X0, 0, 3 * vn * sizeof(T), c->stream));
         const int r = autotune_lanes<T, S>(c, a, X0, X1, ta, 1);
         if (r < 40) return r;
         c->lanes_a = r;
-        HRN_CUDA(c, cudaMemsetAsync(X0, 0, 3 * vn * sizeof(T), c->stream));
-    } else if (is_elem_variant(c->lanes_a)) {
+    }
+    if (is_elem_variant(c->lanes_a)) {
         if (!elem_variant_valid(c, c->lanes_a)) return set_error(c, HRN_EARG, "matrix-free variant not available for this shot count and precision");
         if (int rc = elem_ready(c)) return rc;
     } else if (is_gt_variant(c->lanes_a)) {
@@ -937,6 +1016,10 @@ static int adjoint_t(hrn_ctx *c, int lambda_2mu, int keep_p)
     }
     if (c->ckpt > 0 && is_gt_variant(c->lanes_f))   // the recomputed forward segments
         if (int rc = gt_ready(c, 0)) return rc;
+    cudaEvent_t t0, t1;
+    cudaEventCreate(&t0);
+    cudaEventCreate(&t1);
+    cudaEventRecord(t0, c->stream);
     StageTimer tm(c);
     double *gl = c->d_g.as<double>(), *gmu = gl + c->nj;
     const int gblocks = (c->nel_rd + kGradElems - 1) / kGradElems;
@@ -944,40 +1027,56 @@ static int adjoint_t(hrn_ctx *c, int lambda_2mu, int keep_p)
     const int K = c->ckpt;
     StageArgs<T> af = forward_args<T, S>(c);
     TileArgs taf{c->d_tiles.as<int32_t>(), c->ntiles, std::min(c->ntiles, 2 * c->num_sms), c->d_step_err.as<int>()};
-    int it = 0;
-    for (int n = c->nstep; n >= 1; --n, ++it) {
-        const int k0 = K > 0 ? (n / K) * K : 0;   // first step of n's checkpoint segment
-        if (K > 0 && (n == c->nstep || n % K == K - 1)) {
-            // recompute the forward history of steps k0 .. min(k0 + K - 1, nstep - 1) from the checkpoint
-            T *R0 = c->d_Xr.as<T>(), *R1 = R0 + 3 * vn;
-            HRN_CUDA(c, cudaMemcpyAsync(R0, c->d_ckpt.as<T>() + size_t(n / K) * 3 * vn, 3 * vn * sizeof(T),
-                                        cudaMemcpyDeviceToDevice, c->stream));
-            const int m1 = std::min(k0 + K - 1, c->nstep - 1);
-            for (int m = k0; m <= m1; ++m) {
-                af.srcv = forward_src<T, S>(c, m);
-                af.hist = c->d_ckseg.as<T>() + size_t(m - k0) * c->nstore * S;
-                T *Xm = ((m - k0) & 1) ? R1 : R0, *Ym = ((m - k0) & 1) ? R0 : R1;
-                launch_step<T, S>(c, af, Xm, Ym, c->timing ? &tm : nullptr, c->lanes_f, taf, 0);
+    // stream work only: memsets, every adjoint step with its sources, the recomputed
+    // forward segments and the gradient
+    auto body = [&]() -> int {
+        HRN_CUDA(c, cudaMemsetAsync(X0, 0, 3 * vn * sizeof(T), c->stream));
+        HRN_CUDA(c, cudaMemsetAsync(c->d_g.p, 0, size_t(2) * c->nj * 8, c->stream));
+        if (keep_p) HRN_CUDA(c, cudaMemsetAsync(c->d_phist.p, 0, c->d_phist.bytes, c->stream));
+        int it = 0;
+        for (int n = c->nstep; n >= 1; --n, ++it) {
+            const int k0 = K > 0 ? (n / K) * K : 0;   // first step of n's checkpoint segment
+            if (K > 0 && (n == c->nstep || n % K == K - 1)) {
+                // recompute the forward history of steps k0 .. min(k0 + K - 1, nstep - 1) from the checkpoint
+                T *R0 = c->d_Xr.as<T>(), *R1 = R0 + 3 * vn;
+                HRN_CUDA(c, cudaMemcpyAsync(R0, c->d_ckpt.as<T>() + size_t(n / K) * 3 * vn, 3 * vn * sizeof(T),
+                                            cudaMemcpyDeviceToDevice, c->stream));
+                const int m1 = std::min(k0 + K - 1, c->nstep - 1);
+                for (int m = k0; m <= m1; ++m) {
+                    af.srcv = forward_src<T, S>(c, m);
+                    af.hist = c->d_ckseg.as<T>() + size_t(m - k0) * c->nstore * S;
+                    T *Xm = ((m - k0) & 1) ? R1 : R0, *Ym = ((m - k0) & 1) ? R0 : R1;
+                    launch_step<T, S>(c, af, Xm, Ym, c->timing ? &tm : nullptr, c->lanes_f, taf, 0);
+                }
             }
+            const T *u_n = K > 0 ? c->d_ckseg.as<T>() + size_t(n - k0) * c->nstore * S
+                                 : c->d_hist.as<T>() + size_t(n) * c->nstore * S;
+            if (c->nslot_a > 0)
+                k_src_adj<T, S><<<(c->nslot_a * S + 127) / 128, 128, 0, c->stream>>>(
+                    n, c->nstep, rv.stride, c->nrec3, c->nslot_a, c->d_aslot_ptr.as<int32_t>(), c->d_aslot_q.as<int32_t>(),
+                    c->d_aslot_eq.as<int32_t>(), rv.map, static_cast<const T *>(rv.hist), c->d_dis.as<double>(),
+                    c->d_im.as<double>(), c->d_srcv_a.as<T>(), shot_nstep_ptr(c), rec_mask_ptr(c)); ++c->launches;
+            a.hist = keep_p ? c->d_phist.as<T>() + size_t(n) * c->nstore * S : nullptr;
+            T *X = (it & 1) ? X1 : X0, *Y = (it & 1) ? X0 : X1;
+            launch_step<T, S>(c, a, X, Y, c->timing ? &tm : nullptr, c->lanes_a, ta, 1);
+            if (n <= c->nstep - 1 && c->nel_rd > 0)
+                k_gradient<T, S><<<gblocks, 128, 0, c->stream>>>(c->nel_rd, c->d_rd_store.as<int32_t>(), c->d_rd_elems.as<int32_t>(),
+                                                                 c->d_inod.as<int32_t>(), c->d_rd_geom.as<double>(),
+                                                                 u_n, X + vn,
+                                                                 c->d_store_eq.as<int32_t>(), gl, gmu, c->dt, lambda_2mu); ++c->launches;
         }
-        const T *u_n = K > 0 ? c->d_ckseg.as<T>() + size_t(n - k0) * c->nstore * S
-                             : c->d_hist.as<T>() + size_t(n) * c->nstore * S;
-        if (c->nslot_a > 0)
-            k_src_adj<T, S><<<(c->nslot_a * S + 127) / 128, 128, 0, c->stream>>>(
-                n, c->nstep, rv.stride, c->nrec3, c->nslot_a, c->d_aslot_ptr.as<int32_t>(), c->d_aslot_q.as<int32_t>(),
-                c->d_aslot_eq.as<int32_t>(), rv.map, static_cast<const T *>(rv.hist), c->d_dis.as<double>(),
-                c->d_im.as<double>(), c->d_srcv_a.as<T>(), shot_nstep_ptr(c), rec_mask_ptr(c)); ++c->launches;
-        a.hist = keep_p ? c->d_phist.as<T>() + size_t(n) * c->nstore * S : nullptr;
-        T *X = (it & 1) ? X1 : X0, *Y = (it & 1) ? X0 : X1;
-        launch_step<T, S>(c, a, X, Y, c->timing ? &tm : nullptr, c->lanes_a, ta, 1);
-        if (n <= c->nstep - 1 && c->nel_rd > 0)
-            k_gradient<T, S><<<gblocks, 128, 0, c->stream>>>(c->nel_rd, c->d_rd_store.as<int32_t>(), c->d_rd_elems.as<int32_t>(),
-                                                             c->d_inod.as<int32_t>(), c->d_rd_geom.as<double>(),
-                                                             u_n, X + vn,
-                                                             c->d_store_eq.as<int32_t>(), gl, gmu, c->dt, lambda_2mu); ++c->launches;
-    }
-    HRN_CUDA(c, cudaGetLastError());
+        HRN_CUDA(c, cudaGetLastError());
+        return 0;
+    };
+    const uint64_t sig[6] = {alloc_generation().load(), c->epoch, uint64_t(c->lanes_a) | (uint64_t(c->lanes_f) << 32),
+                             uint64_t(keep_p != 0), uint64_t(lambda_2mu != 0), uintptr_t(c->stream)};
+    const int rc = run_loop(c, c->gadj, sig, body);
     cudaEventRecord(t1, c->stream);
+    if (rc) {
+        cudaEventDestroy(t0);
+        cudaEventDestroy(t1);
+        return rc;
+    }
     HRN_CUDA(c, cudaEventSynchronize(t1));
     float ms = 0.f;
     cudaEventElapsedTime(&ms, t0, t1);
@@ -988,7 +1087,7 @@ static int adjoint_t(hrn_ctx *c, int lambda_2mu, int keep_p)
     c->last_stage_launches = c->timing ? int64_t(tm.used / 2) : 0;
     c->acc_stage_ms += c->last_stage_ms;
     c->acc_stage_launches += c->last_stage_launches;
-    if (int rc = check_step_error(c)) return rc;
+    if (int rc2 = check_step_error(c)) return rc2;
     c->have_phist = keep_p != 0;
     return 0;
 }

@@ -67,6 +67,17 @@ class Solver:
     def set_stream(self, stream_ptr: int | None):
         self._check(self._L.hrn_set_stream(self.h, C.c_void_p(stream_ptr or 0)))
 
+    def set_graphs(self, on: bool):
+        """Capture each forward / adjoint call's launches as a CUDA graph and replay
+        it on later calls (on by default)."""
+        self._check(self._L.hrn_set_graphs(self.h, int(bool(on))))
+
+    def graph_stats(self):
+        """(time loops captured, graph launches) so far."""
+        a, b = C.c_int64(), C.c_int64()
+        self._check(self._L.hrn_graph_stats(self.h, C.byref(a), C.byref(b)))
+        return a.value, b.value
+
     def set_timing(self, on: bool):
         self._check(self._L.hrn_set_timing(self.h, int(bool(on))))
 

@@ -205,6 +205,20 @@ int hrn_lbfgs_direction(hrn_ctx *ctx, int32_t iter, int32_t iter_begin, const do
  * context's own stream).  The caller keeps the stream alive. */
 int hrn_set_stream(hrn_ctx *ctx, void *stream);
 
+/* CUDA graphs of the time loops (on by default).  hrn_forward and
+ * hrn_adjoint_gradient capture all launches of a call -- every stage, source,
+ * history, trace and gradient launch of every step -- into one graph on the
+ * context's stream and replay it on later calls while no setting has changed and
+ * no buffer of the context has been reallocated; new values in the buffers (a
+ * reassembled operator, new data) need no new capture.  Calls with timing on, on
+ * the legacy default stream, or the first call of a variant still to be tuned run
+ * the launches directly.  No reference counterpart: the reference steps with
+ * PETSc calls from the host. */
+int hrn_set_graphs(hrn_ctx *ctx, int32_t enable);
+
+/* Time loops captured and graph launches made by this context so far. */
+int hrn_graph_stats(hrn_ctx *ctx, int64_t *captures, int64_t *replays);
+
 /* With timing on, every launch of the fused RK4 stage kernel is bracketed by
  * CUDA events on the launching stream. */
 int hrn_set_timing(hrn_ctx *ctx, int32_t enable);
