@@ -56,6 +56,11 @@ def parse_args():
                     help="stage-kernel variant for forward and adjoint (0 = chosen by timing on first use)")
     ap.add_argument("--no-graphs", action="store_true",
                     help="launch every kernel directly instead of replaying the captured time loops")
+    ap.add_argument("--workload", choices=["inversion", "uneven"], default="inversion",
+                    help="inversion: the 16x16x8 plain inversion loop (default); uneven: batched uneven "
+                         "shots on the 80x80x40 + PML 4 mesh, FP32 stepping, checkpointed adjoint")
+    ap.add_argument("--length-scale", type=float, default=0.03,
+                    help="uneven workload: record lengths scaled by this factor (a bounded sample)")
     return ap.parse_args()
 
 
@@ -357,6 +362,109 @@ def run_native(args, rank, world, local_rank):
 PRECOND_WEIGHTS = os.path.join(ROOT, "hirensi_b200", "data", "precond_cnn_16x16x8.npz")
 
 
+# ---------------------------------------------------------------------------
+# batched uneven shots on the large mesh
+
+def run_uneven(args, rank, world, local_rank):
+    """64 shots of uneven record length (1500-4000 steps scaled by --length-scale) and
+    receiver count (100-900) on the 80x80x40 + PML 4 mesh (12.7 M equations), planned
+    into batches of 8 by record length (hirensi_b200.batching); per batch: forward with
+    the state checkpointed every 100 steps, misfit, adjoint with recomputed segments and
+    the fused gradient, FP32 stepping with FP64 reductions.  Batches are sharded over
+    ranks.  The unit counts each shot's own steps: DOF x (2 nstep_s + 1) per shot."""
+    import torch
+    from hirensi_b200 import batching as B
+    from hirensi_b200 import build
+    from hirensi_b200.configs import uneven_config
+    from hirensi_b200.solver import Solver
+
+    build.build()
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    t_setup = time.perf_counter()
+    prob = uneven_config(length_scale=args.length_scale)
+    m = prob.mesh
+    lengths = [sh.nstep for sh in prob.shots]
+    plan = B.plan(lengths, 8)
+    mine = plan[rank::world]
+    s = Solver("fp32", device=local_rank)
+    s.set_graphs(not args.no_graphs)
+    s.set_mesh(m, prob.rho_el)
+    s.assemble(prob.lam, prob.mu)
+    s.set_history(m.store_eq)
+    s.set_checkpointing(100)
+    if args.variant:
+        s.set_variant(args.variant, args.variant)
+
+    def run_batch(ids):
+        b = B.pack(prob.shots, ids)
+        B.configure(s, b, prob.dt, m.store_position)
+        s.set_data(np.zeros((len(ids), len(b.eqdis), b.nstep + 1)))
+        s.forward()
+        s.misfit(None)
+        s.adjoint_gradient(None, to_host=False)
+
+    # warm-up: tunes the stage variants on this operator and builds their tables
+    run_batch(mine[0])
+    torch.cuda.synchronize(dev)
+    setup_s = time.perf_counter() - t_setup
+    clk = ClockSampler(local_rank)
+    clk.start()
+    l0 = s.launch_count()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for ids in mine:
+        run_batch(ids)
+    e1.record()
+    torch.cuda.synchronize(dev)
+    ms = e0.elapsed_time(e1)
+    clocks = clk.stop()
+    launches = s.launch_count() - l0
+    units = sum(prob.dof * (2 * lengths[i] + 1) for ids in mine for i in ids)
+    if world > 1:
+        import torch.distributed as dist
+        t = torch.tensor([ms, units], dtype=torch.float64, device=dev)
+        dist.all_reduce(t[:1], op=dist.ReduceOp.MAX)
+        dist.all_reduce(t[1:], op=dist.ReduceOp.SUM)
+        ms, units = float(t[0]), float(t[1])
+    # roofline: per-launch stage times of one batch's forward
+    b0 = B.pack(prob.shots, mine[0])
+    B.configure(s, b0, prob.dt, m.store_position)
+    s.set_timing(True)
+    t0 = s.last_timing()
+    s.forward()
+    t1 = s.last_timing()
+    s.set_timing(False)
+    stage_us = (t1[1] - t0[1]) / max(t1[2] - t0[2], 1) * 1e3
+    nnz = [int(s.operator_csr(w)[2].size) for w in range(3)]
+    bytes_launch = stage_bytes(sum(nnz), m.neq, len(mine[0]), 4)
+    peak, peak_kind = measured_peaks()
+    kname, _ = stage_kernel_name(s.variant()[0])
+    achieved = bytes_launch / (stage_us * 1e-6) / 1e9
+    result = {"metric": METRIC, "value": units / (ms * 1e-3) / 1e9, "unit": UNIT, "n_gpus": world,
+              "steps": len(mine), "warmup": 1, "ms_per_step": ms / len(mine), "higher_is_better": True,
+              "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+              "data": "synthetic (seeded layered model with ellipsoidal inclusions; zero measured data)",
+              "config": {"workload": prob.name, "equations": m.neq, "dof": prob.dof, "nnz_CKG": nnz,
+                         "shots": len(prob.shots), "batches": len(plan), "shots_per_batch": 8,
+                         "record_lengths": [min(lengths), max(lengths)], "length_scale": args.length_scale,
+                         "receivers_per_shot": [min(len(sh.eqdis) // 3 for sh in prob.shots),
+                                                max(len(sh.eqdis) // 3 for sh in prob.shots)],
+                         "checkpoint_interval": 100, "stage_variant_fwd_adj": list(s.variant()),
+                         "setup_s": setup_s,
+                         "step": "one batch of 8 shots: forward + misfit + checkpointed adjoint with gradient",
+                         "l2": "inputs larger than L2"},
+              "gpu_launches": int(launches),
+              "roofline": {"bound": "hbm", "kernel": kname.replace("double", "float").replace(",4>", ",8>"),
+                           "achieved": achieved, "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
+                           "frac": achieved / peak, "bytes_per_launch": bytes_launch, "avg_launch_us": stage_us,
+                           "traffic": None},
+              "clocks": clocks}
+    s.close()
+    return result
+
+
 def fwi_leg(precision, prob, dis, local_rank, iters, learned=False, target=None, variant=None):
     """Wall time of `iters` L-BFGS iterations (memory 5) of the inversion loop from
     the initial model, all vectors on the device; misfit reduction reached.  With
@@ -471,6 +579,8 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     if args.impl == "reference":
         res = run_reference(args, rank, world)
+    elif args.workload == "uneven":
+        res = run_uneven(args, rank, world, local_rank)
     else:
         res = run_native(args, rank, world, local_rank)
     if rank == 0 and res is not None:

@@ -128,3 +128,76 @@ def forward_config(nstep: int = 2000) -> Problem:
     p.lam_true, p.mu_true, p.lam0, p.mu0 = lam, mu, lam, mu
     p.name = "forward_16x16x8_pml3"
     return p
+
+
+@dataclasses.dataclass
+class UnevenProblem:
+    """Batched uneven shots on a large mesh: nodal lambda, mu, element density and
+    one ``batching.Shot`` per source (no data)."""
+    name: str
+    mesh: Mesh
+    lam: np.ndarray
+    mu: np.ndarray
+    rho_el: np.ndarray
+    dt: float
+    shots: list
+    freqs: np.ndarray
+
+    @property
+    def dof(self) -> int:
+        return self.mesh.rd_dof
+
+
+def uneven_config(seed: int = 0, nx: int = 80, ny: int = 80, nz: int = 40, h: float = 2.5, npml: int = 4,
+                  nshot: int = 64, dt: float = 1.0e-4, lengths=(1500, 4000), receivers=(100, 900),
+                  length_scale: float = 1.0) -> UnevenProblem:
+    """The batched uneven-shot workload: nx x ny x nz 27-node hexahedra (h) plus an
+    npml-element PML; a seeded model of 3-6 horizontal layers (Vs 150-600 m/s,
+    Poisson ratio 0.25-0.40, density 1800-2200 kg/m^3) with 1-3 ellipsoidal Vs
+    inclusions of +-20-40 %; nshot vertical Ricker forces at random surface nodes
+    (5-25 Hz), each with its own record length and 100-900 random surface receivers.
+    length_scale < 1 shortens every record (a bounded sample of the workload)."""
+    from .batching import Shot
+    rng = np.random.default_rng(seed)
+    mesh = box_mesh(nx, ny, nz, h, npml)
+    depth = nz * h
+    nlay = int(rng.integers(3, 7))
+    tops = np.sort(rng.uniform(0.05, 0.9, nlay - 1) * depth)          # interface depths, ascending
+    vs_l = np.sort(rng.uniform(150.0, 600.0, nlay))                    # stiffer with depth
+    nu_l = rng.uniform(0.25, 0.40, nlay)
+    rho_l = rng.uniform(1800.0, 2200.0, nlay) * 1.0e-6
+
+    def layer_of(z):
+        """Layer index of a point: the number of interfaces above it."""
+        return (-np.asarray(z)[..., None] > tops[None, :]).sum(-1)
+
+    lay = layer_of(mesh.xyz[:, 2])
+    vs = vs_l[lay].copy()
+    (x0, x1), (y0, y1), (z0, _) = mesh.rd_box
+    for _ in range(int(rng.integers(1, 4))):
+        c = np.array([rng.uniform(x0, x1), rng.uniform(y0, y1), rng.uniform(z0 * 0.8, z0 * 0.1)])
+        ax = rng.uniform(0.05, 0.2, 3) * np.array([x1 - x0, y1 - y0, -z0])
+        amp = rng.uniform(0.2, 0.4) * rng.choice([-1.0, 1.0])
+        r2 = (((mesh.xyz - c) / ax) ** 2).sum(axis=1)
+        vs = np.where(r2 <= 1.0, vs * (1.0 + amp), vs)
+    vs = extend_into_pml(mesh, vs)
+    lay = extend_into_pml(mesh, lay)
+    nu = nu_l[lay]
+    mu = rho_l[lay] * vs * vs
+    lam = 2.0 * mu * nu / (1.0 - 2.0 * nu)
+    cz = mesh.xyz[mesh.inod, 2].mean(axis=1)
+    rho_el = rho_l[np.clip(layer_of(np.minimum(cz, 0.0)), 0, nlay - 1)]
+    # surface nodes of the regular domain
+    sx, sy, sz = mesh.xyz[:, 0], mesh.xyz[:, 1], mesh.xyz[:, 2]
+    surf = np.nonzero((np.abs(sz) < 1e-9) & (sx >= x0 - 1e-9) & (sx <= x1 + 1e-9) & (sy >= y0 - 1e-9) & (sy <= y1 + 1e-9))[0]
+    shots = []
+    freqs = rng.uniform(5.0, 25.0, nshot)
+    for k in range(nshot):
+        n = int(rng.integers(lengths[0], lengths[1] + 1))
+        n = max(2, int(round(n * length_scale)))
+        src = int(rng.choice(surf))
+        nrec = int(rng.integers(receivers[0], receivers[1] + 1))
+        rec = np.sort(rng.choice(surf, size=nrec, replace=False))
+        shots.append(Shot(mesh.equations([src], comps=(2,)), np.ones(1), time_table(n, dt, 2, float(freqs[k])),
+                          mesh.equations(rec)))
+    return UnevenProblem(f"uneven_{nx}x{ny}x{nz}_pml{npml}_{nshot}shots", mesh, lam, mu, rho_el, dt, shots, freqs)
