@@ -655,6 +655,31 @@ int hrn_forward(hrn_ctx *c)
     return run_forward(c);
 }
 
+int hrn_get_state(hrn_ctx *c, int32_t step, int32_t shot, double *x1, double *x2, double *x3)
+{
+    if (!c) return HRN_EARG;
+    if (!c->have_forward) return set_error(c, HRN_ESTATE, "no forward state: call hrn_forward first");
+    if (c->ckpt <= 0) return set_error(c, HRN_ESTATE, "states are kept only with checkpointing (hrn_set_checkpointing)");
+    if (step < 0 || step > c->nstep || step % c->ckpt != 0)
+        return set_error(c, HRN_EARG, "step must be a multiple of the checkpoint interval within 0..nstep");
+    if (shot < 0 || shot >= c->nshot) return set_error(c, HRN_EARG, "shot out of range");
+    const size_t S = c->nshot, vn = size_t(c->neq) * S, eb = c->elem_bytes();
+    std::vector<unsigned char> h(3 * vn * eb);
+    HRN_CUDA(c, cudaStreamSynchronize(c->stream));
+    HRN_CUDA(c, cudaMemcpy(h.data(), static_cast<const unsigned char *>(c->d_ckpt.p) + size_t(step / c->ckpt) * 3 * vn * eb,
+                           h.size(), cudaMemcpyDeviceToHost));
+    double *out[3] = {x1, x2, x3};
+    for (int k = 0; k < 3; ++k) {
+        if (!out[k]) continue;
+        for (int i = 0; i < c->neq; ++i) {
+            const size_t at = size_t(k) * vn + size_t(i) * S + size_t(shot);
+            out[k][i] = c->precision == HRN_FP64 ? reinterpret_cast<const double *>(h.data())[at]
+                                                 : double(reinterpret_cast<const float *>(h.data())[at]);
+        }
+    }
+    return HRN_OK;
+}
+
 int hrn_get_history(hrn_ctx *c, int32_t shot, double *u_store)
 {
     if (!c || !u_store) return HRN_EARG;

@@ -40,6 +40,7 @@ class Solver:
         self.nrec3 = 0
         self.nj = 0
         self.neq = 0
+        self.ckpt_interval = 0
 
     # -- plumbing ---------------------------------------------------------------
     def _check(self, rc):
@@ -187,6 +188,7 @@ class Solver:
         """0: keep the whole forward history; K > 0: keep the forward state every
         K steps and recompute each segment's history during the adjoint."""
         self._check(self._L.hrn_set_checkpointing(self.h, int(interval)))
+        self.ckpt_interval = int(interval)
 
     def set_variant(self, forward: int = 0, adjoint: int = 0):
         """Force the stage-kernel variant, 0 = chosen by timing on first use.
@@ -215,6 +217,12 @@ class Solver:
         u = np.zeros((self.nstep + 1, self.nstore))
         self._check(self._L.hrn_get_history(self.h, shot, dptr(u)))
         return u
+
+    def state(self, step: int, shot: int = 0):
+        """(x1, x2, x3) [neq] of a shot at a checkpointed step (needs set_checkpointing)."""
+        x = [np.zeros(self.neq) for _ in range(3)]
+        self._check(self._L.hrn_get_state(self.h, int(step), int(shot), *[v.ctypes.data for v in x]))
+        return tuple(x)
 
     def traces(self) -> np.ndarray:
         t = np.zeros((self.nshot, self.nrec3, self.nstep + 1))

@@ -136,6 +136,14 @@ int hrn_get_history(hrn_ctx *ctx, int32_t shot, double *u_store);
 /* Receiver traces U_Store(EqDis_MAP, 0:NStep) of every shot: traces[nshot][nrec3][nstep+1]. */
 int hrn_get_traces(hrn_ctx *ctx, double *traces);
 
+/* Full forward state of one shot at a checkpointed step (step a multiple of the
+ * checkpoint interval, 0 <= step <= NSTEP): x1 (time integral of u), x2 = u and
+ * x3 = du/dt over all equations, [neq] each; NULL skips an array.  This is the
+ * data of the reference's ParaView snapshots, which scatter x2 of every
+ * NSParaview-th step to the nodes (S4/Solver_PETSc_Explicit.F90:936-975,
+ * S4/ParaView.F90:1206-1440); hirensi_b200/snapshots.py writes the files. */
+int hrn_get_state(hrn_ctx *ctx, int32_t step, int32_t shot, double *x1, double *x2, double *x3);
+
 /* Compute_Misfit (S4/Solver_PETSc_Inverse.F90:591-657) summed over shots;
  * dis_meas NULL uses the data of hrn_set_data. */
 int hrn_misfit(hrn_ctx *ctx, const double *dis_meas, double *cost);
