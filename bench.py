@@ -179,7 +179,11 @@ def run_native(args, rank, world, local_rank):
     nstep = 40 if args.profile_case else args.nstep
     prob = inversion_config(nstep=nstep)
     m = prob.mesh
-    stream = torch.cuda.current_stream(dev)
+    # one stream for the library and for torch (copies, the gradient all-reduce): the
+    # library runs a null stream handle on a private non-blocking stream, which torch's
+    # default stream would not be ordered with
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(stream)
 
     def make_solver(precision, variant=True):
         s = Solver(precision, device=local_rank)
@@ -359,7 +363,7 @@ def run_native(args, rank, world, local_rank):
     return result
 
 
-PRECOND_WEIGHTS = os.path.join(ROOT, "hirensi_b200", "data", "precond_cnn_16x16x8.npz")
+PRECOND_WEIGHTS = os.path.join(ROOT, "hirensi_b200", "data", "precond_cnn6_16x16x8.npz")
 
 
 # ---------------------------------------------------------------------------

@@ -42,6 +42,7 @@ SIGNATURES = {
     "hrn_misfit_noalloc": (C.c_int, [VP, VP, PD]),
     "hrn_set_checkpointing": (C.c_int, [VP, C.c_int32]),
     "hrn_illumination": (C.c_int, [VP, VP]),
+    "hrn_pseudo_hessian": (C.c_int, [VP, VP, VP]),
     "hrn_cnn_conv3d_forward": (C.c_int, [C.c_int32] * 5 + [VP, VP, VP, C.c_int32, VP, VP]),
     "hrn_cnn_conv3d_backward": (C.c_int, [C.c_int32] * 5 + [VP, VP, VP, C.c_int32, VP, VP, VP, VP, VP]),
     "hrn_adjoint_gradient": (C.c_int, [VP, PD, C.c_int32, C.c_int32, PD, PD]),

@@ -160,6 +160,7 @@ struct hrn_ctx {
     int nstore = 0;
     std::vector<int32_t> h_store_eq;
     hrn::DevBuf d_store_eq, d_store_pos;      // [nstore], [neq] (-1 = not stored)
+    hrn::DevBuf d_store_iota;                 // [nstore] 0 .. nstore-1 (pseudo-Hessian)
 
     // ---- shots
     int nshot = 0, nstep = 0;
@@ -264,6 +265,7 @@ int launch_scale_operator(hrn_ctx *c);
 int run_forward(hrn_ctx *c);
 int run_adjoint_gradient(hrn_ctx *c, int lambda_2mu, int keep_p);
 int run_misfit(hrn_ctx *c, double *cost);
+int run_pseudo_hessian(hrn_ctx *c, double *hl, double *hm);
 int build_rd_geometry(hrn_ctx *c);
 int assemble_device(hrn_ctx *c, bool discover_pattern);
 int finalize_pattern_from_keys(hrn_ctx *c, const std::vector<uint64_t> &keys);

@@ -335,6 +335,16 @@ int hrn_illumination(hrn_ctx *c, double *d_out)
     return HRN_OK;
 }
 
+int hrn_pseudo_hessian(hrn_ctx *c, double *d_h_lambda, double *d_h_mu)
+{
+    if (!c || !d_h_lambda || !d_h_mu) return HRN_EARG;
+    if (!c->have_forward) return set_error(c, HRN_ESTATE, "no forward history: call hrn_forward first");
+    if (c->ckpt > 0) return set_error(c, HRN_ESTATE, "the pseudo-Hessian needs the whole forward history (checkpointing is on)");
+    if (!c->have_mesh) return set_error(c, HRN_ESTATE, "no mesh: call hrn_set_mesh first");
+    cudaSetDevice(c->device);
+    return run_pseudo_hessian(c, d_h_lambda, d_h_mu);
+}
+
 int hrn_gradient_mass(hrn_ctx *c, double *d_mg)
 {
     if (!c || !d_mg) return HRN_EARG;

@@ -1111,6 +1111,36 @@ static int misfit_t(hrn_ctx *c, double *cost)
     return 0;
 }
 
+// Diagonal pseudo-Hessian of the lambda / mu model: the gradient's zero-lag
+// correlation (k_gradient) with the forward wavefield in place of the adjoint one,
+// sum over n = 1 .. nstep-1 and shots of dt * [ (div u)^2 ] and of the strain-energy
+// term, at the regular-domain nodes.  hl, hm: device arrays [nj].
+template <typename T, int S>
+static int pseudo_hessian_t(hrn_ctx *c, double *hl, double *hm)
+{
+    if (int rc = build_rd_store(c)) return rc;
+    if (c->d_store_iota.bytes != size_t(c->nstore) * 4) {
+        std::vector<int32_t> iota(static_cast<size_t>(c->nstore));
+        for (int i = 0; i < c->nstore; ++i) iota[i] = i;
+        HRN_CUDA(c, c->d_store_iota.alloc(iota.size() * 4));
+        HRN_CUDA(c, cudaMemcpy(c->d_store_iota.p, iota.data(), iota.size() * 4, cudaMemcpyHostToDevice));
+    }
+    HRN_CUDA(c, cudaMemsetAsync(hl, 0, size_t(c->nj) * 8, c->stream));
+    HRN_CUDA(c, cudaMemsetAsync(hm, 0, size_t(c->nj) * 8, c->stream));
+    const int gblocks = (c->nel_rd + kGradElems - 1) / kGradElems;
+    if (c->nel_rd > 0)
+        for (int n = 1; n <= c->nstep - 1; ++n) {
+            const T *u_n = c->d_hist.as<T>() + size_t(n) * c->nstore * S;
+            // p := u: the history row read again through the identity position map
+            k_gradient<T, S><<<gblocks, 128, 0, c->stream>>>(c->nel_rd, c->d_rd_store.as<int32_t>(), c->d_rd_elems.as<int32_t>(),
+                                                             c->d_inod.as<int32_t>(), c->d_rd_geom.as<double>(), u_n, u_n,
+                                                             c->d_store_iota.as<int32_t>(), hl, hm, c->dt, 0);
+            ++c->launches;
+        }
+    HRN_CUDA(c, cudaGetLastError());
+    return 0;
+}
+
 #define HRN_DISPATCH_S(FN, T, ...)                        \
     switch (c->nshot) {                                   \
     case 1: return FN<T, 1>(c, ##__VA_ARGS__);            \
@@ -1134,6 +1164,12 @@ int run_adjoint_gradient(hrn_ctx *c, int lambda_2mu, int keep_p)
 {
     if (c->precision == HRN_FP64) { HRN_DISPATCH_S(adjoint_t, double, lambda_2mu, keep_p) }
     HRN_DISPATCH_S(adjoint_t, float, lambda_2mu, keep_p)
+}
+
+int run_pseudo_hessian(hrn_ctx *c, double *hl, double *hm)
+{
+    if (c->precision == HRN_FP64) { HRN_DISPATCH_S(pseudo_hessian_t, double, hl, hm) }
+    HRN_DISPATCH_S(pseudo_hessian_t, float, hl, hm)
 }
 
 int run_misfit(hrn_ctx *c, double *cost)

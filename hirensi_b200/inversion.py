@@ -219,8 +219,14 @@ class DeviceBackend:
         self.map = torch.from_numpy(np.ascontiguousarray(mesh.extend_to, dtype=np.int32)).to(self.dev)
         self.L = solver._L
         self.h = solver.h
-        # one stream for the library and for the tensors it reads and writes
-        solver.set_stream(torch.cuda.current_stream(self.dev).cuda_stream)
+        # One stream for the library and for the tensors it reads and writes.  A
+        # stream of its own: the library runs a null stream handle on its private
+        # non-blocking stream, which would not be ordered with torch's default stream.
+        self.stream = torch.cuda.Stream(self.dev)
+        solver.set_stream(self.stream.cuda_stream)
+
+    def _on(self):
+        return self.torch.cuda.stream(self.stream)
 
     def _p(self, t):
         return t.data_ptr()
@@ -229,13 +235,16 @@ class DeviceBackend:
         self.s._check(rc)
 
     def zeros(self):
-        return self.torch.zeros(self.n, dtype=self.torch.float64, device=self.dev)
+        with self._on():
+            return self.torch.zeros(self.n, dtype=self.torch.float64, device=self.dev)
 
     def vec(self, host):
-        return self.torch.from_numpy(np.ascontiguousarray(host, dtype=np.float64)).to(self.dev)
+        with self._on():
+            return self.torch.from_numpy(np.ascontiguousarray(host, dtype=np.float64)).to(self.dev)
 
     def host(self, v):
-        return v.cpu().numpy()
+        with self._on():
+            return v.cpu().numpy()
 
     def copy(self, src, dst):
         self.axpby(1.0, src, 0.0, None, dst)
@@ -281,9 +290,10 @@ class DeviceBackend:
         import ctypes as C
         mg = self.zeros()
         self._ck(self.L.hrn_gradient_mass(self.h, C.c_void_p(self._p(mg))))
-        keep = mg > 1.0e-10
-        img = self.torch.where(keep, 1.0 / self.torch.where(keep, mg, self.torch.ones_like(mg)), self.torch.zeros_like(mg))
-        return img.contiguous(), keep.to(self.torch.float64).contiguous()
+        with self._on():
+            keep = mg > 1.0e-10
+            img = self.torch.where(keep, 1.0 / self.torch.where(keep, mg, self.torch.ones_like(mg)), self.torch.zeros_like(mg))
+            return img.contiguous(), keep.to(self.torch.float64).contiguous()
 
     def tv(self, lam, mu, reg_l, reg_m):
         import ctypes as C
@@ -313,6 +323,17 @@ class DeviceBackend:
     def illumination(self):
         """Source illumination of the stored nodes of the last forward (host array)."""
         import ctypes as C
-        out = self.torch.zeros(self.s.nstore // 3, dtype=self.torch.float64, device=self.dev)
-        self._ck(self.L.hrn_illumination(self.h, C.c_void_p(self._p(out))))
-        return out.cpu().numpy()
+        with self._on():
+            out = self.torch.zeros(self.s.nstore // 3, dtype=self.torch.float64, device=self.dev)
+            self._ck(self.L.hrn_illumination(self.h, C.c_void_p(self._p(out))))
+            return out.cpu().numpy()
+
+    def pseudo_hessian(self):
+        """Diagonal pseudo-Hessian (lambda, mu) [nj] of the last forward (host arrays)."""
+        import ctypes as C
+        nj = self.mesh.nj
+        with self._on():
+            out = self.torch.zeros(2, nj, dtype=self.torch.float64, device=self.dev)
+            self._ck(self.L.hrn_pseudo_hessian(self.h, C.c_void_p(self._p(out[0])), C.c_void_p(self._p(out[1]))))
+            h = out.cpu().numpy()
+        return h[0], h[1]

@@ -1,13 +1,14 @@
 """Learned gradient preconditioner of the inversion.
 
-A small 3-D CNN looks at the gradient, the source illumination and the current
-shear-wave speed on the regular-domain node lattice, and returns a positive
+A small 3-D CNN looks at the gradient, the source illumination, the current
+shear-wave speed and (in the 6-input form) the diagonal pseudo-Hessian on the
+regular-domain node lattice, and returns a positive
 diagonal scale D for each of the lambda and mu gradients.  The inversion tries
 the scaled steepest-descent direction -D * g first.  Its Armijo line search on
 the true misfit accepts it, or the iteration falls back to the plain L-BFGS
 direction (``hirensi_b200.inversion.FWI``).
 
-* Network: four 3x3x3 convolutions (4 -> 16 -> 16 -> 16 -> 2 channels, ReLU
+* Network: four 3x3x3 convolutions (4 or 6 -> 16 -> 16 -> 16 -> 2 channels, ReLU
   between), BF16 weights and activations with FP32 accumulation, run by the
   library's own kernels (hrn_cnn_conv3d_forward / _backward).  D = exp(clip(z, -4, 4)).
 * Loss of one sample: sum over lambda, mu of 1 - cos^2(D * q, dm), where q = -g
@@ -28,7 +29,7 @@ import dataclasses
 
 import numpy as np
 
-CH = (4, 16, 16, 16, 2)       # channels of the five activations
+CH = (4, 16, 16, 16, 2)       # channels of the five activations (4-input form)
 ZCLIP = 4.0
 
 
@@ -123,17 +124,28 @@ class Lattice:
         return out
 
 
-def features(lat: Lattice, g_l, g_m, illum_store, vs) -> np.ndarray:
-    """Input channels [4, nz, ny, nx]: the two gradients scaled to unit max, the log
-    illumination standardized, the shear-wave speed / 400."""
+def features(lat: Lattice, g_l, g_m, illum_store, vs, ph=None) -> np.ndarray:
+    """Input channels [4 or 6, nz, ny, nx]: the two gradients scaled to unit max, the
+    log illumination standardized, the shear-wave speed / 400, and with ph = (H_lambda,
+    H_mu) [nj] the log pseudo-Hessian diagonals standardized."""
     def unit(v):
         m = np.abs(v).max()
         return v / m if m > 0 else v
 
+    def log_std(v):
+        v = np.asarray(v, dtype=np.float64)
+        v = np.log(np.maximum(v, 0.0) + 1e-300 + np.max(v) * 1e-12)
+        return (v - v.mean()) / (v.std() + 1e-12)
+
     il = np.zeros(int(np.prod(lat.shape)))
-    il[lat.store_to_voxel] = np.log(np.asarray(illum_store) + 1e-300 + np.max(illum_store) * 1e-12)
-    il = (il - il.mean()) / (il.std() + 1e-12)
-    return np.stack([unit(lat.to_grid(g_l)), unit(lat.to_grid(g_m)), il.reshape(lat.shape), lat.to_grid(vs) / 400.0])
+    il[lat.store_to_voxel] = log_std(illum_store)
+    ch = [unit(lat.to_grid(g_l)), unit(lat.to_grid(g_m)), il.reshape(lat.shape), lat.to_grid(vs) / 400.0]
+    if ph is not None:
+        for h in ph:
+            g = np.zeros(int(np.prod(lat.shape)))
+            g[lat.store_to_voxel] = log_std(np.asarray(h)[lat.store_nodes])
+            ch.append(g.reshape(lat.shape))
+    return np.stack(ch)
 
 
 def cosine_loss(a: np.ndarray, t: np.ndarray):
@@ -152,11 +164,16 @@ def cosine_loss(a: np.ndarray, t: np.ndarray):
 # the network on the device kernels
 
 class Net:
-    def __init__(self, seed: int = 0, weights: dict | None = None):
+    def __init__(self, seed: int = 0, weights: dict | None = None, inputs: int = 4):
+        if weights is not None:
+            inputs = int(np.asarray(weights["w0"]).shape[1])
+        if inputs not in (4, 6):
+            raise ValueError("the network takes 4 or 6 input channels")
+        self.ch = (inputs,) + CH[1:]
         rng = np.random.default_rng(seed)
         self.w, self.b = [], []
         for i in range(4):
-            cin, cout = CH[i], CH[i + 1]
+            cin, cout = self.ch[i], self.ch[i + 1]
             std = np.sqrt(2.0 / (cin * 27)) * (0.1 if i == 3 else 1.0)
             self.w.append(rng.standard_normal((cout, cin, 27)).astype(np.float32) * np.float32(std))
             self.b.append(np.zeros(cout, dtype=np.float32))
@@ -192,7 +209,8 @@ class DeviceNet:
         self.stream = torch.cuda.current_stream(self.dev).cuda_stream
         V = int(np.prod(shape))
         self.V = V
-        self.act = [torch.zeros(c * V, dtype=torch.int16, device=self.dev) for c in CH]   # BF16 bits
+        self.ch = net.ch
+        self.act = [torch.zeros(c * V, dtype=torch.int16, device=self.dev) for c in self.ch]   # BF16 bits
         self.sync_weights()
 
     def _ck(self, rc):
@@ -205,8 +223,9 @@ class DeviceNet:
         self.bd = [t.from_numpy(b).to(self.dev) for b in self.net.b]
 
     def forward(self, x: np.ndarray) -> np.ndarray:
-        """x [4, nz, ny, nx] -> z [2, nz, ny, nx] (the network's last activation)."""
+        """x [inputs, nz, ny, nx] -> z [2, nz, ny, nx] (the network's last activation)."""
         t = self.torch
+        CH = self.ch
         nz, ny, nx = self.shape
         self.act[0].copy_(t.from_numpy(to_bf16_bits(x).view(np.int16).ravel()))
         for i in range(4):
@@ -219,6 +238,7 @@ class DeviceNet:
     def backward(self, gz: np.ndarray):
         """Weight and bias gradients for dL/dz = gz (after a forward of the same input)."""
         t = self.torch
+        CH = self.ch
         nz, ny, nx = self.shape
         gy = t.from_numpy(np.ascontiguousarray(gz, dtype=np.float32).ravel()).to(self.dev)
         gws, gbs = [None] * 4, [None] * 4
@@ -323,7 +343,8 @@ class LearnedPreconditioner:
         gl, gm = backend.host(g_l), backend.host(g_m)
         il = backend.illumination()
         vs = np.sqrt(np.maximum(backend.host(mu), 0.0) / self.rho)
-        x = features(self.lat, gl, gm, il, vs)
+        ph = backend.pseudo_hessian() if self.dnet.ch[0] == 6 else None
+        x = features(self.lat, gl, gm, il, vs, ph)
         D = scale_from_z(self.dnet.forward(x))
         nj = self.mesh.nj
         pl = -self.lat.from_grid(D[0], nj) * gl
@@ -396,7 +417,7 @@ def default_inversion_config():
     return InversionConfig(m_lbfgs=5, bounds_lambda=(10.0, 2000.0), bounds_mu=(10.0, 1000.0))
 
 
-def generate_samples(runner: _Runner, seeds, iters: int = 3, log=None):
+def generate_samples(runner: _Runner, seeds, iters: int = 3, log=None, inputs: int = 4):
     """(x, q, dm) of the first `iters` iterations of a plain inversion of each seeded model."""
     out = []
     nj = runner.prob.mesh.nj
@@ -410,7 +431,7 @@ def generate_samples(runner: _Runner, seeds, iters: int = 3, log=None):
             gl, gm = b.host(g_l), b.host(g_m)
             lh, mh = b.host(lam), b.host(mu)
             vs = np.sqrt(np.maximum(mh, 0.0) / runner.rho)
-            x = features(runner.lat, gl, gm, b.illumination(), vs)
+            x = features(runner.lat, gl, gm, b.illumination(), vs, b.pseudo_hessian() if inputs == 6 else None)
             q = np.stack([runner.lat.to_grid(-gl), runner.lat.to_grid(-gm)])
             dm = np.stack([runner.lat.to_grid(lam_t - lh), runner.lat.to_grid(mu_t - mh)])
             out.append((x, q, dm))
@@ -466,6 +487,8 @@ def main(argv=None):
     ap.add_argument("--nstep", type=int, default=2000)
     ap.add_argument("--fwi-iters", type=int, default=10)
     ap.add_argument("--eval-only", help="skip training: evaluate these weights")
+    ap.add_argument("--inputs", type=int, choices=[4, 6], default=6,
+                    help="input channels: 4 = gradients, illumination, Vs; 6 = also the pseudo-Hessian diagonals")
     a = ap.parse_args(argv)
     t0 = time.time()
     prob = inversion_config(nstep=a.nstep)
@@ -475,10 +498,10 @@ def main(argv=None):
         for g in fwi_gain(runner, dnet, range(5000, 5000 + a.eval_models), a.fwi_iters):
             print(g, flush=True)
         return
-    train_s = generate_samples(runner, range(1000, 1000 + a.models), a.iters)
-    eval_s = generate_samples(runner, range(5000, 5000 + a.eval_models), a.iters)
+    train_s = generate_samples(runner, range(1000, 1000 + a.models), a.iters, inputs=a.inputs)
+    eval_s = generate_samples(runner, range(5000, 5000 + a.eval_models), a.iters, inputs=a.inputs)
     t_data = time.time() - t0
-    dnet = DeviceNet(Net(seed=0), runner.lat.shape)
+    dnet = DeviceNet(Net(seed=0, inputs=a.inputs), runner.lat.shape)
     hist = train(dnet, train_s, epochs=a.epochs, lr=a.lr, log=lambda ep, L: print(f"epoch {ep} loss {L:.4f}", flush=True))
     t_train = time.time() - t0 - t_data
     ev_net, ev_one = evaluate(dnet, eval_s)
@@ -487,7 +510,7 @@ def main(argv=None):
     summary = {"train_samples": len(train_s), "eval_samples": len(eval_s), "epochs": a.epochs,
                "loss_first_epoch": hist[0], "loss_last_epoch": hist[-1], "eval_loss_network": ev_net,
                "eval_loss_unscaled_gradient": ev_one, "fwi": gains, "data_s": t_data, "train_s": t_train,
-               "nstep": a.nstep, "shape": list(runner.lat.shape)}
+               "nstep": a.nstep, "shape": list(runner.lat.shape), "inputs": a.inputs}
     with open(a.out.replace(".npz", ".json"), "w") as f:
         json.dump(summary, f, indent=1)
     print(json.dumps({k: v for k, v in summary.items() if k != "fwi"}), flush=True)

@@ -261,6 +261,14 @@ int hrn_launch_count(hrn_ctx *ctx, int64_t *n);
  * the history rows (needs the whole history, i.e. no checkpointing). */
 int hrn_illumination(hrn_ctx *ctx, double *d_out);
 
+/* Diagonal pseudo-Hessian of the lambda / mu model from the forward history: the
+ * zero-lag correlation of the gradient (..._Control_OtD, S4/Element_Matrices_3D.F90:
+ * 1725-1890) with the forward wavefield in place of the adjoint one, i.e.
+ * dt * sum_n sum_shots of (div u)^2 (lambda) and of the strain-energy term (mu),
+ * n = 1 .. NSTEP-1, at the regular-domain nodes.  d_h_lambda, d_h_mu: device
+ * arrays [nj], overwritten.  Needs the whole forward history. */
+int hrn_pseudo_hessian(hrn_ctx *ctx, double *d_h_lambda, double *d_h_mu);
+
 /* 3x3x3 convolution with zero padding on a [channel][nz][ny][nx] grid, BF16 x, w
  * and y, FP32 bias and accumulation: y = act(b + w * x), act = ReLU when relu != 0.
  * w is [cout][cin][27] (tap k = 9 dz + 3 dy + dx).  At most 16 channels in and out.

@@ -91,7 +91,8 @@ def test_trained_network_beats_plain_and_unit_scale_on_held_out_models(gpu_lib):
     import os
     from hirensi_b200.configs import inversion_config
     root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-    weights = os.path.join(root, "hirensi_b200", "data", "precond_cnn_16x16x8.npz")
+    # the network with the pseudo-Hessian inputs, as bench.py uses it
+    weights = os.path.join(root, "hirensi_b200", "data", "precond_cnn6_16x16x8.npz")
     runner = Lr._Runner(inversion_config(nstep=2000), "fp32")
     dnet = Lr.DeviceNet(Lr.Net.load(weights), runner.lat.shape)
     rows = Lr.fwi_gain(runner, dnet, [5000, 5001], n_iter=5)

@@ -65,3 +65,20 @@ def test_lattice_of_box_mesh():
     x = Lr.features(lat, v, -v, np.ones(m.nstore // 3), np.full(m.nj, 200.0))
     assert x.shape == (4, 5, 7, 9)
     assert np.abs(x[0]).max() == 1.0 and np.allclose(x[3], 0.5)
+
+
+def test_features_with_pseudo_hessian_channels():
+    from hirensi_b200.learned import Lattice, features
+    from hirensi_b200.mesh import box_mesh
+    m = box_mesh(2, 2, 1, 2.5, 1)
+    lat = Lattice.of(m)
+    rng = np.random.default_rng(0)
+    nj = m.nj
+    g_l, g_m, vs = rng.standard_normal(nj), rng.standard_normal(nj), 200.0 + rng.random(nj)
+    il = rng.random(len(m.store_nodes)) + 0.1
+    x4 = features(lat, g_l, g_m, il, vs)
+    x6 = features(lat, g_l, g_m, il, vs, (rng.random(nj) + 1e-3, rng.random(nj) + 1e-3))
+    assert x4.shape == (4,) + lat.shape and x6.shape == (6,) + lat.shape
+    assert np.array_equal(x6[:4], x4)
+    for c in (4, 5):
+        assert abs(x6[c].mean()) < 1e-9 and abs(x6[c].std() - 1.0) < 1e-9
