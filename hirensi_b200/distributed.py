@@ -49,7 +49,14 @@ class ShotParallelBackend:
 
     def _allreduce(self, x):
         t = self._torch.from_numpy(x) if isinstance(x, np.ndarray) else x
-        self._dist.all_reduce(t, op=self._dist.ReduceOp.SUM, group=self.group)
+        stream = getattr(self.backend, "stream", None)
+        if stream is not None and not isinstance(x, np.ndarray):
+            # device vectors: order the collective after the library's kernels on the
+            # backend's stream, and later work on that stream after the collective
+            with self._torch.cuda.stream(stream):
+                self._dist.all_reduce(t, op=self._dist.ReduceOp.SUM, group=self.group)
+        else:
+            self._dist.all_reduce(t, op=self._dist.ReduceOp.SUM, group=self.group)
 
     def forward(self, lam, mu):
         j = np.array([self.backend.forward(lam, mu)], dtype=np.float64)
