@@ -124,3 +124,18 @@ def test_staged_tiles_split_to_fit_shared_memory(gpu_lib):
     for k in range(nshot):
         assert np.abs(hists[81][k]).max() > 0
         assert np.array_equal(hists[85][k], hists[81][k])
+
+
+@pytest.mark.parametrize("nshot,precision", [(5, "fp64"), (6, "fp64"), (7, "fp32"), (6, "fp32")])
+def test_staged_tiles_odd_shot_counts(gpu_lib, nshot, precision):
+    """Shot counts whose records take the scalar and 2-wide shared-memory paths."""
+    p = tiny(nshot=nshot, nstep=60)
+    out = {}
+    for v in (45, 41):
+        with _assembled_solver(p, p["lam"], p["mu"], precision) as s:
+            s.set_variant(v, v)
+            s.forward()
+            out[v] = [s.history(k) for k in range(nshot)]
+    for k in range(nshot):
+        assert np.abs(out[41][k]).max() > 0
+        assert np.array_equal(out[45][k], out[41][k])
