@@ -560,12 +560,15 @@ def run_reference(args, rank, world):
     v = float(np.median([x["value"] for x in vals]))
     cb = dict(vals[-1])
     cb["value"] = v
+    # one step of the workload (4 shots, forward + adjoint) at the sampled rate
+    units_per_step = prob.dof * ((prob.nstep + 1) + prob.nstep) * prob.nshot
     return {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "ms_per_step": units_per_step / (v * 1e9) * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic", "impl": "reference",
             "config": {"workload": prob.name + f"_4shots_{prob.nstep}steps", "dof": prob.dof,
                        "note": "CPU restatement of the reference solver (Fortran + PETSc not in the image); "
-                               "each step is a bounded sample: 1 shot, 51 forward + 50 adjoint steps"},
+                               "each step is a bounded sample: 1 shot, 51 forward + 50 adjoint steps; "
+                               "ms_per_step is the whole workload step at the sampled rate"},
             "cpu_baseline": cb, "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
