@@ -61,6 +61,8 @@ def parse_args():
                          "shots on the 80x80x40 + PML 4 mesh, FP32 stepping, checkpointed adjoint")
     ap.add_argument("--length-scale", type=float, default=0.03,
                     help="uneven workload: record lengths scaled by this factor (a bounded sample)")
+    ap.add_argument("--inflight", type=int, default=2,
+                    help="uneven workload: batches in flight at once, each on its own context and stream")
     return ap.parse_args()
 
 
@@ -375,7 +377,8 @@ def run_uneven(args, rank, world, local_rank):
     into batches of 8 by record length (hirensi_b200.batching); per batch: forward with
     the state checkpointed every 100 steps, misfit, adjoint with recomputed segments and
     the fused gradient, FP32 stepping with FP64 reductions.  Batches are sharded over
-    ranks.  The unit counts each shot's own steps: DOF x (2 nstep_s + 1) per shot."""
+    ranks, and --inflight batches run at once on separate contexts (streams) of a GPU.
+    The unit counts each shot's own steps: DOF x (2 nstep_s + 1) per shot."""
     import torch
     from hirensi_b200 import batching as B
     from hirensi_b200 import build
@@ -391,40 +394,72 @@ def run_uneven(args, rank, world, local_rank):
     lengths = [sh.nstep for sh in prob.shots]
     plan = B.plan(lengths, 8)
     mine = plan[rank::world]
-    s = Solver("fp32", device=local_rank)
-    s.set_graphs(not args.no_graphs)
-    s.set_mesh(m, prob.rho_el)
-    s.assemble(prob.lam, prob.mu)
-    s.set_history(m.store_eq)
-    s.set_checkpointing(100)
+    import threading
+
+    def make_solver():
+        sv = Solver("fp32", device=local_rank)
+        sv.set_graphs(not args.no_graphs)
+        sv.set_mesh(m, prob.rho_el)
+        sv.assemble(prob.lam, prob.mu)
+        sv.set_history(m.store_eq)
+        sv.set_checkpointing(100)
+        return sv
+
+    def run_batch(sv, ids):
+        b = B.pack(prob.shots, ids)
+        B.configure(sv, b, prob.dt, m.store_position)
+        sv.set_data(np.zeros((len(ids), len(b.eqdis), b.nstep + 1)))
+        sv.forward()
+        sv.misfit(None)
+        sv.adjoint_gradient(None, to_host=False)
+
+    # warm-up: the first context tunes the stage variants on this operator; the others
+    # take its choice; each builds its tables on one batch
+    solvers = [make_solver() for _ in range(max(1, args.inflight))]
+    s = solvers[0]
     if args.variant:
         s.set_variant(args.variant, args.variant)
-
-    def run_batch(ids):
-        b = B.pack(prob.shots, ids)
-        B.configure(s, b, prob.dt, m.store_position)
-        s.set_data(np.zeros((len(ids), len(b.eqdis), b.nstep + 1)))
-        s.forward()
-        s.misfit(None)
-        s.adjoint_gradient(None, to_host=False)
-
-    # warm-up: tunes the stage variants on this operator and builds their tables
-    run_batch(mine[0])
+    run_batch(s, mine[0])
+    for sv in solvers[1:]:
+        sv.set_variant(*s.variant())
+        run_batch(sv, mine[0])
     torch.cuda.synchronize(dev)
     setup_s = time.perf_counter() - t_setup
     clk = ClockSampler(local_rank)
     clk.start()
-    l0 = s.launch_count()
+    l0 = sum(sv.launch_count() for sv in solvers)
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
+    # the batches in flight: each context (its own stream) takes the next batch in turn;
+    # every library call blocks its host thread until its work is done
+    queue = list(mine)
+    lock = threading.Lock()
+    errors = []
+
+    def worker(sv):
+        try:
+            while True:
+                with lock:
+                    if not queue:
+                        return
+                    ids = queue.pop(0)
+                run_batch(sv, ids)
+        except Exception as exc:   # reported after the join
+            errors.append(exc)
+
     e0.record()
-    for ids in mine:
-        run_batch(ids)
+    threads = [threading.Thread(target=worker, args=(sv,)) for sv in solvers]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join()
     e1.record()
     torch.cuda.synchronize(dev)
+    if errors:
+        raise errors[0]
     ms = e0.elapsed_time(e1)
     clocks = clk.stop()
-    launches = s.launch_count() - l0
+    launches = sum(sv.launch_count() for sv in solvers) - l0
     units = sum(prob.dof * (2 * lengths[i] + 1) for ids in mine for i in ids)
     if world > 1:
         import torch.distributed as dist
@@ -456,6 +491,7 @@ def run_uneven(args, rank, world, local_rank):
                          "receivers_per_shot": [min(len(sh.eqdis) // 3 for sh in prob.shots),
                                                 max(len(sh.eqdis) // 3 for sh in prob.shots)],
                          "checkpoint_interval": 100, "stage_variant_fwd_adj": list(s.variant()),
+                         "batches_in_flight": len(solvers),
                          "setup_s": setup_s,
                          "step": "one batch of 8 shots: forward + misfit + checkpointed adjoint with gradient",
                          "l2": "inputs larger than L2"},
@@ -465,7 +501,8 @@ def run_uneven(args, rank, world, local_rank):
                            "frac": achieved / peak, "bytes_per_launch": bytes_launch, "avg_launch_us": stage_us,
                            "traffic": None},
               "clocks": clocks}
-    s.close()
+    for sv in solvers:
+        sv.close()
     return result
 
 
