@@ -56,9 +56,11 @@ def parse_args():
                     help="stage-kernel variant for forward and adjoint (0 = chosen by timing on first use)")
     ap.add_argument("--no-graphs", action="store_true",
                     help="launch every kernel directly instead of replaying the captured time loops")
-    ap.add_argument("--workload", choices=["inversion", "uneven"], default="inversion",
+    ap.add_argument("--workload", choices=["inversion", "uneven", "xl"], default="inversion",
                     help="inversion: the 16x16x8 plain inversion loop (default); uneven: batched uneven "
-                         "shots on the 80x80x40 + PML 4 mesh, FP32 stepping, checkpointed adjoint")
+                         "shots on the 80x80x40 + PML 4 mesh, FP32 stepping, checkpointed adjoint; "
+                         "xl: one evaluation on the 160x160x80 + PML 6 mesh (86.6 M equations)")
+    ap.add_argument("--max-batches", type=int, default=0, help="uneven / xl: time at most this many batches")
     ap.add_argument("--length-scale", type=float, default=0.03,
                     help="uneven workload: record lengths scaled by this factor (a bounded sample)")
     ap.add_argument("--inflight", type=int, default=2,
@@ -389,11 +391,24 @@ def run_uneven(args, rank, world, local_rank):
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
     t_setup = time.perf_counter()
-    prob = uneven_config(length_scale=args.length_scale)
+    if args.workload == "xl":
+        # 8 shots of 6000-8000 steps and 2500 receivers; dt at 0.15 of the GLL-spacing
+        # CFL limit of the fastest P wave of the model distribution (Vs 600, nu 0.40);
+        # two shots per batch keep the checkpointed adjoint inside the HBM
+        vp_max = 600.0 * np.sqrt(2.0 * (1.0 - 0.40) / (1.0 - 2.0 * 0.40))
+        dt = 0.15 * (0.5 * 2.5) / vp_max
+        prob = uneven_config(nx=160, ny=160, nz=80, npml=6, nshot=8, dt=dt, lengths=(6000, 8000),
+                             receivers=(2500, 2500), length_scale=args.length_scale)
+        per_batch, ckpt = 2, 50
+    else:
+        prob = uneven_config(length_scale=args.length_scale)
+        per_batch, ckpt = 8, 100
     m = prob.mesh
     lengths = [sh.nstep for sh in prob.shots]
-    plan = B.plan(lengths, 8)
+    plan = B.plan(lengths, per_batch)
     mine = plan[rank::world]
+    if args.max_batches:
+        mine = mine[:args.max_batches]
     import threading
 
     def make_solver():
@@ -402,7 +417,7 @@ def run_uneven(args, rank, world, local_rank):
         sv.set_mesh(m, prob.rho_el)
         sv.assemble(prob.lam, prob.mu)
         sv.set_history(m.store_eq)
-        sv.set_checkpointing(100)
+        sv.set_checkpointing(ckpt)
         return sv
 
     def run_batch(sv, ids):
@@ -415,7 +430,8 @@ def run_uneven(args, rank, world, local_rank):
 
     # warm-up: the first context tunes the stage variants on this operator; the others
     # take its choice; each builds its tables on one batch
-    solvers = [make_solver() for _ in range(max(1, args.inflight))]
+    # the xl mesh holds one context in HBM
+    solvers = [make_solver() for _ in range(1 if args.workload == "xl" else max(1, args.inflight))]
     s = solvers[0]
     if args.variant:
         s.set_variant(args.variant, args.variant)
@@ -476,7 +492,7 @@ def run_uneven(args, rank, world, local_rank):
     t1 = s.last_timing()
     s.set_timing(False)
     stage_us = (t1[1] - t0[1]) / max(t1[2] - t0[2], 1) * 1e3
-    nnz = [int(s.operator_csr(w)[2].size) for w in range(3)]
+    nnz = [s.operator_nnz(w) for w in range(3)]
     bytes_launch = stage_bytes(sum(nnz), m.neq, len(mine[0]), 4)
     peak, peak_kind = measured_peaks()
     kname, _ = stage_kernel_name(s.variant()[0])
@@ -486,11 +502,12 @@ def run_uneven(args, rank, world, local_rank):
               "scaling": "weak", "vs_baseline": None, "dtype": "f32",
               "data": "synthetic (seeded layered model with ellipsoidal inclusions; zero measured data)",
               "config": {"workload": prob.name, "equations": m.neq, "dof": prob.dof, "nnz_CKG": nnz,
-                         "shots": len(prob.shots), "batches": len(plan), "shots_per_batch": 8,
+                         "shots": len(prob.shots), "batches": len(plan), "batches_timed": len(mine),
+                         "shots_per_batch": per_batch, "dt": prob.dt,
                          "record_lengths": [min(lengths), max(lengths)], "length_scale": args.length_scale,
                          "receivers_per_shot": [min(len(sh.eqdis) // 3 for sh in prob.shots),
                                                 max(len(sh.eqdis) // 3 for sh in prob.shots)],
-                         "checkpoint_interval": 100, "stage_variant_fwd_adj": list(s.variant()),
+                         "checkpoint_interval": ckpt, "stage_variant_fwd_adj": list(s.variant()),
                          "batches_in_flight": len(solvers),
                          "setup_s": setup_s,
                          "step": "one batch of 8 shots: forward + misfit + checkpointed adjoint with gradient",
@@ -623,7 +640,7 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     if args.impl == "reference":
         res = run_reference(args, rank, world)
-    elif args.workload == "uneven":
+    elif args.workload in ("uneven", "xl"):
         res = run_uneven(args, rank, world, local_rank)
     else:
         res = run_native(args, rank, world, local_rank)

@@ -120,6 +120,12 @@ class Solver:
         """Assemble from device-resident nodal lambda, mu (raw device pointers, FP64 [nj])."""
         self._check(self._L.hrn_assemble_device(self.h, C.c_void_p(lam_ptr), C.c_void_p(mu_ptr)))
 
+    def operator_nnz(self, which: int) -> int:
+        """Stored entries of C (0), K (1) or G (2)."""
+        nnz = C.c_int64()
+        self._check(self._L.hrn_get_operator_csr(self.h, which, None, None, None, C.byref(nnz)))
+        return nnz.value
+
     def operator_csr(self, which: int):
         nnz = C.c_int64()
         self._check(self._L.hrn_get_operator_csr(self.h, which, None, None, None, C.byref(nnz)))
