@@ -56,11 +56,10 @@ def parse_args():
                     help="stage-kernel variant for forward and adjoint (0 = chosen by timing on first use)")
     ap.add_argument("--no-graphs", action="store_true",
                     help="launch every kernel directly instead of replaying the captured time loops")
-    ap.add_argument("--workload", choices=["inversion", "uneven", "xl"], default="inversion",
+    ap.add_argument("--workload", choices=["inversion", "uneven"], default="inversion",
                     help="inversion: the 16x16x8 plain inversion loop (default); uneven: batched uneven "
-                         "shots on the 80x80x40 + PML 4 mesh, FP32 stepping, checkpointed adjoint; "
-                         "xl: one evaluation on the 160x160x80 + PML 6 mesh (86.6 M equations)")
-    ap.add_argument("--max-batches", type=int, default=0, help="uneven / xl: time at most this many batches")
+                         "shots on the 80x80x40 + PML 4 mesh, FP32 stepping, checkpointed adjoint")
+    ap.add_argument("--max-batches", type=int, default=0, help="uneven: time at most this many batches")
     ap.add_argument("--length-scale", type=float, default=0.03,
                     help="uneven workload: record lengths scaled by this factor (a bounded sample)")
     ap.add_argument("--inflight", type=int, default=2,
@@ -391,18 +390,8 @@ def run_uneven(args, rank, world, local_rank):
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
     t_setup = time.perf_counter()
-    if args.workload == "xl":
-        # 8 shots of 6000-8000 steps and 2500 receivers; dt at 0.15 of the GLL-spacing
-        # CFL limit of the fastest P wave of the model distribution (Vs 600, nu 0.40);
-        # two shots per batch keep the checkpointed adjoint inside the HBM
-        vp_max = 600.0 * np.sqrt(2.0 * (1.0 - 0.40) / (1.0 - 2.0 * 0.40))
-        dt = 0.15 * (0.5 * 2.5) / vp_max
-        prob = uneven_config(nx=160, ny=160, nz=80, npml=6, nshot=8, dt=dt, lengths=(6000, 8000),
-                             receivers=(2500, 2500), length_scale=args.length_scale)
-        per_batch, ckpt = 2, 50
-    else:
-        prob = uneven_config(length_scale=args.length_scale)
-        per_batch, ckpt = 8, 100
+    prob = uneven_config(length_scale=args.length_scale)
+    per_batch, ckpt = 8, 100
     m = prob.mesh
     lengths = [sh.nstep for sh in prob.shots]
     plan = B.plan(lengths, per_batch)
@@ -430,8 +419,7 @@ def run_uneven(args, rank, world, local_rank):
 
     # warm-up: the first context tunes the stage variants on this operator; the others
     # take its choice; each builds its tables on one batch
-    # the xl mesh holds one context in HBM
-    solvers = [make_solver() for _ in range(1 if args.workload == "xl" else max(1, args.inflight))]
+    solvers = [make_solver() for _ in range(max(1, args.inflight))]
     s = solvers[0]
     if args.variant:
         s.set_variant(args.variant, args.variant)
@@ -640,7 +628,7 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     if args.impl == "reference":
         res = run_reference(args, rank, world)
-    elif args.workload in ("uneven", "xl"):
+    elif args.workload == "uneven":
         res = run_uneven(args, rank, world, local_rank)
     else:
         res = run_native(args, rank, world, local_rank)

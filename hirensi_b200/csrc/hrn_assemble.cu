@@ -24,6 +24,7 @@
 #include <cuda_runtime.h>
 #include <thrust/device_ptr.h>
 #include <thrust/execution_policy.h>
+#include <thrust/merge.h>
 #include <thrust/sort.h>
 #include <thrust/unique.h>
 
@@ -122,7 +123,7 @@ __device__ __forceinline__ void put(const AsmArgs &A, int row, int col, int tag,
     const uint32_t key = (uint32_t(tag) << kTagBits) | uint32_t(col);
     int lo = A.rowptr[row], hi = A.rowptr[row + 1] - 1;
     while (lo <= hi) {
-        const int mid = (lo + hi) >> 1;
+        const int mid = lo + ((hi - lo) >> 1);   // no overflow past 2^30 entries
         const uint32_t m = A.colx[mid];
         if (m == key) { A.raw[mid] = add(A.raw[mid], v); return; }
         if (m < key) lo = mid + 1; else hi = mid - 1;
@@ -375,28 +376,37 @@ static int build_colors(hrn_ctx *c)
     return 0;
 }
 
-static int run_kernels(hrn_ctx *c, AsmArgs A)
+// The kernels of elements [off, off + n) of one (colour, kind) group.
+static int run_group(hrn_ctx *c, AsmArgs A, int g, int off, int n)
 {
     const int th = 256;
-    const int ngroups = int(c->color_off.size()) - 1;   // (colour, kind) groups
-    for (int g = 0; g < ngroups; ++g) {
-        const int n = c->color_off[g + 1] - c->color_off[g];
-        if (n == 0) continue;
-        A.elems = c->d_el_color_list.as<int32_t>() + c->color_off[g];
-        A.nel = n;
-        const bool pml = (g % 2) == 1;
-        k_asm_diag<<<(n * 27 + th - 1) / th, th, 0, c->stream>>>(A, pml ? 1 : 0); ++c->launches;
-        if (!pml) {
-            const int64_t tot = int64_t(n) * 513 * 9;
-            k_asm_rd_k<<<unsigned((tot + th - 1) / th), th, 0, c->stream>>>(A); ++c->launches;
-        } else {
-            const int64_t tot = int64_t(n) * 189 * 54;
-            k_asm_ea<<<unsigned((tot + th - 1) / th), th, 0, c->stream>>>(A); ++c->launches;
-        }
-        HRN_CUDA(c, cudaGetLastError());
+    if (n <= 0) return 0;
+    A.elems = c->d_el_color_list.as<int32_t>() + c->color_off[g] + off;
+    A.nel = n;
+    const bool pml = (g % 2) == 1;
+    k_asm_diag<<<(n * 27 + th - 1) / th, th, 0, c->stream>>>(A, pml ? 1 : 0); ++c->launches;
+    if (!pml) {
+        const int64_t tot = int64_t(n) * 513 * 9;
+        k_asm_rd_k<<<unsigned((tot + th - 1) / th), th, 0, c->stream>>>(A); ++c->launches;
+    } else {
+        const int64_t tot = int64_t(n) * 189 * 54;
+        k_asm_ea<<<unsigned((tot + th - 1) / th), th, 0, c->stream>>>(A); ++c->launches;
     }
+    HRN_CUDA(c, cudaGetLastError());
     return 0;
 }
+
+static int run_kernels(hrn_ctx *c, AsmArgs A)
+{
+    const int ngroups = int(c->color_off.size()) - 1;   // (colour, kind) groups
+    for (int g = 0; g < ngroups; ++g)
+        if (int rc = run_group(c, A, g, 0, c->color_off[g + 1] - c->color_off[g])) return rc;
+    return 0;
+}
+
+// Most candidate keys one element of a kind can emit (diagonal, stiffness, PML blocks).
+constexpr unsigned long long kKeysRd = 513ull * 9, kKeysPml = 27ull * 9 + 189ull * 15 * 2 * 3;
+constexpr unsigned long long kKeysPerSlice = 1ull << 29;   // 4 GiB of candidate keys per slice
 
 int assemble_device(hrn_ctx *c, bool discover_pattern)
 {
@@ -415,32 +425,51 @@ int assemble_device(hrn_ctx *c, bool discover_pattern)
     A.err = c->d_asm_err.as<int>();
     HRN_CUDA(c, cudaMemsetAsync(c->d_asm_err.p, 0, 16, c->stream));
     if (discover_pattern) {
-        int64_t nrd = 0, npml = 0;
-        for (int e = 0; e < c->nel; ++e) (c->h_mtel[e] == 1 ? nrd : npml)++;
-        const unsigned long long cap = (unsigned long long)(nrd * 513 * 9 + npml * (27 * 9 + 189 * 15 * 2 * 3));
-        DevBuf keys, count;
-        HRN_CUDA(c, keys.alloc(std::max<size_t>(size_t(cap), 1) * 8));
+        // Candidate keys slice by slice of each (colour, kind) group: each slice's keys
+        // are sorted and made unique, then merged into the sorted set of all keys so
+        // far, so device memory stays bounded by one slice plus the final pattern.
+        DevBuf keys, count, acc, tmp;
+        HRN_CUDA(c, keys.alloc(size_t(kKeysPerSlice) * 8));
         HRN_CUDA(c, count.alloc(8));
-        HRN_CUDA(c, cudaMemsetAsync(count.p, 0, 8, c->stream));
+        size_t na = 0;
         A.discover = 1;
         A.keys = keys.as<uint64_t>();
         A.count = count.as<unsigned long long>();
-        A.cap = cap;
-        if (int rc = run_kernels(c, A)) return rc;
-        unsigned long long n = 0;
-        int err = 0;
-        HRN_CUDA(c, cudaMemcpyAsync(&n, count.p, 8, cudaMemcpyDeviceToHost, c->stream));
-        HRN_CUDA(c, cudaMemcpyAsync(&err, c->d_asm_err.p, 4, cudaMemcpyDeviceToHost, c->stream));
-        HRN_CUDA(c, cudaStreamSynchronize(c->stream));
-        if (err == 4) return set_error(c, HRN_EMESH, "a PML point lies in the top PML zone");
-        if (err || n > cap) return set_error(c, HRN_ESTATE, "internal: pattern discovery overflow");
-        thrust::device_ptr<uint64_t> kp(keys.as<uint64_t>());
-        thrust::sort(thrust::cuda::par.on(c->stream), kp, kp + n);
-        const size_t nu = size_t(thrust::unique(thrust::cuda::par.on(c->stream), kp, kp + n) - kp);
-        std::vector<uint64_t> hk(nu);
-        HRN_CUDA(c, cudaMemcpyAsync(hk.data(), keys.p, nu * 8, cudaMemcpyDeviceToHost, c->stream));
-        HRN_CUDA(c, cudaStreamSynchronize(c->stream));
+        const int ngroups = int(c->color_off.size()) - 1;
+        for (int g = 0; g < ngroups; ++g) {
+            const int ng = c->color_off[g + 1] - c->color_off[g];
+            const unsigned long long per = (g % 2) == 1 ? kKeysPml : kKeysRd;
+            const int slice = int(std::max<unsigned long long>(1, kKeysPerSlice / per));
+            for (int off = 0; off < ng; off += slice) {
+                const int n = std::min(slice, ng - off);
+                A.cap = (unsigned long long)n * per;
+                HRN_CUDA(c, cudaMemsetAsync(count.p, 0, 8, c->stream));
+                if (int rc = run_group(c, A, g, off, n)) return rc;
+                unsigned long long nk = 0;
+                int err = 0;
+                HRN_CUDA(c, cudaMemcpyAsync(&nk, count.p, 8, cudaMemcpyDeviceToHost, c->stream));
+                HRN_CUDA(c, cudaMemcpyAsync(&err, c->d_asm_err.p, 4, cudaMemcpyDeviceToHost, c->stream));
+                HRN_CUDA(c, cudaStreamSynchronize(c->stream));
+                if (err == 4) return set_error(c, HRN_EMESH, "a PML point lies in the top PML zone");
+                if (err || nk > A.cap) return set_error(c, HRN_ESTATE, "internal: pattern discovery overflow");
+                thrust::device_ptr<uint64_t> kp(keys.as<uint64_t>());
+                thrust::sort(thrust::cuda::par.on(c->stream), kp, kp + nk);
+                const size_t nu = size_t(thrust::unique(thrust::cuda::par.on(c->stream), kp, kp + nk) - kp);
+                // merge with the keys found so far
+                HRN_CUDA(c, tmp.alloc(std::max<size_t>(na + nu, 1) * 8));
+                thrust::device_ptr<uint64_t> ap(acc.as<uint64_t>()), tp(tmp.as<uint64_t>());
+                const size_t nm = size_t(thrust::merge(thrust::cuda::par.on(c->stream), ap, ap + na, kp, kp + nu, tp) - tp);
+                na = size_t(thrust::unique(thrust::cuda::par.on(c->stream), tp, tp + nm) - tp);
+                std::swap(acc.p, tmp.p);
+                std::swap(acc.bytes, tmp.bytes);
+            }
+        }
         keys.release();
+        tmp.release();
+        std::vector<uint64_t> hk(na);
+        if (na) HRN_CUDA(c, cudaMemcpyAsync(hk.data(), acc.p, na * 8, cudaMemcpyDeviceToHost, c->stream));
+        HRN_CUDA(c, cudaStreamSynchronize(c->stream));
+        acc.release();
         if (int rc = finalize_pattern_from_keys(c, hk)) return rc;
     }
     // values
