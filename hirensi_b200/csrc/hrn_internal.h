@@ -134,6 +134,8 @@ struct hrn_ctx {
     hrn::DevBuf d_rd_geom;        // [nel_rd][27][10] DJI (9) and w*detJ per GLL point (FP64)
     hrn::DevBuf d_rd_store;       // [nel_rd][27] history node index (store index / 3)
     bool have_rd_store = false;
+    hrn::DevBuf d_gslot;          // [2][nel_rd][27] gradient of each element point, summed over steps (FP64)
+    hrn::DevBuf d_gnode_ptr, d_gnode_slot;   // [nj + 1], [nel_rd * 27]: the slots of every node, ascending
     // device assembly
     hrn::DevBuf d_asm_geom;       // [nel][27][10] for all elements
     hrn::DevBuf d_el_color_list;  // elements sorted by colour

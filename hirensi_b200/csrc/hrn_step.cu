@@ -328,7 +328,7 @@ __global__ void __launch_bounds__(128) k_gradient(int nel_rd, const int32_t *__r
                                                   const double *__restrict__ geom, const T *__restrict__ hist_n,
                                                   const T *__restrict__ x2, const int32_t *__restrict__ store_eq,
                                                   double *__restrict__ g_lam, double *__restrict__ g_mu, double dt,
-                                                  int lambda_2mu)
+                                                  int lambda_2mu)   // g_lam, g_mu: [nel_rd][27] point slots
 {
     __shared__ T su[kGradElems][27][3][S];
     __shared__ T sp[kGradElems][27][3][S];
@@ -400,9 +400,27 @@ __global__ void __launch_bounds__(128) k_gradient(int nel_rd, const int32_t *__r
         tl += (sl * fac0) * dt;
         tm += (sm * fac0) * dt;
     }
-    const int node = inod[size_t(rd_elems[e]) * 27 + c_node_at[q]];
-    atomicAdd(g_lam + node, tl);
-    atomicAdd(g_mu + node, tm);
+    // one thread owns each (element, point) slot: the sum over steps needs no atomics
+    g_lam[size_t(e) * 27 + q] += tl;
+    g_mu[size_t(e) * 27 + q] += tm;
+}
+
+// Node sums of the gradient slots in a fixed order (ascending element, then point),
+// so the gradient is the same bit for bit from run to run.  Nodes without a slot
+// (PML-only nodes) get 0.
+__global__ void k_gradient_nodes(int nj, const int32_t *__restrict__ ptr, const int32_t *__restrict__ slots,
+                                 const double *__restrict__ slot_l, const double *__restrict__ slot_m,
+                                 double *__restrict__ g_lam, double *__restrict__ g_mu)
+{
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= nj) return;
+    double sl = 0.0, sm = 0.0;
+    for (int k = ptr[j]; k < ptr[j + 1]; ++k) {
+        sl += slot_l[slots[k]];
+        sm += slot_m[slots[k]];
+    }
+    g_lam[j] = sl;
+    g_mu[j] = sm;
 }
 
 // ----------------------------------------------------------------------------
@@ -611,6 +629,17 @@ __global__ void k_geometry(int nel, const int32_t *__restrict__ elems, const int
 #undef S_
 }
 
+static const int kLocalIjk[27][3] = {{2, 0, 0}, {2, 2, 0}, {0, 2, 0}, {0, 0, 0}, {2, 0, 2}, {2, 2, 2}, {0, 2, 2}, {0, 0, 2},
+                                     {2, 1, 0}, {1, 2, 0}, {0, 1, 0}, {1, 0, 0}, {2, 0, 1}, {2, 2, 1}, {0, 2, 1}, {0, 0, 1},
+                                     {2, 1, 2}, {1, 2, 2}, {0, 1, 2}, {1, 0, 2}, {1, 1, 0}, {2, 1, 1}, {1, 2, 1}, {0, 1, 1},
+                                     {1, 0, 1}, {1, 1, 2}, {1, 1, 1}};
+
+// local node at GLL point q = 9c + 3b + a
+static void gll_node_at(int (&node_at)[27])
+{
+    for (int i = 0; i < 27; ++i) node_at[9 * kLocalIjk[i][2] + 3 * kLocalIjk[i][1] + kLocalIjk[i][0]] = i;
+}
+
 static int upload_tables(hrn_ctx *c)
 {
     static const int ijk[27][3] = {{2, 0, 0}, {2, 2, 0}, {0, 2, 0}, {0, 0, 0}, {2, 0, 2}, {2, 2, 2}, {0, 2, 2}, {0, 0, 2},
@@ -700,7 +729,48 @@ static int build_rd_store(hrn_ctx *c)
     }
     HRN_CUDA(c, c->d_rd_store.alloc(rs.size() * 4));
     if (!rs.empty()) HRN_CUDA(c, cudaMemcpy(c->d_rd_store.p, rs.data(), rs.size() * 4, cudaMemcpyHostToDevice));
+    // gradient slots of every node, in ascending (element, point) order
+    int node_at[27];
+    gll_node_at(node_at);
+    std::vector<int32_t> ptr(size_t(c->nj) + 1, 0), slots(size_t(c->nel_rd) * 27);
+    std::vector<int32_t> slot_node(slots.size());
+    k = 0;
+    for (int e = 0; e < c->nel; ++e) {
+        if (c->h_mtel[e] != 1) continue;
+        for (int q = 0; q < 27; ++q) {
+            const int node = c->h_inod[size_t(e) * 27 + node_at[q]];
+            slot_node[size_t(k) * 27 + q] = node;
+            ptr[size_t(node) + 1]++;
+        }
+        ++k;
+    }
+    for (int j = 0; j < c->nj; ++j) ptr[j + 1] += ptr[j];
+    std::vector<int32_t> fill(ptr.begin(), ptr.end() - 1);
+    for (size_t sidx = 0; sidx < slot_node.size(); ++sidx) slots[fill[slot_node[sidx]]++] = int32_t(sidx);
+    HRN_CUDA(c, c->d_gnode_ptr.alloc(ptr.size() * 4));
+    HRN_CUDA(c, c->d_gnode_slot.alloc(std::max<size_t>(slots.size(), 1) * 4));
+    HRN_CUDA(c, c->d_gslot.alloc(std::max<size_t>(slots.size(), 1) * 2 * 8));
+    HRN_CUDA(c, cudaMemcpy(c->d_gnode_ptr.p, ptr.data(), ptr.size() * 4, cudaMemcpyHostToDevice));
+    if (!slots.empty()) HRN_CUDA(c, cudaMemcpy(c->d_gnode_slot.p, slots.data(), slots.size() * 4, cudaMemcpyHostToDevice));
     c->have_rd_store = true;
+    return 0;
+}
+
+// Zero the gradient slots (on the stream) / sum them into node vectors g_l, g_m [nj].
+static int gradient_slots_clear(hrn_ctx *c)
+{
+    HRN_CUDA(c, cudaMemsetAsync(c->d_gslot.p, 0, c->d_gslot.bytes, c->stream));
+    return 0;
+}
+
+static int gradient_slots_to_nodes(hrn_ctx *c, double *g_l, double *g_m)
+{
+    const size_t ns = size_t(c->nel_rd) * 27;
+    k_gradient_nodes<<<(c->nj + 255) / 256, 256, 0, c->stream>>>(c->nj, c->d_gnode_ptr.as<int32_t>(),
+                                                                 c->d_gnode_slot.as<int32_t>(), c->d_gslot.as<double>(),
+                                                                 c->d_gslot.as<double>() + ns, g_l, g_m);
+    ++c->launches;
+    HRN_CUDA(c, cudaGetLastError());
     return 0;
 }
 
@@ -1022,6 +1092,7 @@ static int adjoint_t(hrn_ctx *c, int lambda_2mu, int keep_p)
     cudaEventRecord(t0, c->stream);
     StageTimer tm(c);
     double *gl = c->d_g.as<double>(), *gmu = gl + c->nj;
+    double *gsl = c->d_gslot.as<double>(), *gsm = gsl + size_t(c->nel_rd) * 27;   // point slots
     const int gblocks = (c->nel_rd + kGradElems - 1) / kGradElems;
     const RecView rv = rec_view(c);
     const int K = c->ckpt;
@@ -1031,7 +1102,7 @@ static int adjoint_t(hrn_ctx *c, int lambda_2mu, int keep_p)
     // forward segments and the gradient
     auto body = [&]() -> int {
         HRN_CUDA(c, cudaMemsetAsync(X0, 0, 3 * vn * sizeof(T), c->stream));
-        HRN_CUDA(c, cudaMemsetAsync(c->d_g.p, 0, size_t(2) * c->nj * 8, c->stream));
+        if (int rc = gradient_slots_clear(c)) return rc;
         if (keep_p) HRN_CUDA(c, cudaMemsetAsync(c->d_phist.p, 0, c->d_phist.bytes, c->stream));
         int it = 0;
         for (int n = c->nstep; n >= 1; --n, ++it) {
@@ -1063,8 +1134,9 @@ static int adjoint_t(hrn_ctx *c, int lambda_2mu, int keep_p)
                 k_gradient<T, S><<<gblocks, 128, 0, c->stream>>>(c->nel_rd, c->d_rd_store.as<int32_t>(), c->d_rd_elems.as<int32_t>(),
                                                                  c->d_inod.as<int32_t>(), c->d_rd_geom.as<double>(),
                                                                  u_n, X + vn,
-                                                                 c->d_store_eq.as<int32_t>(), gl, gmu, c->dt, lambda_2mu); ++c->launches;
+                                                                 c->d_store_eq.as<int32_t>(), gsl, gsm, c->dt, lambda_2mu); ++c->launches;
         }
+        if (int rc = gradient_slots_to_nodes(c, gl, gmu)) return rc;
         HRN_CUDA(c, cudaGetLastError());
         return 0;
     };
@@ -1125,8 +1197,8 @@ static int pseudo_hessian_t(hrn_ctx *c, double *hl, double *hm)
         HRN_CUDA(c, c->d_store_iota.alloc(iota.size() * 4));
         HRN_CUDA(c, cudaMemcpy(c->d_store_iota.p, iota.data(), iota.size() * 4, cudaMemcpyHostToDevice));
     }
-    HRN_CUDA(c, cudaMemsetAsync(hl, 0, size_t(c->nj) * 8, c->stream));
-    HRN_CUDA(c, cudaMemsetAsync(hm, 0, size_t(c->nj) * 8, c->stream));
+    if (int rc = gradient_slots_clear(c)) return rc;
+    double *gsl = c->d_gslot.as<double>(), *gsm = gsl + size_t(c->nel_rd) * 27;
     const int gblocks = (c->nel_rd + kGradElems - 1) / kGradElems;
     if (c->nel_rd > 0)
         for (int n = 1; n <= c->nstep - 1; ++n) {
@@ -1134,9 +1206,10 @@ static int pseudo_hessian_t(hrn_ctx *c, double *hl, double *hm)
             // p := u: the history row read again through the identity position map
             k_gradient<T, S><<<gblocks, 128, 0, c->stream>>>(c->nel_rd, c->d_rd_store.as<int32_t>(), c->d_rd_elems.as<int32_t>(),
                                                              c->d_inod.as<int32_t>(), c->d_rd_geom.as<double>(), u_n, u_n,
-                                                             c->d_store_iota.as<int32_t>(), hl, hm, c->dt, 0);
+                                                             c->d_store_iota.as<int32_t>(), gsl, gsm, c->dt, 0);
             ++c->launches;
         }
+    if (int rc = gradient_slots_to_nodes(c, hl, hm)) return rc;
     HRN_CUDA(c, cudaGetLastError());
     return 0;
 }

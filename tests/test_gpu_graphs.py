@@ -1,6 +1,7 @@
 """CUDA graphs of the time loops (hrn_set_graphs): a replayed call gives what the
-same call gives launched directly, bit for bit for the histories, traces and
-misfit, and to rounding for the gradient (its atomic sums run in varying order)."""
+same call gives launched directly, bit for bit (histories, traces, misfit and
+gradient), except with the atomic matrix-free variants, whose sums run in varying
+order."""
 import numpy as np
 import pytest
 
@@ -57,11 +58,13 @@ def test_replayed_calls_equal_direct_launches(gpu_lib, variant, ckpt):
         if atomic:
             assert abs(out[0] - ref[0]) <= 1e-12 * ref[0]
             assert rel_l2(out[3], ref[3]) < 1e-12
+            assert rel_l2(out[1], ref[1]) < 1e-12
+            assert rel_l2(out[2], ref[2]) < 1e-12
         else:
             assert out[0] == ref[0]
             assert np.array_equal(out[3], ref[3])
-        assert rel_l2(out[1], ref[1]) < 1e-12
-        assert rel_l2(out[2], ref[2]) < 1e-12
+            assert np.array_equal(out[1], ref[1])
+            assert np.array_equal(out[2], ref[2])
 
 
 def test_replay_follows_reassembly_and_new_data(gpu_lib):
@@ -85,7 +88,7 @@ def test_replay_follows_reassembly_and_new_data(gpu_lib):
         ref = _evaluate(s0, 0.5 * dis)
     assert got[0] == ref[0]
     assert np.array_equal(got[3], ref[3])
-    assert rel_l2(got[1], ref[1]) < 1e-13
+    assert np.array_equal(got[1], ref[1])
 
 
 def test_new_settings_capture_again(gpu_lib):
