@@ -362,6 +362,12 @@ int hrn_destroy(hrn_ctx *c)
     cudaSetDevice(c->device);
     cudaStreamSynchronize(c->stream);
     for (cudaEvent_t e : c->ev_pool) cudaEventDestroy(e);
+    if (c->side_stream) {
+        cudaStreamSynchronize(c->side_stream);
+        cudaStreamDestroy(c->side_stream);
+        cudaEventDestroy(c->ev_fork);
+        cudaEventDestroy(c->ev_join);
+    }
     if (c->own_stream) cudaStreamDestroy(c->own_stream);
     delete c;
     return HRN_OK;

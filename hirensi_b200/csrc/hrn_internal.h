@@ -100,6 +100,8 @@ struct hrn_ctx {
     std::string err;
     cudaStream_t own_stream = nullptr;
     cudaStream_t stream = nullptr;
+    cudaStream_t side_stream = nullptr;       // the adjoint's gradient launches, beside the stages
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
 
     // ---- operator: one CSR per row holding the C, K and G entries in that order;
     // the top 2 bits of each column index name the matrix (0 = C, 1 = K, 2 = G).

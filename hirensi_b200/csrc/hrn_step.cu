@@ -1054,6 +1054,11 @@ template <typename T, int S>
 static int adjoint_t(hrn_ctx *c, int lambda_2mu, int keep_p)
 {
     if (int rc = build_rd_store(c)) return rc;
+    if (!c->side_stream) {
+        HRN_CUDA(c, cudaStreamCreateWithFlags(&c->side_stream, cudaStreamNonBlocking));
+        HRN_CUDA(c, cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming));
+        HRN_CUDA(c, cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming));
+    }
     const size_t vn = size_t(c->neq) * S;
     T *X0 = c->d_X.as<T>(), *X1 = X0 + 3 * vn;
     if (keep_p) HRN_CUDA(c, c->d_phist.alloc(size_t(c->nstep + 1) * c->nstore * S * sizeof(T)));
@@ -1105,7 +1110,11 @@ static int adjoint_t(hrn_ctx *c, int lambda_2mu, int keep_p)
         if (int rc = gradient_slots_clear(c)) return rc;
         if (keep_p) HRN_CUDA(c, cudaMemsetAsync(c->d_phist.p, 0, c->d_phist.bytes, c->stream));
         int it = 0;
+        bool forked = false;   // a gradient launch is pending on the side stream
         for (int n = c->nstep; n >= 1; --n, ++it) {
+            // the previous step's gradient read the state this step overwrites and the
+            // history segment a recompute overwrites: it must be done first
+            if (forked) HRN_CUDA(c, cudaStreamWaitEvent(c->stream, c->ev_join, 0));
             const int k0 = K > 0 ? (n / K) * K : 0;   // first step of n's checkpoint segment
             if (K > 0 && (n == c->nstep || n % K == K - 1)) {
                 // recompute the forward history of steps k0 .. min(k0 + K - 1, nstep - 1) from the checkpoint
@@ -1129,13 +1138,21 @@ static int adjoint_t(hrn_ctx *c, int lambda_2mu, int keep_p)
                     c->d_im.as<double>(), c->d_srcv_a.as<T>(), shot_nstep_ptr(c), rec_mask_ptr(c)); ++c->launches;
             a.hist = keep_p ? c->d_phist.as<T>() + size_t(n) * c->nstore * S : nullptr;
             T *X = (it & 1) ? X1 : X0, *Y = (it & 1) ? X0 : X1;
+            if (n <= c->nstep - 1 && c->nel_rd > 0) {
+                // the zero-lag correlation of this step's state runs on the side stream,
+                // next to the step's stages (they read X and write Y, KB, MB)
+                HRN_CUDA(c, cudaEventRecord(c->ev_fork, c->stream));
+                HRN_CUDA(c, cudaStreamWaitEvent(c->side_stream, c->ev_fork, 0));
+                k_gradient<T, S><<<gblocks, 128, 0, c->side_stream>>>(c->nel_rd, c->d_rd_store.as<int32_t>(), c->d_rd_elems.as<int32_t>(),
+                                                                      c->d_inod.as<int32_t>(), c->d_rd_geom.as<double>(),
+                                                                      u_n, X + vn,
+                                                                      c->d_store_eq.as<int32_t>(), gsl, gsm, c->dt, lambda_2mu); ++c->launches;
+                HRN_CUDA(c, cudaEventRecord(c->ev_join, c->side_stream));
+                forked = true;
+            }
             launch_step<T, S>(c, a, X, Y, c->timing ? &tm : nullptr, c->lanes_a, ta, 1);
-            if (n <= c->nstep - 1 && c->nel_rd > 0)
-                k_gradient<T, S><<<gblocks, 128, 0, c->stream>>>(c->nel_rd, c->d_rd_store.as<int32_t>(), c->d_rd_elems.as<int32_t>(),
-                                                                 c->d_inod.as<int32_t>(), c->d_rd_geom.as<double>(),
-                                                                 u_n, X + vn,
-                                                                 c->d_store_eq.as<int32_t>(), gsl, gsm, c->dt, lambda_2mu); ++c->launches;
         }
+        if (forked) HRN_CUDA(c, cudaStreamWaitEvent(c->stream, c->ev_join, 0));
         if (int rc = gradient_slots_to_nodes(c, gl, gmu)) return rc;
         HRN_CUDA(c, cudaGetLastError());
         return 0;
