@@ -537,6 +537,10 @@ def fwi_leg(precision, prob, dis, local_rank, iters, learned=False, target=None,
     if learned:
         from hirensi_b200.learned import DeviceNet, LearnedPreconditioner, Lattice, Net
         pre = LearnedPreconditioner(DeviceNet(Net.load(PRECOND_WEIGHTS), Lattice.of(m).shape), m, RHO)
+    # warm-up outside the timed region, as a driver that keeps its solver between
+    # inversions has it: one iteration builds the variant's tables, the inversion's
+    # buffers and the captured time loops, and loads the network's kernels
+    FWI(backend, cfg, preconditioner=pre).run(prob.lam0, prob.mu0, n_iter=1)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     hist = FWI(backend, cfg, preconditioner=pre).run(prob.lam0, prob.mu0, n_iter=iters, target_reduction=target)
@@ -548,7 +552,8 @@ def fwi_leg(precision, prob, dis, local_rank, iters, learned=False, target=None,
     out = {"iterations": len(hist) - 1, "wall_s": wall, "misfit_initial": J0, "misfit_final": J,
            "misfit_reduction": 1.0 - J / J0, "time_to_50pct_reduction_s": t_half,
            "forward_solves": sum(1 + h["armijo"] + (1 if h.get("learned") is False else 0) for h in hist[1:]) + 1,
-           "config": "L-BFGS memory 5, TV regularization, reference step rules, bounds lambda [10,2000] mu [10,1000]"}
+           "config": "L-BFGS memory 5, TV regularization, reference step rules, bounds lambda [10,2000] mu [10,1000]",
+           "warmup": "one inversion iteration (tables, buffers, captured time loops) before the timed inversion"}
     if learned:
         out["learned_steps_accepted"] = int(sum(1 for h in hist[1:] if h.get("learned")))
         out["weights"] = os.path.relpath(PRECOND_WEIGHTS, ROOT)

@@ -752,6 +752,12 @@ static int build_rd_store(hrn_ctx *c)
     HRN_CUDA(c, c->d_gslot.alloc(std::max<size_t>(slots.size(), 1) * 2 * 8));
     HRN_CUDA(c, cudaMemcpy(c->d_gnode_ptr.p, ptr.data(), ptr.size() * 4, cudaMemcpyHostToDevice));
     if (!slots.empty()) HRN_CUDA(c, cudaMemcpy(c->d_gnode_slot.p, slots.data(), slots.size() * 4, cudaMemcpyHostToDevice));
+    // identity map of the history rows (the pseudo-Hessian reads u through it), allocated
+    // here with the other gradient tables so that later calls allocate nothing
+    std::vector<int32_t> iota(static_cast<size_t>(std::max(c->nstore, 1)));
+    for (int i = 0; i < c->nstore; ++i) iota[i] = i;
+    HRN_CUDA(c, c->d_store_iota.alloc(iota.size() * 4));
+    HRN_CUDA(c, cudaMemcpy(c->d_store_iota.p, iota.data(), iota.size() * 4, cudaMemcpyHostToDevice));
     c->have_rd_store = true;
     return 0;
 }
@@ -1207,13 +1213,7 @@ static int misfit_t(hrn_ctx *c, double *cost)
 template <typename T, int S>
 static int pseudo_hessian_t(hrn_ctx *c, double *hl, double *hm)
 {
-    if (int rc = build_rd_store(c)) return rc;
-    if (c->d_store_iota.bytes != size_t(c->nstore) * 4) {
-        std::vector<int32_t> iota(static_cast<size_t>(c->nstore));
-        for (int i = 0; i < c->nstore; ++i) iota[i] = i;
-        HRN_CUDA(c, c->d_store_iota.alloc(iota.size() * 4));
-        HRN_CUDA(c, cudaMemcpy(c->d_store_iota.p, iota.data(), iota.size() * 4, cudaMemcpyHostToDevice));
-    }
+    if (int rc = build_rd_store(c)) return rc;   // also the identity map of the history rows
     if (int rc = gradient_slots_clear(c)) return rc;
     double *gsl = c->d_gslot.as<double>(), *gsm = gsl + size_t(c->nel_rd) * 27;
     const int gblocks = (c->nel_rd + kGradElems - 1) / kGradElems;
