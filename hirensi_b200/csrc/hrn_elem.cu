@@ -682,12 +682,9 @@ static int elem_buffers(hrn_ctx *c)
 template <typename T, int S, int SV, int ADJ, int ACC>
 static void launch_elem(const ElemArgs<T> &A, const StageArgs<T> &a, int stage, int mat, int blocks, cudaStream_t st)
 {
-    static bool attr_set = false;
+    static std::atomic<uint64_t> smem_done{0};
     constexpr size_t smem = elem_smem_bytes<T, S, SV>();
-    if (!attr_set) {
-        cudaFuncSetAttribute(k_elem<T, S, SV, ADJ, ACC>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-        attr_set = true;
-    }
+    smem_limit_once(k_elem<T, S, SV, ADJ, ACC>, int(smem), smem_done);
     k_elem<T, S, SV, ADJ, ACC><<<blocks, elems_per_block<S, SV>() * 27 * (S / SV), smem, st>>>(A, a, stage, mat);
 }
 

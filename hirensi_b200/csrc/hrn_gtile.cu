@@ -522,11 +522,8 @@ int gt_ready(hrn_ctx *c, int adj)
 template <typename T, int S, int STAGE, int G, int MAT>
 static void launch_gt(const StageArgs<T> &a, const GtArgs<T> &g, int ntiles, size_t smem, cudaStream_t st)
 {
-    static bool attr_set = false;
-    if (!attr_set) {
-        cudaFuncSetAttribute(rk4_stage_gt<T, S, STAGE, G, MAT>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kGtBudget));
-        attr_set = true;
-    }
+    static std::atomic<uint64_t> smem_done{0};
+    smem_limit_once(rk4_stage_gt<T, S, STAGE, G, MAT>, int(kGtBudget), smem_done);
     rk4_stage_gt<T, S, STAGE, G, MAT><<<ntiles, kGtThreads, smem, st>>>(a, g);
 }
 

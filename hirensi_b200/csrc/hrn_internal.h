@@ -21,6 +21,20 @@ inline std::atomic<uint64_t> &alloc_generation()
     return g;
 }
 
+// Raise a kernel's dynamic shared-memory limit once per device: the attribute
+// belongs to the device that is current, and contexts on several devices or
+// threads may launch the same kernel.  `done` holds one bit per device.
+template <typename K>
+inline void smem_limit_once(K kernel, int bytes, std::atomic<uint64_t> &done)
+{
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const uint64_t bit = dev >= 0 && dev < 64 ? (uint64_t(1) << dev) : 0;
+    if (bit && (done.load() & bit)) return;
+    cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    done.fetch_or(bit);
+}
+
 // Owning device buffer (cudaMalloc / cudaFree).
 struct DevBuf {
     void *p = nullptr;

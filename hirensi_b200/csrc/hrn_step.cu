@@ -517,12 +517,9 @@ inline bool is_elem_variant(int v) { return (v >= 90 && v <= 95) || (v >= 100 &&
 template <typename T, int S, int STAGE, int G, int MAT>
 static void launch_tile(const StageArgs<T> &a, const TileArgs &ta, cudaStream_t st)
 {
-    static bool attr_set = false;
+    static std::atomic<uint64_t> smem_done{0};
     constexpr size_t smem = tile_smem_bytes<T>();
-    if (!attr_set) {
-        cudaFuncSetAttribute(rk4_stage_tile<T, S, STAGE, G, MAT>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-        attr_set = true;
-    }
+    smem_limit_once(rk4_stage_tile<T, S, STAGE, G, MAT>, int(smem), smem_done);
     rk4_stage_tile<T, S, STAGE, G, MAT><<<ta.grid, kTileThreads, smem, st>>>(a, ta.tiles, ta.ntiles, ta.err);
 }
 
