@@ -543,7 +543,14 @@ template <typename T, int S>
 static int gt_stage_t(hrn_ctx *c, const StageArgs<T> &a, int stage, int adj, int variant)
 {
     const GtSet &gs = c->gt[adj];
-    if (!gs.built || gs.ntiles == 0) return 0;
+    if (!gs.built) {
+        // the tables are built before every time loop; reaching here without them is an
+        // internal error, flagged so that the call fails instead of skipping the stage
+        static const int two = 2;
+        cudaMemcpyAsync(c->d_step_err.p, &two, sizeof(int), cudaMemcpyHostToDevice, c->stream);
+        return set_error(c, HRN_ESTATE, "staged-gather tables not built");
+    }
+    if (gs.ntiles == 0) return 0;   // no rows
     const GtArgs<T> g{gs.d_tinfo.as<int4>(), gs.d_row.as<int32_t>(), gs.d_ent.as<int32_t>(), gs.d_ukey.as<uint32_t>(),
                       gs.d_lidx.as<uint16_t>(), gs.d_val.as<T>(), c->d_step_err.as<int>()};
     switch (stage) {

@@ -866,7 +866,8 @@ static int check_step_error(hrn_ctx *c)
     HRN_CUDA(c, cudaMemcpy(&err, c->d_step_err.p, 4, cudaMemcpyDeviceToHost));
     if (err) {
         cudaMemset(c->d_step_err.p, 0, 4);
-        return set_error(c, HRN_ECUDA, "a bounded wait of the tiled stage kernel timed out");
+        if (err == 2) return set_error(c, HRN_ESTATE, "a stage ran without the tables of its kernel variant");
+        return set_error(c, HRN_ECUDA, "a bounded wait of a stage kernel (bulk copies into shared memory) timed out");
     }
     return 0;
 }
