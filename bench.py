@@ -56,10 +56,12 @@ def parse_args():
                     help="stage-kernel variant for forward and adjoint (0 = chosen by timing on first use)")
     ap.add_argument("--no-graphs", action="store_true",
                     help="launch every kernel directly instead of replaying the captured time loops")
-    ap.add_argument("--workload", choices=["inversion", "uneven"], default="inversion",
+    ap.add_argument("--workload", choices=["inversion", "uneven", "xl"], default="inversion",
                     help="inversion: the 16x16x8 plain inversion loop (default); uneven: batched uneven "
-                         "shots on the 80x80x40 + PML 4 mesh, FP32 stepping, checkpointed adjoint")
-    ap.add_argument("--max-batches", type=int, default=0, help="uneven: time at most this many batches")
+                         "shots on the 80x80x40 + PML 4 mesh, FP32 stepping, checkpointed adjoint; "
+                         "xl: the same on the 160x160x80 + PML 6 mesh (86.6 M equations) with the "
+                         "matrix-free operator")
+    ap.add_argument("--max-batches", type=int, default=0, help="uneven / xl: time at most this many batches")
     ap.add_argument("--length-scale", type=float, default=0.03,
                     help="uneven workload: record lengths scaled by this factor (a bounded sample)")
     ap.add_argument("--inflight", type=int, default=2,
@@ -379,7 +381,10 @@ def run_uneven(args, rank, world, local_rank):
     the state checkpointed every 100 steps, misfit, adjoint with recomputed segments and
     the fused gradient, FP32 stepping with FP64 reductions.  Batches are sharded over
     ranks, and --inflight batches run at once on separate contexts (streams) of a GPU.
-    The unit counts each shot's own steps: DOF x (2 nstep_s + 1) per shot."""
+    The unit counts each shot's own steps: DOF x (2 nstep_s + 1) per shot.
+
+    xl: 8 shots on the 160x160x80 + PML 6 mesh (86.6 M equations), two per batch,
+    checkpoints every 50 steps, one context, matrix-free operator."""
     import torch
     from hirensi_b200 import batching as B
     from hirensi_b200 import build
@@ -390,8 +395,20 @@ def run_uneven(args, rank, world, local_rank):
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
     t_setup = time.perf_counter()
-    prob = uneven_config(length_scale=args.length_scale)
-    per_batch, ckpt = 8, 100
+    if args.workload == "xl":
+        # 8 shots of 6000-8000 steps and 2500 receivers; dt at 0.15 of the GLL-spacing
+        # CFL limit of the fastest P wave of the model distribution (Vs 600, nu 0.40).
+        # The CSR of this mesh would exceed the 2^31 entry range: C, K, G are applied
+        # element by element, and two shots per batch keep the checkpointed adjoint's
+        # segment history inside the HBM.
+        vp_max = 600.0 * np.sqrt(2.0 * (1.0 - 0.40) / (1.0 - 2.0 * 0.40))
+        dt = 0.15 * (0.5 * 2.5) / vp_max
+        prob = uneven_config(nx=160, ny=160, nz=80, npml=6, nshot=8, dt=dt, lengths=(6000, 8000),
+                             receivers=(2500, 2500), length_scale=args.length_scale)
+        per_batch, ckpt = 2, 50
+    else:
+        prob = uneven_config(length_scale=args.length_scale)
+        per_batch, ckpt = 8, 100
     m = prob.mesh
     lengths = [sh.nstep for sh in prob.shots]
     plan = B.plan(lengths, per_batch)
@@ -404,6 +421,8 @@ def run_uneven(args, rank, world, local_rank):
         sv = Solver("fp32", device=local_rank)
         sv.set_graphs(not args.no_graphs)
         sv.set_mesh(m, prob.rho_el)
+        if args.workload == "xl":
+            sv.set_operator_mode(True)
         sv.assemble(prob.lam, prob.mu)
         sv.set_history(m.store_eq)
         sv.set_checkpointing(ckpt)
@@ -419,7 +438,7 @@ def run_uneven(args, rank, world, local_rank):
 
     # warm-up: the first context tunes the stage variants on this operator; the others
     # take its choice; each builds its tables on one batch
-    solvers = [make_solver() for _ in range(max(1, args.inflight))]
+    solvers = [make_solver() for _ in range(1 if args.workload == "xl" else max(1, args.inflight))]
     s = solvers[0]
     if args.variant:
         s.set_variant(args.variant, args.variant)
@@ -481,6 +500,8 @@ def run_uneven(args, rank, world, local_rank):
     s.set_timing(False)
     stage_us = (t1[1] - t0[1]) / max(t1[2] - t0[2], 1) * 1e3
     nnz = [s.operator_nnz(w) for w in range(3)]
+    # matrix-free: no stored entries, so the vector part of the stage (the least any
+    # stage moves) is the algorithmic figure
     bytes_launch = stage_bytes(sum(nnz), m.neq, len(mine[0]), 4)
     peak, peak_kind = measured_peaks()
     kname, _ = stage_kernel_name(s.variant()[0])
@@ -498,10 +519,11 @@ def run_uneven(args, rank, world, local_rank):
                          "checkpoint_interval": ckpt, "stage_variant_fwd_adj": list(s.variant()),
                          "batches_in_flight": len(solvers),
                          "setup_s": setup_s,
-                         "step": "one batch of 8 shots: forward + misfit + checkpointed adjoint with gradient",
+                         "operator": "matrix-free" if args.workload == "xl" else "csr",
+                         "step": f"one batch of {per_batch} shots: forward + misfit + checkpointed adjoint with gradient",
                          "l2": "inputs larger than L2"},
               "gpu_launches": int(launches),
-              "roofline": {"bound": "hbm", "kernel": kname.replace("double", "float").replace(",4>", ",8>"),
+              "roofline": {"bound": "hbm", "kernel": kname.replace("double", "float").replace(",4>", f",{per_batch}>"),
                            "achieved": achieved, "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
                            "frac": achieved / peak, "bytes_per_launch": bytes_launch, "avg_launch_us": stage_us,
                            "traffic": None},
@@ -633,7 +655,7 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     if args.impl == "reference":
         res = run_reference(args, rank, world)
-    elif args.workload == "uneven":
+    elif args.workload in ("uneven", "xl"):
         res = run_uneven(args, rank, world, local_rank)
     else:
         res = run_native(args, rank, world, local_rank)

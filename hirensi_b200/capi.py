@@ -57,6 +57,7 @@ SIGNATURES = {
     "hrn_set_variant": (C.c_int, [VP, C.c_int32, C.c_int32]),
     "hrn_set_shot_records": (C.c_int, [VP, VP, VP]),
     "hrn_set_graphs": (C.c_int, [VP, C.c_int32]),
+    "hrn_set_operator_mode": (C.c_int, [VP, C.c_int32]),
     "hrn_get_state": (C.c_int, [VP, C.c_int32, C.c_int32, VP, VP, VP]),
     "hrn_graph_stats": (C.c_int, [VP, VP, VP]),
     "hrn_get_variant": (C.c_int, [VP, PI, PI]),

@@ -52,6 +52,7 @@ struct AsmArgs {
     double *raw, *diag_m;
     // discover mode
     int discover;
+    int no_csr;                 // matrix-free operator: DIAG_M only, no CSR entries
     unsigned long long *count;
     unsigned long long cap;
     uint64_t *keys;
@@ -113,7 +114,7 @@ __device__ bool pml_ab(const double *x, const double *P, double A[10])
 
 __device__ __forceinline__ void put(const AsmArgs &A, int row, int col, int tag, double v)
 {
-    if (row < 0 || col < 0 || v == 0.0) return;   // PETSc: negative index ignored, zero not inserted
+    if (row < 0 || col < 0 || v == 0.0 || A.no_csr) return;   // PETSc: negative index ignored, zero not inserted
     if (A.discover) {
         const unsigned long long k = atomicAdd(A.count, 1ull);
         if (k < A.cap) A.keys[k] = (uint64_t(uint32_t(row)) << 32) | (uint64_t(tag) << kTagBits) | uint64_t(col);
@@ -408,6 +409,36 @@ static int run_kernels(hrn_ctx *c, AsmArgs A)
 constexpr unsigned long long kKeysRd = 513ull * 9, kKeysPml = 27ull * 9 + 189ull * 15 * 2 * 3;
 constexpr unsigned long long kKeysPerSlice = 1ull << 29;   // 4 GiB of candidate keys per slice
 
+// Matrix-free operator: only DIAG_M and its inverse (the element kernels apply C, K
+// and G from the mesh and the nodal material).
+static int assemble_mass_only(hrn_ctx *c, AsmArgs A)
+{
+    const int th = 256;
+    HRN_CUDA(c, c->d_diag_m.alloc(size_t(c->neq) * 8));
+    HRN_CUDA(c, c->d_im.alloc(size_t(c->neq) * 8));
+    HRN_CUDA(c, cudaMemsetAsync(c->d_diag_m.p, 0, size_t(c->neq) * 8, c->stream));
+    A.discover = 0;
+    A.no_csr = 1;
+    A.diag_m = c->d_diag_m.as<double>();
+    const int ngroups = int(c->color_off.size()) - 1;
+    for (int g = 0; g < ngroups; ++g) {
+        const int n = c->color_off[g + 1] - c->color_off[g];
+        if (n == 0) continue;
+        A.elems = c->d_el_color_list.as<int32_t>() + c->color_off[g];
+        A.nel = n;
+        k_asm_diag<<<(n * 27 + th - 1) / th, th, 0, c->stream>>>(A, (g % 2) == 1 ? 1 : 0); ++c->launches;
+        HRN_CUDA(c, cudaGetLastError());
+    }
+    k_inv_mass<<<(c->neq + 255) / 256, 256, 0, c->stream>>>(c->neq, c->d_diag_m.as<double>(), c->d_im.as<double>()); ++c->launches;
+    HRN_CUDA(c, cudaGetLastError());
+    int err = 0;
+    HRN_CUDA(c, cudaMemcpyAsync(&err, c->d_asm_err.p, 4, cudaMemcpyDeviceToHost, c->stream));
+    HRN_CUDA(c, cudaStreamSynchronize(c->stream));
+    if (err == 4) return set_error(c, HRN_EMESH, "a PML point lies in the top PML zone");
+    if (err) return set_error(c, HRN_ESTATE, "internal: assembly error flag");
+    return 0;
+}
+
 int assemble_device(hrn_ctx *c, bool discover_pattern)
 {
     if (int rc = upload_asm_tables(c)) return rc;
@@ -424,6 +455,7 @@ int assemble_device(hrn_ctx *c, bool discover_pattern)
     A.pml = c->d_pml.as<double>();
     A.err = c->d_asm_err.as<int>();
     HRN_CUDA(c, cudaMemsetAsync(c->d_asm_err.p, 0, 16, c->stream));
+    if (c->mf_only) return assemble_mass_only(c, A);
     if (discover_pattern) {
         // Candidate keys slice by slice of each (colour, kind) group: each slice's keys
         // are sorted and made unique, then merged into the sorted set of all keys so

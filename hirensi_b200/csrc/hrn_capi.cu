@@ -429,6 +429,7 @@ int hrn_set_operator_csr(hrn_ctx *c, int32_t neq, const int32_t *c_ia, const int
 {
     if (!c) return HRN_EARG;
     ++c->epoch;
+    if (c->mf_only) return set_error(c, HRN_ESTATE, "the context is in matrix-free operator mode");
     if (neq <= 0 || !c_ia || !k_ia || !g_ia || !diag_m) return set_error(c, HRN_EARG, "bad operator arguments");
     if (c->have_mesh && neq != c->neq) return set_error(c, HRN_EARG, "neq differs from the mesh");
     cudaSetDevice(c->device);
@@ -514,12 +515,24 @@ static int assemble_common(hrn_ctx *c, const double *lambda, const double *mu, b
         HRN_CUDA(c, cudaMemcpyAsync(c->d_lam.p, lambda, size_t(c->nj) * 8, cudaMemcpyHostToDevice, c->stream));
         HRN_CUDA(c, cudaMemcpyAsync(c->d_mu.p, mu, size_t(c->nj) * 8, cudaMemcpyHostToDevice, c->stream));
     }
-    const bool first = !c->have_pattern;
-    if (int rc = assemble_device(c, first)) return rc;
+    const bool first = c->mf_only ? !c->have_operator : !c->have_pattern;
+    if (int rc = assemble_device(c, !c->mf_only && first)) return rc;
     c->have_operator = true;
     c->op_from_mesh = true;
     c->have_forward = false;
     if (first) return rebind(c);
+    return HRN_OK;
+}
+
+int hrn_set_operator_mode(hrn_ctx *c, int32_t matrix_free_only)
+{
+    if (!c) return HRN_EARG;
+    ++c->epoch;
+    if (!c->have_mesh) return set_error(c, HRN_ESTATE, "no mesh: call hrn_set_mesh first");
+    const bool mf = matrix_free_only != 0;
+    if (mf == c->mf_only) return HRN_OK;
+    if (c->have_operator) return set_error(c, HRN_ESTATE, "choose the operator mode before the first assembly");
+    c->mf_only = mf;
     return HRN_OK;
 }
 
@@ -538,6 +551,7 @@ int hrn_get_operator_csr(hrn_ctx *c, int32_t which, int32_t *ia, int32_t *ja, do
     cudaSetDevice(c->device);
     if (nnz) *nnz = c->nnz_w[which];
     if (!ia && !ja && !a) return HRN_OK;
+    if (c->mf_only) return set_error(c, HRN_ESTATE, "a matrix-free operator has no stored entries");
     std::vector<double> raw(size_t(std::max<int64_t>(c->nnz, 1)));
     HRN_CUDA(c, cudaStreamSynchronize(c->stream));
     HRN_CUDA(c, cudaMemcpy(raw.data(), c->d_raw.p, size_t(c->nnz) * 8, cudaMemcpyDeviceToHost));

@@ -161,6 +161,7 @@ struct hrn_ctx {
     hrn::DevBuf d_asm_err;        // device error flag of the assembly kernels
     // matrix-free element operator (variants 90 and 91 of the stage kernels)
     bool op_from_mesh = false;    // the operator was assembled from the current mesh and material
+    bool mf_only = false;         // assemble DIAG_M only: the operator is applied matrix-free (no CSR)
     bool have_elem = false;       // element lists, node slot lists and the row map are built
     int nel_pml_e = 0, nel_rd_e = 0;
     hrn::DevBuf d_el_order;       // element ids in processing order: PML, then regular domain

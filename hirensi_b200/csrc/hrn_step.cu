@@ -833,14 +833,17 @@ static int autotune_lanes(hrn_ctx *c, StageArgs<T> a, T *X, T *Y, const TileArgs
     a.hist = nullptr;
     float best = 1e30f;
     int pick = 80;
-    std::vector<int> cand(kVariants, kVariants + 10);
-    if (gt_ready(c, adj) == 0)
+    std::vector<int> cand;
+    if (c->have_pattern) cand.assign(kVariants, kVariants + 10);   // none with a matrix-free operator
+    if (c->have_pattern && gt_ready(c, adj) == 0)
         for (int v : {44, 45, 84, 85}) cand.push_back(v);
     if (c->op_from_mesh) {
         if (int rc = elem_ready(c)) return rc;
         for (int v : {90, 91, 92, 93, 94, 95, 100, 101, 102, 103, 104, 105})
             if (elem_variant_valid(c, v)) cand.push_back(v);
     }
+    if (cand.empty())
+        return set_error(c, HRN_EARG, "no stage variant serves this operator, shot count and precision");
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
@@ -986,6 +989,8 @@ static int forward_t(hrn_ctx *c)
         if (r < 40) return r;
         c->lanes_f = r;
     }
+    if (c->mf_only && !is_elem_variant(c->lanes_f))
+        return set_error(c, HRN_EARG, "the operator is matrix-free: use variants 90-95 / 100-105");
     if (is_elem_variant(c->lanes_f)) {
         if (!elem_variant_valid(c, c->lanes_f)) return set_error(c, HRN_EARG, "matrix-free variant not available for this shot count and precision");
         if (int rc = elem_ready(c)) return rc;
@@ -1087,6 +1092,8 @@ static int adjoint_t(hrn_ctx *c, int lambda_2mu, int keep_p)
         if (r < 40) return r;
         c->lanes_a = r;
     }
+    if (c->mf_only && !is_elem_variant(c->lanes_a))
+        return set_error(c, HRN_EARG, "the operator is matrix-free: use variants 90-95 / 100-105");
     if (is_elem_variant(c->lanes_a)) {
         if (!elem_variant_valid(c, c->lanes_a)) return set_error(c, HRN_EARG, "matrix-free variant not available for this shot count and precision");
         if (int rc = elem_ready(c)) return rc;

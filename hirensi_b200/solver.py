@@ -113,6 +113,11 @@ class Solver:
         self.nj = mesh.nj
         self.neq = mesh.neq
 
+    def set_operator_mode(self, matrix_free: bool):
+        """True: assemble DIAG_M only and apply C, K, G matrix-free (variants 90-105);
+        call after set_mesh, before the first assemble."""
+        self._check(self._L.hrn_set_operator_mode(self.h, int(bool(matrix_free))))
+
     def assemble(self, lam, mu):
         self._check(self._L.hrn_assemble(self.h, dptr(f64(lam)), dptr(f64(mu))))
 

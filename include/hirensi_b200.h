@@ -68,6 +68,15 @@ int hrn_set_mesh(hrn_ctx *ctx, int32_t nj, int32_t nel, int32_t neq,
                  const double *xyz, const int32_t *inod, const int32_t *mtel,
                  const int32_t *id, const double *rho_el, const double *pml_param);
 
+/* Operator mode, chosen after hrn_set_mesh and before the first assembly.
+ * matrix_free_only = 0 (default): hrn_assemble builds the CSR of C, K, G as below, and
+ * every stage variant is available.  matrix_free_only = 1: hrn_assemble computes only
+ * DIAG_M, and C, K, G are applied element by element from the mesh and the nodal
+ * material (variants 90-95 / 100-105).  This needs no stored entries, so meshes whose
+ * CSR would not fit the device (or the 2^31 entry range) can run.  No reference
+ * counterpart: the reference always assembles PETSc matrices. */
+int hrn_set_operator_mode(hrn_ctx *ctx, int32_t matrix_free_only);
+
 /* Device assembly of C, K, G and DIAG_M from nodal lambda, mu (host arrays [nj]):
  * replaces ASSEM_REGULAR_DOMAIN_PETSC_3D (S4/Assemble_PETSc_3D.F90:6-184) and
  * ASSEM_PML_PETSC_3D (:192-436).  The first call fixes the sparsity pattern
@@ -77,7 +86,8 @@ int hrn_assemble(hrn_ctx *ctx, const double *lambda, const double *mu);
 /* hrn_assemble with lambda, mu already on the device (device pointers [nj]). */
 int hrn_assemble_device(hrn_ctx *ctx, const double *d_lambda, const double *d_mu);
 
-/* Download the current operator (unscaled).  With ia/ja/a NULL only *nnz is set. */
+/* Download the current operator (unscaled).  With ia/ja/a NULL only *nnz is set
+ * (0 for a matrix-free operator, which has no entries to download). */
 int hrn_get_operator_csr(hrn_ctx *ctx, int32_t which, int32_t *ia, int32_t *ja, double *a, int64_t *nnz);
 int hrn_get_diag_m(hrn_ctx *ctx, double *diag_m);
 

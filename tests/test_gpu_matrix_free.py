@@ -127,3 +127,40 @@ def test_matrix_free_needs_an_assembled_operator(gpu_lib):
     with pytest.raises(HrnError):
         s.forward()
     s.close()
+
+
+def test_operator_without_csr_equals_assembled_operator(gpu_lib):
+    """hrn_set_operator_mode(matrix-free): only DIAG_M is assembled and the element
+    kernels apply C, K, G; results equal those of the same variant on the fully
+    assembled operator bit for bit (slot variant), and the tuner picks a matrix-free
+    variant."""
+    from hirensi_b200.capi import HrnError
+    from hirensi_b200.solver import Solver
+    p = tiny(nshot=2, nstep=120)
+    _, _, hist_t = oracle_forward(p, p["lam_t"], p["mu_t"])
+    dis = np.stack([traces_from_history(p, h) for h in hist_t])
+    out = []
+    for mf in (False, True):
+        with Solver("fp64") as s:
+            s.set_mesh(p["mesh"], RHO)
+            s.set_operator_mode(mf)
+            s.assemble(p["lam"], p["mu"])
+            s.set_history(p["mesh"].store_eq)
+            s.set_shots(p["nstep"], p["dt"], p["src_eq"], p["src_b"], p["ftab"])
+            s.set_receivers(p["eqdis"], p["eqdis_map"])
+            s.set_variant(92, 92)
+            s.forward()
+            gl, gm = s.adjoint_gradient(dis)
+            out.append(([s.history(k) for k in range(2)], gl, gm, s.diag_m()))
+            if mf:
+                assert s.operator_nnz(1) == 0
+                s.set_variant(41, 41)
+                with pytest.raises(HrnError):
+                    s.forward()
+                s.set_variant(0, 0)
+                s.forward()
+                assert 90 <= s.variant()[0] <= 105
+    for k in range(2):
+        assert np.array_equal(out[0][0][k], out[1][0][k])
+    assert np.array_equal(out[0][1], out[1][1]) and np.array_equal(out[0][2], out[1][2])
+    assert np.array_equal(out[0][3], out[1][3])
