@@ -164,7 +164,7 @@ def stage_bytes(nnz_total: int, n: int, shots: int, bv: int) -> float:
     (value + 4-byte column), three row pointers, and per shot four stage vectors
     read/written per stage plus the x1..x3 update once per step
     (one quarter of the bytes of a whole RK4 step)."""
-    matrix = nnz_total * (bv + 4) + 3 * 4 * (n + 1)
+    matrix = nnz_total * (bv + 4) + (3 * 4 * (n + 1) if nnz_total else 0)
     vectors = shots * (4 * n * bv + 6 * n * bv / 4.0)
     return float(matrix + vectors)
 
@@ -383,7 +383,7 @@ def run_uneven(args, rank, world, local_rank):
     ranks, and --inflight batches run at once on separate contexts (streams) of a GPU.
     The unit counts each shot's own steps: DOF x (2 nstep_s + 1) per shot.
 
-    xl: 8 shots on the 160x160x80 + PML 6 mesh (86.6 M equations), two per batch,
+    xl: 8 shots on the 160x160x80 + PML 6 mesh (86.6 M equations), four per batch,
     checkpoints every 50 steps, one context, matrix-free operator."""
     import torch
     from hirensi_b200 import batching as B
@@ -399,13 +399,13 @@ def run_uneven(args, rank, world, local_rank):
         # 8 shots of 6000-8000 steps and 2500 receivers; dt at 0.15 of the GLL-spacing
         # CFL limit of the fastest P wave of the model distribution (Vs 600, nu 0.40).
         # The CSR of this mesh would exceed the 2^31 entry range: C, K, G are applied
-        # element by element, and two shots per batch keep the checkpointed adjoint's
-        # segment history inside the HBM.
+        # element by element.  Four FP32 shots per batch hold about 40 GB of segment
+        # history (50 steps) and 25 GB of checkpoints.
         vp_max = 600.0 * np.sqrt(2.0 * (1.0 - 0.40) / (1.0 - 2.0 * 0.40))
         dt = 0.15 * (0.5 * 2.5) / vp_max
         prob = uneven_config(nx=160, ny=160, nz=80, npml=6, nshot=8, dt=dt, lengths=(6000, 8000),
                              receivers=(2500, 2500), length_scale=args.length_scale)
-        per_batch, ckpt = 2, 50
+        per_batch, ckpt = 4, 50
     else:
         prob = uneven_config(length_scale=args.length_scale)
         per_batch, ckpt = 8, 100
