@@ -121,3 +121,36 @@ def test_surface_traction_integrates_face_area():
     assert abs(efs[54:81].sum() - 6.0) < 1e-14 and np.all(efs[:54] == 0.0)
     with pytest.raises(ValueError):
         O.element_fs(box_xt(origin=(0.0, 0.0, -5.0)), 5)
+
+
+@pytest.mark.parametrize("eps", [np.diag([1.0, 0.0, 0.0]),
+                                 np.array([[0.3, -0.2, 0.5], [-0.2, -0.7, 0.1], [0.5, 0.1, 0.4]])])
+def test_element_k_patch_test_gives_exact_boundary_tractions(eps):
+    """Uniform strain eps on an affine box with uniform lam, mu: K u equals the
+    consistent boundary forces of the stress sig = lam tr(eps) I + 2 mu eps, that
+    is F_I = sum over the faces f holding node I of (int_f N_I dA) sig n_f, with
+    int_f N_I dA = W_a W_b area_f / 4 for the GLL weights W = (1/3, 4/3, 1/3).
+    The 3-point GLL rule integrates grad N_I . sig exactly here, so the identity
+    holds to rounding.  A swap of the roles of lam and mu breaks it."""
+    h = (2.0, 3.0, 1.5)
+    xt = box_xt(h=h)
+    lam0, mu0 = 130.0, 85.0
+    ek = O.element_k(xt, np.full(27, lam0), np.full(27, mu0))
+    u = (eps @ xt).reshape(-1)                      # u_c(x) = sum_k eps_ck x_k at every node
+    sig = lam0 * np.trace(eps) * np.eye(3) + 2.0 * mu0 * eps
+    W = np.array([1.0, 4.0, 1.0]) / 3.0
+    area = [h[1] * h[2], h[0] * h[2], h[0] * h[1]]  # faces normal to x, y, z
+    f_ref = np.zeros((3, 27))
+    for i, ijk in enumerate(LOCAL_IJK):
+        for ax in range(3):
+            if ijk[ax] == 1:
+                continue
+            n = np.zeros(3)
+            n[ax] = 1.0 if ijk[ax] == 2 else -1.0
+            a, b = [ijk[k] for k in range(3) if k != ax]
+            f_ref[:, i] += W[a] * W[b] * area[ax] / 4.0 * (sig @ n)
+    f = ek @ u
+    scale = np.abs(f_ref).max()
+    assert np.abs(f - f_ref.reshape(-1)).max() < 1e-12 * scale
+    centre = [i for i, ijk in enumerate(LOCAL_IJK) if tuple(ijk) == (1, 1, 1)][0]
+    assert np.abs(f.reshape(3, 27)[:, centre]).max() < 1e-12 * scale

@@ -114,3 +114,24 @@ def test_finite_difference_gradient(prob):
     assert cos > 0.999
     big = np.abs(fd) > 0.1 * np.abs(fd).max()
     assert np.median(np.abs(fd[big] - adj[big]) / np.abs(fd[big])) < 0.1
+
+
+def test_forward_is_fourth_order_in_dt():
+    """Known answer of the integrator: the displacement at a fixed time from steps
+    dt, dt/2, dt/4 (the source sampled at t, t + dt/2, t + dt each step) differs by
+    amounts whose ratio is 2^4 = 16, as for classical RK4 on the semi-discrete
+    system with its C (damping) and G (integral) terms."""
+    p = tiny(nshot=1, nstep=300)
+    om = O.OracleMesh(p["mesh"], RHO)
+    S = O.OracleSystem.assemble(om, p["lam"], p["mu"])
+    b = np.zeros(p["mesh"].neq)
+    b[p["src_eq"][0]] = 1.0
+    T = 0.024
+    end = {}
+    for dt in (2e-4, 1e-4, 5e-5):
+        n = int(round(T / dt))
+        end[dt] = S.forward(b, O.time_table(n, dt, 2, 60.0), n, dt, p["mesh"].store_eq)[-1]
+    assert np.abs(end[5e-5]).max() > 0
+    e1 = np.linalg.norm(end[2e-4] - end[1e-4])
+    e2 = np.linalg.norm(end[1e-4] - end[5e-5])
+    assert 14.0 < e1 / e2 < 18.0
