@@ -463,7 +463,8 @@ int hrn_set_mesh(hrn_ctx *c, int32_t nj, int32_t nel, int32_t neq, const double 
     ++c->epoch;
     if (nj <= 0 || nel <= 0 || neq <= 0 || !xyz || !inod || !mtel || !id || !rho_el || !pml_param)
         return set_error(c, HRN_EARG, "bad mesh arguments");
-    if (c->have_pattern && neq != c->neq) return set_error(c, HRN_EARG, "neq differs from the operator");
+    if ((c->have_pattern || (c->mf_only && c->have_operator)) && neq != c->neq)
+        return set_error(c, HRN_EARG, "neq differs from the operator");
     for (int64_t k = 0; k < int64_t(nel) * 27; ++k)
         if (inod[k] < 0 || inod[k] >= nj) return set_error(c, HRN_EARG, "INOD entry out of range");
     for (int64_t k = 0; k < int64_t(nj) * 9; ++k)
