@@ -40,6 +40,9 @@ namespace hrn {
 __constant__ double e_pml[24];              // PML_PARAM rows x+, x-, y+, y-, z+, z-; cols alpha0, beta0, L, x0
 
 constexpr uint32_t kRdSlot = 0x80000000u;   // slot of a regular-domain element (displacements only)
+// Element grids of at least this many blocks per SM (about eight waves of the
+// combined kernel) take separate PML and regular-domain launches.
+constexpr int kElemSplitBlocksPerSm = 16;
 
 // D[a][b] = l_b'(xi_a) of the 3-point GLL basis: row a (derivative at point a)
 // and column b (derivative of basis b at the three points).
@@ -87,7 +90,8 @@ __device__ void pml_coefs(const double *x, double A[10])
 
 template <typename T>
 struct ElemArgs {
-    int nel_pml, nel_rd, nb_pml;     // elements in processing order: PML first, then the regular domain
+    int nel_pml, nel_rd, nb_pml;     // elements in processing order: PML first, then the regular domain;
+                                     // blocks of PML elements in a combined launch
     const int32_t *el_eq;            // [P][27][9] equation of each point's DOF (-1 fixed)
     const int32_t *el_node;          // [P][27] node of each point
     const double *el_geom;           // [P][27][10] DJI and w*detJ
@@ -105,12 +109,19 @@ constexpr int elems_per_block() { return (S / SV) >= 8 ? 1 : 8 / (S / SV); }
 
 constexpr int kCoef = 14;   // per point: lam, mu, F3 F2 F1 of kinds e, p, w, then b, c, d
 
-// displacement inputs Uu [EPB][3][27][3][S], fluxes V [EPB][27][9][S],
-// coefficients [EPB][27][kCoef], equation numbers [EPB][27][9]
-template <typename T, int S, int SV>
+// Per element of a block, PML / regular domain: displacement inputs U
+// [3 or 1 inputs][27][3][S], fluxes V [27][9][S], coefficients [27][kCoef or 2]
+// (lam, mu only in the regular domain), equation numbers [27][9 or 3] (atomic
+// variants).  A regular-domain element needs a third of the PML element's inputs.
+template <int S, bool PML>
+constexpr int elem_u_stride() { return (PML ? 3 : 1) * 81 * S; }
+template <bool PML>
+constexpr int elem_ncoef() { return PML ? kCoef : 2; }
+template <typename T, int S, int SV, bool PML>
 constexpr size_t elem_smem_bytes()
 {
-    return size_t(elems_per_block<S, SV>()) * ((3 * 81 * S + 243 * S + 27 * kCoef) * sizeof(T) + 243 * sizeof(int));
+    return size_t(elems_per_block<S, SV>()) *
+           ((elem_u_stride<S, PML>() + 243 * S + 27 * elem_ncoef<PML>()) * sizeof(T) + 27 * (PML ? 9 : 3) * sizeof(int));
 }
 
 // N consecutive values from shared or global memory, vectorized when N values
@@ -246,7 +257,8 @@ __device__ __forceinline__ void elem_body(const ElemArgs<T> &A, const StageArgs<
     const bool active = e0 + el < ngrp;
     const int p = pbase + e0 + el;
     const size_t pq = size_t(p) * 27 + q;
-    T *Ue = U + el * 3 * 81 * S;
+    constexpr int NC = elem_ncoef<PML>();
+    T *Ue = U + el * elem_u_stride<S, PML>();
     T ji[9];
     T f0 = T(0), rho = T(0);
     // all global loads of the block are issued in this one phase; the TP
@@ -273,10 +285,10 @@ __device__ __forceinline__ void elem_body(const ElemArgs<T> &A, const StageArgs<
             for (int k = 0; k < S; ++k) dst[k] = v[k];
         }
         if constexpr (ACC == 1)
-            for (int d = tp; d < NDOF; d += TP) eqs[(el * 27 + q) * 9 + d] = __ldg(eqp + d);
+            for (int d = tp; d < NDOF; d += TP) eqs[(el * 27 + q) * NDOF + d] = __ldg(eqp + d);
         const int node = __ldg(A.el_node + pq);
-        T *cf = coef + (el * 27 + q) * kCoef;
-        for (int j = tp; j < (PML ? kCoef : 2); j += TP)
+        T *cf = coef + (el * 27 + q) * NC;
+        for (int j = tp; j < NC; j += TP)
             cf[j] = T(j == 0 ? __ldg(A.lam + node) : (j == 1 ? __ldg(A.mu + node) : __ldg(A.pmlw + size_t(node) * 12 + j - 2)));
     }
     __syncthreads();
@@ -328,7 +340,7 @@ __device__ __forceinline__ void elem_body(const ElemArgs<T> &A, const StageArgs<
             }
     };
     if (active) {
-        const T *cf = coef + (el * 27 + q) * kCoef;
+        const T *cf = coef + (el * 27 + q) * NC;
         const T lam = cf[0], mu = cf[1];
         const T l2 = lam + T(2) * mu, m2 = T(2) * mu;
         if constexpr (PML) {
@@ -480,7 +492,7 @@ __device__ __forceinline__ void elem_body(const ElemArgs<T> &A, const StageArgs<
             for (int d = 0; d < 6; ++d) st_n<T, SV>(o + (3 + d) * S, ys[d]);
         }
     } else {
-        const int *eqo = eqs + (el * 27 + q) * 9;
+        const int *eqo = eqs + (el * 27 + q) * NDOF;
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
             const int eq = eqo[c];
@@ -496,23 +508,35 @@ __device__ __forceinline__ void elem_body(const ElemArgs<T> &A, const StageArgs<
     }
 }
 
-// One thread per (element, GLL point, SV shots); the first nb_pml blocks take
-// PML elements, the rest regular-domain elements.  ACC = 0: write the
+// One thread per (element, GLL point, SV shots).  PART 1 takes the PML
+// elements and PART 2 the regular-domain elements, one launch each: the
+// regular-domain kernel stages a third of the inputs and keeps fewer values
+// live, so it runs four blocks per SM to the PML kernel's two.  PART 0 takes
+// both in one launch (the first nb_pml blocks PML, shared memory laid out for
+// PML elements), which suits grids of a few waves where a second launch would
+// add a tail.  Every part computes an element the same way.  ACC = 0: write the
 // element's slot; ACC = 1: add into the row accumulator.
-template <typename T, int S, int SV, int ADJ, int ACC>
-__global__ void __launch_bounds__(216, 2) k_elem(const ElemArgs<T> A, const StageArgs<T> a, int stage, int mat)
+template <typename T, int S, int SV, int ADJ, int ACC, int PART>
+__global__ void __launch_bounds__(216, PART == 2 ? 4 : 2) k_elem(const ElemArgs<T> A, const StageArgs<T> a, int stage, int mat)
 {
     constexpr int EPB = elems_per_block<S, SV>();
+    constexpr bool PML_LAYOUT = PART != 2;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T *U = reinterpret_cast<T *>(smem_raw);
-    T *V = U + EPB * 3 * 81 * S;
+    T *V = U + EPB * elem_u_stride<S, PML_LAYOUT>();
     T *coef = V + EPB * 243 * S;
-    int *eqs = reinterpret_cast<int *>(coef + EPB * 27 * kCoef);
-    if (int(blockIdx.x) < A.nb_pml)
-        elem_body<T, S, SV, ADJ, ACC, true>(A, a, stage, mat, 0, A.nel_pml, int(blockIdx.x) * EPB, U, V, coef, eqs);
-    else
-        elem_body<T, S, SV, ADJ, ACC, false>(A, a, stage, mat, A.nel_pml, A.nel_rd, (int(blockIdx.x) - A.nb_pml) * EPB, U, V,
-                                             coef, eqs);
+    int *eqs = reinterpret_cast<int *>(coef + EPB * 27 * elem_ncoef<PML_LAYOUT>());
+    const int b = int(blockIdx.x);
+    if constexpr (PART == 1) {
+        elem_body<T, S, SV, ADJ, ACC, true>(A, a, stage, mat, 0, A.nel_pml, b * EPB, U, V, coef, eqs);
+    } else if constexpr (PART == 2) {
+        elem_body<T, S, SV, ADJ, ACC, false>(A, a, stage, mat, A.nel_pml, A.nel_rd, b * EPB, U, V, coef, eqs);
+    } else {
+        if (b < A.nb_pml)
+            elem_body<T, S, SV, ADJ, ACC, true>(A, a, stage, mat, 0, A.nel_pml, b * EPB, U, V, coef, eqs);
+        else
+            elem_body<T, S, SV, ADJ, ACC, false>(A, a, stage, mat, A.nel_pml, A.nel_rd, (b - A.nb_pml) * EPB, U, V, coef, eqs);
+    }
 }
 
 // PML weights of every node: F3, F2, F1 (directions x, y, z) of the kinds
@@ -679,25 +703,25 @@ static int elem_buffers(hrn_ctx *c)
     return 0;
 }
 
-template <typename T, int S, int SV, int ADJ, int ACC>
+template <typename T, int S, int SV, int ADJ, int ACC, int PART>
 static void launch_elem(const ElemArgs<T> &A, const StageArgs<T> &a, int stage, int mat, int blocks, cudaStream_t st)
 {
     static std::atomic<uint64_t> smem_done{0};
-    constexpr size_t smem = elem_smem_bytes<T, S, SV>();
-    smem_limit_once(k_elem<T, S, SV, ADJ, ACC>, int(smem), smem_done);
-    k_elem<T, S, SV, ADJ, ACC><<<blocks, elems_per_block<S, SV>() * 27 * (S / SV), smem, st>>>(A, a, stage, mat);
+    constexpr size_t smem = elem_smem_bytes<T, S, SV, PART != 2>();
+    smem_limit_once(k_elem<T, S, SV, ADJ, ACC, PART>, int(smem), smem_done);
+    k_elem<T, S, SV, ADJ, ACC, PART><<<blocks, elems_per_block<S, SV>() * 27 * (S / SV), smem, st>>>(A, a, stage, mat);
 }
 
-template <typename T, int S, int SV>
+template <typename T, int S, int SV, int PART>
 static void launch_elem_any(const ElemArgs<T> &A, const StageArgs<T> &a, int stage, int mat, int blocks, int adj, int acc,
                             cudaStream_t st)
 {
     if (adj) {
-        if (acc) launch_elem<T, S, SV, 1, 1>(A, a, stage, mat, blocks, st);
-        else launch_elem<T, S, SV, 1, 0>(A, a, stage, mat, blocks, st);
+        if (acc) launch_elem<T, S, SV, 1, 1, PART>(A, a, stage, mat, blocks, st);
+        else launch_elem<T, S, SV, 1, 0, PART>(A, a, stage, mat, blocks, st);
     } else {
-        if (acc) launch_elem<T, S, SV, 0, 1>(A, a, stage, mat, blocks, st);
-        else launch_elem<T, S, SV, 0, 0>(A, a, stage, mat, blocks, st);
+        if (acc) launch_elem<T, S, SV, 0, 1, PART>(A, a, stage, mat, blocks, st);
+        else launch_elem<T, S, SV, 0, 0, PART>(A, a, stage, mat, blocks, st);
     }
 }
 
@@ -719,10 +743,22 @@ static int elem_stage_t(hrn_ctx *c, const StageArgs<T> &a, int stage, int adj, i
     auto go = [&](auto svc) {
         constexpr int SV = decltype(svc)::value;
         constexpr int EPB = elems_per_block<S, SV>();
-        A.nb_pml = (c->nel_pml_e + EPB - 1) / EPB;
-        const int blocks = A.nb_pml + (c->nel_rd_e + EPB - 1) / EPB;
-        if (blocks > 0) {
-            launch_elem_any<T, S, SV>(A, a, stage, mat, blocks, adj, acc, c->stream);
+        const int nb_pml = (c->nel_pml_e + EPB - 1) / EPB, nb_rd = (c->nel_rd_e + EPB - 1) / EPB;
+        if (nb_pml + nb_rd < kElemSplitBlocksPerSm * c->num_sms) {
+            // a few waves: one combined launch
+            A.nb_pml = nb_pml;
+            if (nb_pml + nb_rd > 0) {
+                launch_elem_any<T, S, SV, 0>(A, a, stage, mat, nb_pml + nb_rd, adj, acc, c->stream);
+                ++c->launches;
+            }
+            return;
+        }
+        if (nb_pml > 0) {
+            launch_elem_any<T, S, SV, 1>(A, a, stage, mat, nb_pml, adj, acc, c->stream);
+            ++c->launches;
+        }
+        if (nb_rd > 0) {
+            launch_elem_any<T, S, SV, 2>(A, a, stage, mat, nb_rd, adj, acc, c->stream);
             ++c->launches;
         }
     };

@@ -164,3 +164,36 @@ def test_operator_without_csr_equals_assembled_operator(gpu_lib):
         assert np.array_equal(out[0][0][k], out[1][0][k])
     assert np.array_equal(out[0][1], out[1][1]) and np.array_equal(out[0][2], out[1][2])
     assert np.array_equal(out[0][3], out[1][3])
+
+
+def test_split_element_launches_on_a_larger_mesh(gpu_lib):
+    """24 x 24 x 12 elements + PML 2 (10,976 elements): the element grids of the
+    FP64 2-shot-per-thread and the FP32 1-shot-per-thread variants exceed 16
+    blocks per SM, so the PML and regular-domain elements run as separate
+    launches.  FP64 results equal the CSR kernel's to rounding (another
+    summation order), FP32 results stay within the FP32 bar."""
+    from hirensi_b200.solver import Solver
+    p = tiny(nshot=4, nstep=30, nx=24, ny=24, nz=12, npml=2)
+    assert p["mesh"].inod.shape[0] == 28 * 28 * 14
+
+    def run(precision, variant):
+        with Solver(precision) as s:
+            s.set_mesh(p["mesh"], RHO)
+            s.assemble(p["lam"], p["mu"])
+            s.set_history(p["mesh"].store_eq)
+            s.set_shots(p["nstep"], p["dt"], p["src_eq"], p["src_b"], p["ftab"])
+            s.set_receivers(p["eqdis"], p["eqdis_map"])
+            s.set_variant(variant, variant)
+            s.forward()
+            return [s.history(k) for k in range(4)]
+
+    ref = run("fp64", 41)
+    assert np.abs(ref[0]).max() > 0
+    for v in (92, 93):
+        h = run("fp64", v)
+        for k in range(4):
+            assert rel_l2(h[k], ref[k]) < 1e-12
+    for v in (90, 91):
+        h = run("fp32", v)
+        for k in range(4):
+            assert rel_l2(h[k], ref[k]) < 1e-4
