@@ -1,5 +1,6 @@
 """Integer layout of the generated meshes (bit-exact numbering rules, CPU)."""
 import numpy as np
+import pytest
 
 from hirensi_b200.mesh import GLL_TO_LOCAL, LOCAL_IJK, box_mesh, element_colors, surface_grid
 
@@ -9,6 +10,20 @@ def test_config1_sizes():
     assert m.nel == 5324 and m.nj == 46575
     assert m.rd_dof == 55539          # 3 x (RD + interface nodes)
     assert int((m.mtel == 1).sum()) == 16 * 16 * 8
+
+
+@pytest.mark.parametrize("nx,ny,nz,npml,nel,nj,dof,neq", [
+    (40, 40, 20, 3, 48668, 406503, 807003, 2083956),        # training meshes
+    (80, 80, 40, 4, 340736, 2788281, 6298803, 12679806),    # batched uneven shots
+])
+def test_larger_config_sizes(nx, ny, nz, npml, nel, nj, dof, neq):
+    """Element, node and regular-domain DOF counts of the larger box meshes, and the
+    equation count (PML nodes carry 9 equations, the outer faces fix u)."""
+    m = box_mesh(nx, ny, nz, 2.5, npml)
+    assert m.nel == nel and m.nj == nj
+    assert m.rd_dof == dof
+    assert m.neq == neq
+    assert int((m.mtel == 1).sum()) == nx * ny * nz
 
 
 def test_constraint_and_numbering_rules():
