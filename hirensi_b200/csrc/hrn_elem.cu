@@ -708,6 +708,7 @@ static void launch_elem(const ElemArgs<T> &A, const StageArgs<T> &a, int stage, 
 {
     static std::atomic<uint64_t> smem_done{0};
     constexpr size_t smem = elem_smem_bytes<T, S, SV, PART != 2>();
+    static_assert(smem <= 227 * 1024, "element kernel block exceeds the shared memory of a CTA");
     smem_limit_once(k_elem<T, S, SV, ADJ, ACC, PART>, int(smem), smem_done);
     k_elem<T, S, SV, ADJ, ACC, PART><<<blocks, elems_per_block<S, SV>() * 27 * (S / SV), smem, st>>>(A, a, stage, mat);
 }
