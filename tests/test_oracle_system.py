@@ -135,3 +135,46 @@ def test_forward_is_fourth_order_in_dt():
     e1 = np.linalg.norm(end[2e-4] - end[1e-4])
     e2 = np.linalg.norm(end[1e-4] - end[5e-5])
     assert 14.0 < e1 / e2 < 18.0
+
+
+@pytest.mark.parametrize("alpha0", [0.0, 5.0])
+def test_pml_without_attenuation_keeps_only_the_stretching_coupling(alpha0):
+    """Known answer of the mixed displacement-stress PML: with beta0 = 0 the
+    coefficients b, c, d and the weights of the p and w kinds vanish (each holds a
+    factor beta).  So G has no entries, K is the regular-domain stiffness alone
+    (no stress DOF, no displacement row of a node outside the regular domain), and
+    C couples displacements and stresses only, through the alpha-only weights of
+    kind e.  K does not depend on alpha0."""
+    from hirensi_b200.mesh import box_mesh
+    from problems import layered
+    m = box_mesh(4, 4, 2, 2.5, 1, alpha0=alpha0, beta0=0.0)
+    lam, mu = layered(m)
+    S = O.OracleSystem.assemble(O.OracleMesh(m, RHO), lam, mu)
+    stress = np.zeros(m.neq, bool)
+    e = m.ID[:, 3:9]
+    stress[e[e >= 0]] = True
+    rd_nodes = np.unique(m.inod[m.mtel == 1])
+    in_rd = np.zeros(m.neq, bool)
+    u = m.ID[rd_nodes, 0:3]
+    in_rd[u[u >= 0]] = True
+
+    def blocks(which):
+        ia, ja, a = S.csr(which)
+        rows = np.repeat(np.arange(m.neq), np.diff(ia))
+        nz = a != 0
+        return rows[nz], ja[nz], a[nz]
+
+    r, c, _ = blocks(2)
+    assert r.size == 0
+    r, c, kv = blocks(1)
+    assert r.size > 0 and not stress[r].any() and not stress[c].any()
+    assert in_rd[r].all() and in_rd[c].all()
+    r, c, _ = blocks(0)
+    assert r.size > 0
+    assert np.all(stress[r] != stress[c])
+    # the regular-domain stiffness is the same for any alpha0
+    m0 = box_mesh(4, 4, 2, 2.5, 1, alpha0=0.0, beta0=0.0)
+    S0 = O.OracleSystem.assemble(O.OracleMesh(m0, RHO), lam, mu)
+    ia0, ja0, a0 = S0.csr(1)
+    ia1, ja1, a1 = S.csr(1)
+    assert np.array_equal(ia0, ia1) and np.array_equal(ja0, ja1) and np.array_equal(a0, a1)
