@@ -2,6 +2,7 @@
 import numpy as np
 import pytest
 
+import oracle as O
 from fwi_oracle import OracleBackend
 from hirensi_b200.inversion import FWI, InversionConfig
 from problems import oracle_forward, tiny, traces_from_history
@@ -30,3 +31,35 @@ def test_lbfgs_iterations_reduce_the_misfit(reg):
     assert all(J[i + 1] <= J[i] for i in range(len(J) - 1))   # Armijo accepted every step
     assert J[-1] < J[0]
     assert all(h["armijo"] < 10 for h in hist[1:])
+
+
+@pytest.mark.parametrize("memory", [1, 2, 10])
+def test_coupled_lbfgs_terminates_on_a_quadratic_with_exact_steps(memory):
+    """Known answer of the two-loop recursion: on a strictly convex quadratic in the
+    coupled (lambda, mu) vector, with exact line searches, L-BFGS with H0 = (y's)/(y'y)
+    of the newest pair makes the conjugate-gradient directions (scaled), so it reaches
+    the minimum in at most dim steps for any memory >= 1 (the ring buffer wraps for
+    memory < dim)."""
+    rng = np.random.default_rng(3)
+    nj = 4
+    Q = rng.standard_normal((2 * nj, 2 * nj))
+    A = Q @ Q.T + 0.5 * np.eye(2 * nj)
+    b = rng.standard_normal(2 * nj)
+    lb = O.LBFGSCoupled(nj, memory, np.ones(nj))
+    x = np.zeros(2 * nj)
+    g = A @ x - b
+    g0 = np.linalg.norm(g)
+    x_pre = g_pre = None
+    for it in range(1, 2 * nj + 1):
+        if it == 1:
+            p_l, p_m = lb.direction(it, 1, g[:nj], g[nj:], None, None, x[:nj], x[nj:], None, None)
+        else:
+            p_l, p_m = lb.direction(it, 1, g[:nj], g[nj:], g_pre[:nj], g_pre[nj:], x[:nj], x[nj:],
+                                    x_pre[:nj], x_pre[nj:])
+        p = np.concatenate([p_l, p_m])
+        assert g @ p < 0                       # a descent direction every time
+        alpha = -(g @ p) / (p @ A @ p)         # exact line search
+        x_pre, g_pre = x.copy(), g.copy()
+        x = x + alpha * p
+        g = A @ x - b
+    assert np.linalg.norm(g) < 1e-9 * g0
