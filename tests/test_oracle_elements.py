@@ -154,3 +154,41 @@ def test_element_k_patch_test_gives_exact_boundary_tractions(eps):
     assert np.abs(f - f_ref.reshape(-1)).max() < 1e-12 * scale
     centre = [i for i, ijk in enumerate(LOCAL_IJK) if tuple(ijk) == (1, 1, 1)][0]
     assert np.abs(f.reshape(3, 27)[:, centre]).max() < 1e-12 * scale
+
+
+def test_tv_regularization_is_the_gradient_of_the_tv_functional():
+    """Known answer of the TV term: per node it is the derivative of
+    T(m) = sum over regular-domain elements and GLL points of w detJ sqrt(|grad m|^2 + eps)
+    with eps = 0.01.  T is evaluated here independently (axis-aligned boxes: grad N =
+    dN/dxi * 2/h, detJ = (h/2)^3) and differenced centrally at a few nodes."""
+    from problems import RHO
+    mesh = box_mesh(3, 3, 2, 2.5, 1)
+    om = O.OracleMesh(mesh, RHO)
+    rng = np.random.default_rng(5)
+    x, y, z = mesh.xyz.T
+    mu = 100.0 + 20.0 * np.sin(0.3 * x) * np.cos(0.2 * y) + 5.0 * z + rng.uniform(-1, 1, mesh.nj)
+    lam = 2.0 * mu
+    _, reg_mu, _, _ = O.tv_reg(om, lam, mu)
+    h = mesh.h
+    W = [1.0 / 3.0, 4.0 / 3.0, 1.0 / 3.0]
+    pts = [(a, b, c) for c in range(3) for b in range(3) for a in range(3)]
+    dN = {q: O.shape_3_27(G[q[0]], G[q[1]], G[q[2]])[1] * (2.0 / h) for q in pts}
+    rd = np.nonzero(mesh.mtel == 1)[0]
+
+    def T(m):
+        tot = 0.0
+        for e in rd:
+            me = m[mesh.inod[e]]
+            for q in pts:
+                g = dN[q].T @ me
+                tot += W[q[0]] * W[q[1]] * W[q[2]] * (h / 2.0) ** 3 * np.sqrt(g @ g + 0.01)
+        return tot
+
+    nodes = np.unique(mesh.inod[rd])
+    for k in rng.choice(nodes, 5, replace=False):
+        d = 1e-3
+        mp, mm = mu.copy(), mu.copy()
+        mp[k] += d
+        mm[k] -= d
+        fd = (T(mp) - T(mm)) / (2 * d)
+        assert abs(fd - reg_mu[k]) <= 1e-6 * max(abs(reg_mu[k]), 1e-3)
