@@ -192,3 +192,30 @@ def test_tv_regularization_is_the_gradient_of_the_tv_functional():
         mm[k] -= d
         fd = (T(mp) - T(mm)) / (2 * d)
         assert abs(fd - reg_mu[k]) <= 1e-6 * max(abs(reg_mu[k]), 1e-3)
+
+
+@pytest.mark.parametrize("shear", [0.0, 0.3])
+def test_element_gradient_is_the_derivative_of_the_stiffness_form(shear):
+    """Known answer tying the control kernel (ELEMENT_g_3D) to ELEMENT_K_3D: the
+    adjoint-state gradient of a parameter of K is u^T (dK/dm_i) p.  EK is linear in
+    the nodal lam and mu, so a unit difference of EK gives dK/dm_i exactly, and
+    element_g must equal u^T (EK(m + e_i) - EK(m)) p for every node i."""
+    xt = box_xt(shear=shear)
+    rng = np.random.default_rng(11)
+    lam = rng.uniform(100.0, 160.0, 27)
+    mu = rng.uniform(60.0, 90.0, 27)
+    eu = rng.standard_normal(81)
+    ep = rng.standard_normal(81)
+    gm, gl = O.element_g(xt, eu, ep)
+    k0 = O.element_k(xt, lam, mu)
+    for i in range(27):
+        e = np.zeros(27)
+        e[i] = 1.0
+        dkm = O.element_k(xt, lam, mu + e) - k0
+        dkl = O.element_k(xt, lam + e, mu) - k0
+        assert abs(eu @ dkm @ ep - gm[i]) <= 1e-9 * np.abs(gm).max()
+        assert abs(eu @ dkl @ ep - gl[i]) <= 1e-9 * np.abs(gl).max()
+    # the (lam + 2 mu, mu) parameterization: d/dmu at fixed lam + 2 mu = d/dmu - 2 d/dlam
+    gm2, gl2 = O.element_g(xt, eu, ep, lambda_2mu=True)
+    assert np.abs(gm2 - (gm - 2.0 * gl)).max() <= 1e-12 * np.abs(gm).max()
+    assert np.array_equal(gl2, gl)
