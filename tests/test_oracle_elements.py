@@ -219,3 +219,25 @@ def test_element_gradient_is_the_derivative_of_the_stiffness_form(shear):
     gm2, gl2 = O.element_g(xt, eu, ep, lambda_2mu=True)
     assert np.abs(gm2 - (gm - 2.0 * gl)).max() <= 1e-12 * np.abs(gm).max()
     assert np.array_equal(gl2, gl)
+
+
+@pytest.mark.parametrize("shear", [0.0, 0.3])
+def test_pml_without_stretching_reduces_to_the_elastic_stiffness(shear):
+    """Known answer of the mixed displacement-stress PML element: with alpha = 1 and
+    beta = 0 (no stretching, no attenuation) the stress rows N_a s' = -EA_upper^T u'
+    can be eliminated, and the displacement rows then carry EA_lower N_a^-1 EA_upper^T,
+    which must be the elastic stiffness EK of the same element and material.  This
+    ties the EA blocks of kind e (upper: strain weights 1, 0, 1, 1; lower: lam + 2 mu,
+    lam, 2 mu) and the EN weights (1, 1, 1, 2, 2, 2) to ELEMENT_K_3D."""
+    xt = box_xt(origin=(12.0, 0.0, -1.5), shear=shear)     # inside the x+ PML zone
+    p = default_pml_param(((-10, 10), (-10, 10), (-10, 0)), 3.0, alpha0=0.0, beta0=0.0)
+    rng = np.random.default_rng(1)
+    lam = rng.uniform(100.0, 160.0, 27)
+    mu = rng.uniform(60.0, 90.0, 27)
+    upper = O.element_ea(xt, lam, mu, p, 101)
+    lower = O.element_ea(xt, lam, mu, p, 104)
+    na = O.element_en(xt, p, 301)
+    assert np.count_nonzero(na - np.diag(np.diag(na))) == 0
+    k_eff = lower @ np.diag(1.0 / np.diag(na)) @ upper.T
+    ek = O.element_k(xt, lam, mu)
+    assert np.abs(k_eff - ek).max() <= 1e-13 * np.abs(ek).max()
