@@ -241,3 +241,37 @@ def test_pml_without_stretching_reduces_to_the_elastic_stiffness(shear):
     k_eff = lower @ np.diag(1.0 / np.diag(na)) @ upper.T
     ek = O.element_k(xt, lam, mu)
     assert np.abs(k_eff - ek).max() <= 1e-13 * np.abs(ek).max()
+
+
+@pytest.mark.parametrize("fr", [5.0, 15.0, 60.0])
+def test_time_function_ricker_known_values(fr):
+    """TIME_FUNCTION case 2 (S4/IO.F90:608-621): with u = 2 pi fr t - 3 sqrt(6) the
+    normalized wavelet starts at 0 (u^2 = 54 cancels the 13 e^-13.5 offset), peaks at
+    -1 at u = 0, is symmetric about that centre, is 0 from t = 6 sqrt(6) / (2 pi fr) on,
+    and is minus a Ricker wavelet of peak frequency fr up to the offset."""
+    w = 2.0 * np.pi * fr
+    tc, tmax = 3.0 * np.sqrt(6.0) / w, 6.0 * np.sqrt(6.0) / w
+    off = 13.0 * np.exp(-13.5)
+    assert abs(O.time_function(0.0, 2, fr)) < 1e-15
+    assert abs(O.time_function(tc, 2, fr) + 1.0) < 1e-15
+    assert O.time_function(tmax, 2, fr) == 0.0 and O.time_function(2 * tmax, 2, fr) == 0.0
+    for tau in (0.1 * tc, 0.37 * tc, 0.8 * tc):
+        a, b = O.time_function(tc - tau, 2, fr), O.time_function(tc + tau, 2, fr)
+        assert abs(a - b) < 1e-14
+        ricker = (1.0 - 2.0 * (np.pi * fr * tau) ** 2) * np.exp(-((np.pi * fr * tau) ** 2))
+        assert abs(a - (-0.5 * ricker - off) / (0.5 + off)) < 1e-14
+
+
+def test_time_function_gaussian_and_table_layout():
+    """Case 3 is exp(-(t - 0.06)^2 / 0.0004); the per-step table holds the values at
+    T, T + dt and T + dt/2 (the three calls of the RK4 step)."""
+    assert O.time_function(0.06, 3) == 1.0
+    assert abs(O.time_function(0.08, 3) - np.exp(-1.0)) < 1e-15
+    dt = 1e-3
+    tab = O.time_table(10, dt, 2, 15.0)
+    for i in range(11):
+        T = i * dt
+        assert tab[i, 0] == O.time_function(T, 2, 15.0)
+        assert tab[i, 1] == O.time_function(T + dt, 2, 15.0)
+        assert tab[i, 2] == O.time_function(T + 0.5 * dt, 2, 15.0)
+    assert np.array_equal(tab[1:, 0], tab[:-1, 1])
