@@ -178,3 +178,26 @@ def test_pml_without_attenuation_keeps_only_the_stretching_coupling(alpha0):
     ia0, ja0, a0 = S0.csr(1)
     ia1, ja1, a1 = S.csr(1)
     assert np.array_equal(ia0, ia1) and np.array_equal(ja0, ja1) and np.array_equal(a0, a1)
+
+
+def test_misfit_formula_with_duplicate_receivers():
+    """Compute_Misfit: J = sum over n = 1..NSTEP of dt/2 |r_n|^2, where r_n is
+    assembled into the equation vector, so receivers that share an equation add
+    before squaring; step 0 does not count."""
+    rng = np.random.default_rng(2)
+    nstep, dt, nstore = 12, 1e-3, 9
+    eqdis = np.array([5, 7, 5, 11, 7, 3], np.int32)           # equations 5 and 7 twice
+    eqdis_map = np.array([0, 4, 0, 8, 4, 2], np.int32)        # their positions in U_Store
+    u = rng.standard_normal((nstep + 1, nstore))
+    d = rng.standard_normal((len(eqdis), nstep + 1))
+    J = O.misfit(nstep, dt, eqdis, eqdis_map, u, d)
+    ref = 0.0
+    for n in range(1, nstep + 1):
+        r = {}
+        for q, e in enumerate(eqdis):
+            r[e] = r.get(e, 0.0) + u[n, eqdis_map[q]] - d[q, n]
+        ref += 0.5 * dt * sum(v * v for v in r.values())
+    assert abs(J - ref) <= 1e-14 * ref
+    d0 = d.copy()
+    d0[:, 0] += 100.0
+    assert O.misfit(nstep, dt, eqdis, eqdis_map, u, d0) == J
