@@ -114,3 +114,36 @@ def test_every_stage_kernel_variant_matches_oracle(gpu_lib, variant):
             assert rel_l2(s.history(k), hist[k]) < TOL64
         s.adjoint_gradient(dis, keep_p=True)
         assert rel_l2(s.adjoint_history(0)[1:], pk[1:]) < TOL64
+
+
+def test_receivers_sharing_equations_fp64(gpu_lib):
+    """Receivers listed twice (the same equations with different measured data): the
+    residuals of one equation add before the misfit squares them and before the
+    adjoint source takes them, as the reference assembles them into one vector."""
+    p = tiny(nshot=2, nstep=150)
+    _, _, hist_t = oracle_forward(p, p["lam_t"], p["mu_t"])
+    om, S, hist = oracle_forward(p, p["lam"], p["mu"])
+    dis1 = np.stack([traces_from_history(p, h) for h in hist_t])
+    eqdis = np.concatenate([p["eqdis"], p["eqdis"][:6]])
+    emap = np.concatenate([p["eqdis_map"], p["eqdis_map"][:6]])
+    rng = np.random.default_rng(4)
+    extra = dis1[:, :6] * (1.0 + 0.1 * rng.standard_normal(dis1[:, :6].shape))
+    dis = np.ascontiguousarray(np.concatenate([dis1, extra], axis=1))
+    store = p["mesh"].store_eq
+    J_ref = sum(O.misfit(p["nstep"], p["dt"], eqdis, emap, hist[k], dis[k]) for k in range(2))
+    g_ref_l = np.zeros(p["mesh"].nj)
+    g_ref_m = np.zeros(p["mesh"].nj)
+    for k in range(2):
+        pk = S.adjoint(p["nstep"], p["dt"], store, hist[k], eqdis, emap, dis[k])
+        gl, gm = O.control(om, p["nstep"], p["dt"], store, hist[k], pk)
+        g_ref_l += gl
+        g_ref_m += gm
+    with _solver(p, S) as s:
+        s.set_receivers(eqdis, emap)
+        s.forward()
+        J = s.misfit(dis)
+        assert J > 0 and abs(J - J_ref) <= TOL64 * J_ref
+        gl, gm = s.adjoint_gradient(dis)
+        assert np.abs(g_ref_m).max() > 0
+        assert rel_l2(gl, g_ref_l) < TOL64
+        assert rel_l2(gm, g_ref_m) < TOL64
