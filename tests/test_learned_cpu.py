@@ -2,7 +2,6 @@
 convolution (the oracle of the device kernels) against finite differences, the
 cosine loss gradient and the regular-domain lattice."""
 import numpy as np
-import pytest
 
 from hirensi_b200 import learned as Lr
 from hirensi_b200.mesh import box_mesh
