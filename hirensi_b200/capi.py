@@ -32,6 +32,7 @@ SIGNATURES = {
     "hrn_assemble": (C.c_int, [VP, PD, PD]),
     "hrn_get_operator_csr": (C.c_int, [VP, C.c_int32, PI, PI, PD, PI64]),
     "hrn_get_diag_m": (C.c_int, [VP, PD]),
+    "hrn_apply_operator": (C.c_int, [VP, C.c_int32, C.c_int32, PD, PD]),
     "hrn_set_history": (C.c_int, [VP, C.c_int32, PI]),
     "hrn_set_shots": (C.c_int, [VP, C.c_int32, C.c_int32, C.c_double, C.c_int32, PI, PD, PD]),
     "hrn_set_receivers": (C.c_int, [VP, C.c_int32, PI, PI]),
@@ -54,6 +55,7 @@ SIGNATURES = {
     "hrn_set_data": (C.c_int, [VP, VP, C.c_int32]),
     "hrn_get_gradient_device": (C.c_int, [VP, VP, VP]),
     "hrn_launch_count": (C.c_int, [VP, PI64]),
+    "hrn_time_stage": (C.c_int, [VP, C.c_int32, C.c_int32, PD]),
     "hrn_set_variant": (C.c_int, [VP, C.c_int32, C.c_int32]),
     "hrn_set_shot_records": (C.c_int, [VP, VP, VP]),
     "hrn_set_graphs": (C.c_int, [VP, C.c_int32]),

@@ -570,6 +570,24 @@ int hrn_get_operator_csr(hrn_ctx *c, int32_t which, int32_t *ia, int32_t *ja, do
     return HRN_OK;
 }
 
+int hrn_apply_operator(hrn_ctx *c, int32_t which, int32_t adjoint, const double *x, double *y)
+{
+    if (!c || !x || !y) return HRN_EARG;
+    if (!c->have_operator) return set_error(c, HRN_ESTATE, "no operator");
+    if (which < 0 || which > 2) return set_error(c, HRN_EARG, "which must be 0 (C), 1 (K) or 2 (G)");
+    if (c->mf_only) return set_error(c, HRN_ESTATE, "a matrix-free operator has no stored entries");
+    cudaSetDevice(c->device);
+    DevBuf dx, dy;
+    const size_t vb = size_t(c->neq) * 8;
+    HRN_CUDA(c, dx.alloc(vb));
+    HRN_CUDA(c, dy.alloc(vb));
+    HRN_CUDA(c, cudaMemcpyAsync(dx.p, x, vb, cudaMemcpyHostToDevice, c->stream));
+    if (int rc = run_apply_operator(c, which, adjoint != 0, dx.as<double>(), dy.as<double>())) return rc;
+    HRN_CUDA(c, cudaMemcpyAsync(y, dy.p, vb, cudaMemcpyDeviceToHost, c->stream));
+    HRN_CUDA(c, cudaStreamSynchronize(c->stream));
+    return HRN_OK;
+}
+
 int hrn_get_diag_m(hrn_ctx *c, double *diag_m)
 {
     if (!c || !diag_m) return HRN_EARG;
@@ -830,6 +848,14 @@ int hrn_set_checkpointing(hrn_ctx *c, int32_t interval)
     c->have_forward = false;
     c->have_phist = false;
     return HRN_OK;
+}
+
+int hrn_time_stage(hrn_ctx *c, int32_t adjoint, int32_t nsteps, double *avg_stage_ms)
+{
+    if (!c || !avg_stage_ms || nsteps < 1) return HRN_EARG;
+    if (int rc = check_ready(c, false)) return rc;
+    cudaSetDevice(c->device);
+    return run_time_stage(c, adjoint != 0, nsteps, avg_stage_ms);
 }
 
 int hrn_launch_count(hrn_ctx *c, int64_t *n)

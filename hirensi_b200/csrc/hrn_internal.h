@@ -281,9 +281,11 @@ inline const uint8_t *rec_mask_ptr(const hrn_ctx *c)
     return c->h_rec_mask.empty() ? nullptr : c->d_rec_mask.as<uint8_t>();
 }
 int launch_scale_operator(hrn_ctx *c);
+int run_apply_operator(hrn_ctx *c, int which, int adj, const double *d_x, double *d_y);
 int run_forward(hrn_ctx *c);
 int run_adjoint_gradient(hrn_ctx *c, int lambda_2mu, int keep_p);
 int run_misfit(hrn_ctx *c, double *cost);
+int run_time_stage(hrn_ctx *c, int adj, int nsteps, double *avg_ms);
 int run_pseudo_hessian(hrn_ctx *c, double *hl, double *hm);
 int build_rd_geometry(hrn_ctx *c);
 int assemble_device(hrn_ctx *c, bool discover_pattern);

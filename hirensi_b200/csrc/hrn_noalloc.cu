@@ -64,7 +64,9 @@ __global__ void k_noalloc_sum(int nshot, int nstep, double dt, const double *__r
 }
 
 // Device address of the scratch array, looked up once per device with that
-// device current (in host code the symbol is only a host-side stand-in).
+// device current (in host code the symbol is only a host-side stand-in).  The
+// address belongs to the device's primary context: after a cudaDeviceReset the
+// cached value is stale, so the entry must not be used across one.
 static int scratch_address(hrn_ctx *c, double **out)
 {
     static std::mutex mu;
@@ -94,6 +96,18 @@ extern "C" int hrn_misfit_noalloc(hrn_ctx *c, const double *d_dis_meas, double *
     if (!c->have_forward) return set_error(c, HRN_ESTATE, "no forward history: call hrn_forward first");
     if (c->nrec3 > 0 && !d_dis_meas) return set_error(c, HRN_EARG, "null measured data");
     HRN_CUDA(c, cudaSetDevice(c->device));
+    if (c->nrec3 > 0) {
+        // hrn_misfit takes a host pointer of the same C type: refuse host memory and
+        // other devices' memory here rather than fault in the kernel
+        cudaPointerAttributes at{};
+        cudaError_t e = cudaPointerGetAttributes(&at, d_dis_meas);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            return set_error(c, HRN_EARG, "d_dis_meas is not a device pointer");
+        }
+        if ((at.type != cudaMemoryTypeDevice && at.type != cudaMemoryTypeManaged) || at.device != c->device)
+            return set_error(c, HRN_EARG, "d_dis_meas must point to device (or managed) memory of the context's device");
+    }
     double *scratch = nullptr;
     if (int rc = scratch_address(c, &scratch)) return rc;
     double *terms = scratch, *out = scratch + kNoAllocMaxTerms;

@@ -237,6 +237,26 @@ __global__ void k_scale_adj(int64_t nnz, const int64_t *__restrict__ permT, cons
     }
 }
 
+// One per-step operator applied to an FP64 vector: y_i = sum over the row's
+// entries of matrix `which` of val * x[col], from the values the stage kernels
+// stream (forward: -iM A, row order; adjoint: the transposed adjoint-scaled
+// values, so y = A'^T x).  Used by the dot-product tests of the device operator.
+template <typename T>
+__global__ void k_apply_operator(int n, const int32_t *__restrict__ rowptr, const uint32_t *__restrict__ colx,
+                                 const T *__restrict__ val, uint32_t which, const double *__restrict__ x,
+                                 double *__restrict__ y)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        double s = 0.0;
+        for (int32_t k = rowptr[i]; k < rowptr[i + 1]; ++k) {
+            const uint32_t cw = colx[k];
+            if ((cw >> kTagBits) != which) continue;
+            s = fma(double(val[k]), x[cw & kColMask], s);
+        }
+        y[i] = s;
+    }
+}
+
 // ----------------------------------------------------------------------------
 // sources
 
@@ -488,6 +508,23 @@ static int scale_operator_t(hrn_ctx *c)
     k_scale_adj<T><<<blocks_for(c->nnz, th), th, 0, c->stream>>>(c->nnz, c->d_permT.as<int64_t>(), c->d_rowidx.as<int32_t>(),
                                                                   c->d_colx.as<uint32_t>(), c->d_raw.as<double>(),
                                                                   c->d_diag_m.as<double>(), c->d_im.as<double>(), c->d_adj.as<T>()); ++c->launches;
+    HRN_CUDA(c, cudaGetLastError());
+    return 0;
+}
+
+int run_apply_operator(hrn_ctx *c, int which, int adj, const double *d_x, double *d_y)
+{
+    const int th = 256;
+    const int32_t *rp = adj ? c->d_rowptrT.as<int32_t>() : c->d_rowptr.as<int32_t>();
+    const uint32_t *cx = adj ? c->d_colxT.as<uint32_t>() : c->d_colx.as<uint32_t>();
+    const int grid = blocks_for(c->neq, th);
+    if (c->precision == HRN_FP64)
+        k_apply_operator<double><<<grid, th, 0, c->stream>>>(c->neq, rp, cx, adj ? c->d_adj.as<double>() : c->d_fwd.as<double>(),
+                                                              uint32_t(which), d_x, d_y);
+    else
+        k_apply_operator<float><<<grid, th, 0, c->stream>>>(c->neq, rp, cx, adj ? c->d_adj.as<float>() : c->d_fwd.as<float>(),
+                                                             uint32_t(which), d_x, d_y);
+    ++c->launches;
     HRN_CUDA(c, cudaGetLastError());
     return 0;
 }
@@ -1248,6 +1285,70 @@ static int pseudo_hessian_t(hrn_ctx *c, double *hl, double *hm)
     case 8: return FN<T, 8>(c, ##__VA_ARGS__);            \
     default: return set_error(c, HRN_EARG, "nshot out of range"); \
     }
+
+// Device time of the stage kernel alone: nsteps RK4 steps (4 stage launches
+// each) of the tuned variant, back to back from the zero state with the first
+// step's sources and no history, bracketed by one pair of CUDA events on the
+// context's stream.  The traffic of a stage does not depend on the values.  The forward history and
+// the checkpoints are untouched; the state and stage buffers are scratch.
+template <typename T, int S>
+static int time_stage_t(hrn_ctx *c, int adj, int nsteps, double *avg_ms)
+{
+    const int lanes = adj ? c->lanes_a : c->lanes_f;
+    if (lanes <= 0) return set_error(c, HRN_ESTATE, "no tuned stage variant: run hrn_forward (and hrn_adjoint_gradient) first");
+    const size_t vn = size_t(c->neq) * S;
+    T *X0 = c->d_X.as<T>(), *X1 = X0 + 3 * vn;
+    StageArgs<T> a = forward_args<T, S>(c);
+    TileArgs ta{c->d_tiles.as<int32_t>(), c->ntiles, std::min(c->ntiles, 2 * c->num_sms), c->d_step_err.as<int>()};
+    if (adj) {
+        a.rowptr = c->d_rowptrT.as<int32_t>();
+        a.seg = c->d_segT.as<int2>();
+        a.colx = c->d_colxT.as<uint32_t>();
+        a.val = c->d_adj.as<T>();
+        a.slot = c->d_slot_a.as<int32_t>();
+        a.nslot = c->nslot_a;
+        a.c = T(-0.5 * c->dt);
+        a.D = T(-c->dt);
+        a.d6 = T(-c->dt / 6.0);
+        ta = TileArgs{c->d_tilesT.as<int32_t>(), c->ntilesT, std::min(c->ntilesT, 2 * c->num_sms), c->d_step_err.as<int>()};
+    }
+    // the sources of the first step (the tables exist once the variant is tuned)
+    a.srcv = adj ? c->d_srcv_a.as<T>() : forward_src<T, S>(c, 0);
+    a.hist = nullptr;
+    if (a.nslot > 0 && !a.srcv) return set_error(c, HRN_ESTATE, "no source table: run the time loop first");
+    if (is_elem_variant(lanes)) {
+        if (int rc = elem_ready(c)) return rc;
+    } else if (is_gt_variant(lanes)) {
+        if (int rc = gt_ready(c, adj)) return rc;
+    }
+    HRN_CUDA(c, cudaMemsetAsync(X0, 0, 6 * vn * sizeof(T), c->stream));
+    launch_step<T, S>(c, a, X0, X1, nullptr, lanes, ta, adj);   // warm-up
+    cudaEvent_t e0, e1;
+    HRN_CUDA(c, cudaEventCreate(&e0));
+    HRN_CUDA(c, cudaEventCreate(&e1));
+    cudaEventRecord(e0, c->stream);
+    for (int n = 0; n < nsteps; ++n) {
+        T *X = (n & 1) ? X1 : X0, *Y = (n & 1) ? X0 : X1;
+        launch_step<T, S>(c, a, X, Y, nullptr, lanes, ta, adj);
+    }
+    cudaEventRecord(e1, c->stream);
+    const cudaError_t es = cudaEventSynchronize(e1);
+    float ms = 0.f;
+    if (es == cudaSuccess) cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    HRN_CUDA(c, es);
+    HRN_CUDA(c, cudaGetLastError());
+    if (int rc = check_step_error(c)) return rc;
+    *avg_ms = double(ms) / (4.0 * nsteps);
+    return 0;
+}
+
+int run_time_stage(hrn_ctx *c, int adj, int nsteps, double *avg_ms)
+{
+    if (c->precision == HRN_FP64) { HRN_DISPATCH_S(time_stage_t, double, adj, nsteps, avg_ms) }
+    HRN_DISPATCH_S(time_stage_t, float, adj, nsteps, avg_ms)
+}
 
 int run_forward(hrn_ctx *c)
 {

@@ -140,6 +140,16 @@ class Solver:
         self._check(self._L.hrn_get_operator_csr(self.h, which, iptr(ia), iptr(ja), dptr(a), C.byref(nnz)))
         return ia, ja, a
 
+    def apply_operator(self, which: int, x, adjoint: bool = False) -> np.ndarray:
+        """One per-step operator on the device: -iM A x (forward) or A'^T x (the
+        adjoint-scaled operator, transposed), A = C (0), K (1) or G (2)."""
+        xv = f64(x)
+        if xv.size != self.neq:
+            raise ValueError("x must have neq entries")
+        y = np.zeros(self.neq)
+        self._check(self._L.hrn_apply_operator(self.h, int(which), int(bool(adjoint)), dptr(xv), dptr(y)))
+        return y
+
     def diag_m(self):
         d = np.zeros(self.neq)
         self._check(self._L.hrn_get_diag_m(self.h, dptr(d)))
@@ -214,6 +224,14 @@ class Solver:
         f, a = C.c_int32(), C.c_int32()
         self._check(self._L.hrn_get_variant(self.h, C.byref(f), C.byref(a)))
         return f.value, a.value
+
+    def time_stage(self, adjoint: bool = False, nsteps: int = 50) -> float:
+        """Milliseconds of one stage launch of the tuned variant, from `nsteps` RK4
+        steps launched back to back under one pair of CUDA events (no per-launch
+        events).  The state buffers are scratch afterwards; the history stays."""
+        ms = C.c_double()
+        self._check(self._L.hrn_time_stage(self.h, int(bool(adjoint)), int(nsteps), C.byref(ms)))
+        return ms.value
 
     def launch_count(self) -> int:
         n = C.c_int64()

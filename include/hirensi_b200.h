@@ -91,6 +91,15 @@ int hrn_assemble_device(hrn_ctx *ctx, const double *d_lambda, const double *d_mu
 int hrn_get_operator_csr(hrn_ctx *ctx, int32_t which, int32_t *ia, int32_t *ja, double *a, int64_t *nnz);
 int hrn_get_diag_m(hrn_ctx *ctx, double *diag_m);
 
+/* One per-step operator of the time loops applied to a host vector x [neq]:
+ * adjoint = 0: y = -iM A x, the scaled matrix of EXPLICIT_RK4_PETSC_PML_3D
+ * (S4/Solver_PETSc_Explicit.F90:815-824); adjoint = 1: y = A'^T x with A' the
+ * adjoint-scaled matrix applied by MatMultTransposeAdd in the adjoint
+ * (:1219-1229, 1319-1364).  which: 0 = C, 1 = K, 2 = G.  It reads the device
+ * values the stage kernels stream, so dot-product tests can check the device
+ * operator.  Not available for a matrix-free operator (HRN_ESTATE). */
+int hrn_apply_operator(hrn_ctx *ctx, int32_t which, int32_t adjoint, const double *x, double *y);
+
 /* ---- problem description --------------------------------------------------- */
 
 /* History equations U_Store_Numbers_Global (S3/PIC_Inversion_Data_Structure.F90:255-300). */
@@ -161,13 +170,16 @@ int hrn_misfit(hrn_ctx *ctx, const double *dis_meas, double *cost);
 /* The misfit of hrn_misfit for callers that cannot allocate device memory.
  * It has no counterpart in the reference.  d_dis_meas is a DEVICE pointer to
  * Dis_meas laid out as for hrn_set_data ([nshot][nrec3][nstep+1]); it is read
- * in place and not kept.  The scratch is one static device array shared by
- * every context and call in the process, so nothing is allocated.  Limit:
- * nshot * (nstep + 1) <= 131072, larger problems return HRN_EARG.  The first
- * call on a device looks the array's address up (cudaGetSymbolAddress) with
- * that device current; make that first call before any stream capture.  Calls
- * whose kernels overlap on one GPU (other streams, other contexts, other host
- * threads) race on the scratch: serialize them.  Blocks until *cost is ready. */
+ * in place and not kept.  A host pointer, or memory of another device, returns
+ * HRN_EARG before anything is launched.  The scratch is one static device array
+ * shared by every context and call in the process, so nothing is allocated.
+ * Limit: nshot * (nstep + 1) <= 131072, larger problems return HRN_EARG.  The
+ * first call on a device looks the array's address up (cudaGetSymbolAddress)
+ * with that device current and keeps it; make that first call before any stream
+ * capture, and do not use the entry across a cudaDeviceReset.  Calls whose
+ * kernels overlap on one GPU (other streams, other contexts, other host threads)
+ * race on the scratch: serialize them.  It synchronizes its stream and returns
+ * once *cost is ready. */
 int hrn_misfit_noalloc(hrn_ctx *ctx, const double *d_dis_meas, double *cost);
 
 /* Adjoint RK4 (OtD) with the zero-lag gradient fused into each step:
@@ -245,6 +257,15 @@ int hrn_set_timing(hrn_ctx *ctx, int32_t enable);
  * duration and number of launches of the fused stage kernel since timing was
  * last enabled. */
 int hrn_last_timing(hrn_ctx *ctx, double *total_ms, double *stage_kernel_ms, int64_t *stage_launches);
+
+/* Device time of one stage launch alone: nsteps RK4 steps (4 stage launches each)
+ * of the tuned variant of the forward (adjoint = 0) or adjoint operator, launched
+ * back to back from a zeroed state with the first step's sources and no history,
+ * bracketed by one pair of CUDA events on the context's stream;
+ * *avg_stage_ms = elapsed / (4 nsteps).  The forward history stays valid; the
+ * state buffers are overwritten.  Needs a tuned variant (after hrn_forward /
+ * hrn_adjoint_gradient).  No reference counterpart: a measurement aid. */
+int hrn_time_stage(hrn_ctx *ctx, int32_t adjoint, int32_t nsteps, double *avg_stage_ms);
 
 /* Stage-kernel variant per operator (forward, adjoint): lanes per row * 10 +
  * (1 if the stage inputs are materialized by the previous stage, 0 if rebuilt

@@ -1040,23 +1040,37 @@ int ora_adjoint(const ora_sys *s, int nstep, double dt, int nstore, const int *s
 }
 
 /* A12: S4/Solver_PETSc_Explicit.F90:1413-1522 with Update_g
- * (S4/Assemble_PETSc_3D.F90:556-661).  Node index = material index. */
+ * (S4/Assemble_PETSc_3D.F90:556-661).  Node index = material index.
+ * The element terms of a step are computed in parallel (nthreads > 1) into one
+ * buffer per element and then added to the nodes serially in element order, so
+ * every thread count gives the bits of the serial loop.  The reference runs the
+ * same element loop on every MPI rank over its own elements. */
 int ora_control(const ora_mesh *m, int nstep, double dt, int nstore, const int *store_eq,
-                const double *u_store, const double *p_store, double *g_lam, double *g_mu, int lambda_2mu)
+                const double *u_store, const double *p_store, double *g_lam, double *g_mu, int lambda_2mu,
+                int nthreads)
 {
     int n = m->neq;
+    set_threads(nthreads);
+    int nrd = 0;
+    for (int e = 0; e < m->nel; ++e) nrd += m->mtel[e] == 1;
+    int *rd = (int *)malloc(sizeof(int) * (size_t)(nrd ? nrd : 1));
+    for (int e = 0, k = 0; e < m->nel; ++e) if (m->mtel[e] == 1) rd[k++] = e;
     double *ub = (double *)calloc((size_t)n, sizeof(double));
     double *pb = (double *)calloc((size_t)n, sizeof(double));
-    for (int istep = 1; istep <= nstep - 1; ++istep) {
+    double *egm = (double *)malloc(sizeof(double) * 27 * (size_t)(nrd ? nrd : 1));
+    double *egl = (double *)malloc(sizeof(double) * 27 * (size_t)(nrd ? nrd : 1));
+    int bad = 0;
+    for (int istep = 1; istep <= nstep - 1 && !bad; ++istep) {
         memset(ub, 0, sizeof(double) * (size_t)n);
         memset(pb, 0, sizeof(double) * (size_t)n);
         for (int i = 0; i < nstore; ++i) {
             ub[store_eq[i]] += u_store[(size_t)istep * nstore + i];
             pb[store_eq[i]] += p_store[(size_t)istep * nstore + i];
         }
-        for (int e = 0; e < m->nel; ++e) {
-            if (m->mtel[e] != 1) continue;
-            double xt[3][27], eu[81], ep[81], gm[27], gl[27];
+        #pragma omp parallel for schedule(static) reduction(|:bad)
+        for (int k = 0; k < nrd; ++k) {
+            int e = rd[k];
+            double xt[3][27], eu[81], ep[81];
             gather_xt(m, e, xt);
             for (int c = 0; c < 3; ++c)
                 for (int i = 0; i < 27; ++i) {
@@ -1064,16 +1078,20 @@ int ora_control(const ora_mesh *m, int nstep, double dt, int nstore, const int *
                     eu[c * 27 + i] = q >= 0 ? ub[q] : 0.0;
                     ep[c * 27 + i] = q >= 0 ? pb[q] : 0.0;
                 }
-            if (ora_element_g(xt, eu, ep, gm, gl, lambda_2mu)) { free(ub); free(pb); return -1; }
+            if (ora_element_g(xt, eu, ep, egm + 27 * (size_t)k, egl + 27 * (size_t)k, lambda_2mu)) bad |= 1;
+        }
+        if (bad) break;
+        for (int k = 0; k < nrd; ++k) {
+            int e = rd[k];
             for (int i = 0; i < 27; ++i) {
                 int node = m->inod[e * 27 + i];
-                g_mu[node] += gm[i] * dt;
-                g_lam[node] += gl[i] * dt;
+                g_mu[node] += egm[27 * (size_t)k + i] * dt;
+                g_lam[node] += egl[27 * (size_t)k + i] * dt;
             }
         }
     }
-    free(ub); free(pb);
-    return 0;
+    free(ub); free(pb); free(egm); free(egl); free(rd);
+    return bad ? -1 : 0;
 }
 
 /* A13: S4/Solver_PETSc_Inverse.F90:591-657 (Compute_Misfit). */

@@ -77,9 +77,11 @@ int ora_forward(const ora_sys *s, const double *b, const double *ftab, int nstep
 int ora_adjoint(const ora_sys *s, int nstep, double dt, int nstore, const int *store_eq,
                 const double *u_store, int nrec3, const int *eqdis, const int *eqdis_map,
                 const double *dis_meas, double *p_store, int nthreads);
-/* A12: control (gradient) accumulation over steps 1..nstep-1, scale dt. */
+/* A12: control (gradient) accumulation over steps 1..nstep-1, scale dt.
+ * nthreads > 1 computes the element terms in parallel; the result is the same. */
 int ora_control(const ora_mesh *m, int nstep, double dt, int nstore, const int *store_eq,
-                const double *u_store, const double *p_store, double *g_lam, double *g_mu, int lambda_2mu);
+                const double *u_store, const double *p_store, double *g_lam, double *g_mu, int lambda_2mu,
+                int nthreads);
 /* A13 */
 double ora_misfit(int nstep, double dt, int nrec3, const int *eqdis, const int *eqdis_map,
                   int nstore, const double *u_store, const double *dis_meas);

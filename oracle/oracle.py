@@ -49,7 +49,7 @@ def lib():
         L.ora_sys_vectors.argtypes = [C.c_void_p, PD, PD]
         L.ora_forward.argtypes = [C.c_void_p, PD, PD, C.c_int, C.c_double, C.c_int, PI, PD, C.c_int]
         L.ora_adjoint.argtypes = [C.c_void_p, C.c_int, C.c_double, C.c_int, PI, PD, C.c_int, PI, PI, PD, PD, C.c_int]
-        L.ora_control.argtypes = [C.POINTER(_Mesh), C.c_int, C.c_double, C.c_int, PI, PD, PD, PD, PD, C.c_int]
+        L.ora_control.argtypes = [C.POINTER(_Mesh), C.c_int, C.c_double, C.c_int, PI, PD, PD, PD, PD, C.c_int, C.c_int]
         L.ora_misfit.restype = C.c_double
         L.ora_misfit.argtypes = [C.c_int, C.c_double, C.c_int, PI, PI, C.c_int, PD, PD]
         L.ora_tv_reg.argtypes = [C.POINTER(_Mesh), PD, PD, PD, PD, PD, PD]
@@ -257,12 +257,14 @@ class OracleSystem:
         return y
 
 
-def control(om: OracleMesh, nstep, dt, store_eq, u_store, p_store, lambda_2mu=False):
+def control(om: OracleMesh, nstep, dt, store_eq, u_store, p_store, lambda_2mu=False, nthreads=0):
+    """Raw (g_lambda, g_mu) of the control accumulation; nthreads 0 keeps the current
+    OpenMP setting, and every thread count gives the same bits."""
     gl = np.zeros(om.mesh.nj)
     gm = np.zeros(om.mesh.nj)
     store_eq = _i32(store_eq)
     rc = lib().ora_control(C.byref(om.c), nstep, float(dt), store_eq.size, _i(store_eq), _d(_f64(u_store)),
-                           _d(_f64(p_store)), _d(gl), _d(gm), int(lambda_2mu))
+                           _d(_f64(p_store)), _d(gl), _d(gm), int(lambda_2mu), int(nthreads))
     assert rc == 0
     return gl, gm
 
