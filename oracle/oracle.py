@@ -359,3 +359,125 @@ class LBFGSCoupled:
             r_l = r_l + self.Ss_l[:, i] * (self.alphas[i] - beta)
             r_m = r_m + self.Ss_m[:, i] * (self.alphas[i] - beta)
         return -r_l, -r_m
+
+
+# --- inversion loop (S4/Program_Main.F90:379-896) ------------------------------
+
+class ArmijoStop(RuntimeError):
+    """The reference STOPs after the tenth Armijo trial (S4/Program_Main.F90:883-889)."""
+
+
+def _extend_and_clip(v, extend_to, lo, hi):
+    """VIII (:633-636) then IX (:638-678): the PML nodes take the material of
+    their interface node (VecScatter INSERT_VALUES), then every node is clipped
+    to the bounds."""
+    v = v[extend_to]
+    return np.where(v < lo, lo, np.where(v > hi, hi, v))
+
+
+def inversion_loop(evaluate, gradient, lam0, mu0, n_iter, img, restriction, extend_to, bounds_lambda, bounds_mu,
+                   m_lbfgs=15, fac_max_update=(5.0, 5.0), tv=None, reg_factor=0.3, bias_lambda=True,
+                   n_iter_bias=50, iter_begin=1):
+    """Numpy restatement of the reference's inversion iterations for
+    Control_Parameter = 'Lambda_Mu', Lambda_variable = 'Lambda' and
+    Search_Direction_Method = 'LBFGS', written from S4/Program_Main.F90:
+    * evaluate(lam, mu) -> misfit of the forward solve of that model (Include
+      'Solve_Forward.F90' + Compute_Misfit);
+    * gradient() -> (g_lambda, g_mu) raw accumulated gradient of the model
+      evaluated last (..._Adjoint_OtD + ..._Control_OtD, before the sign flip);
+    * tv(lam, mu) -> (reg_lambda, reg_mu, cost_lambda, cost_mu) or None for no
+      regularization (Assem_TV_TN_Regularization);
+    * img, restriction: the inverse gradient mass and the regular-domain mask
+      (S4/Control_Problem_Operators.F90:11-22); extend_to: the PML material
+      extension map (vscat_mat_extend).
+    Returns a list of per-iteration records (iteration 0 = the initial model):
+    misfit, alpha_lambda, alpha_mu, armijo trials, and the model after the
+    iteration.  Raises ArmijoStop where the reference STOPs."""
+    fac_l, fac_m = float(fac_max_update[0]), float(fac_max_update[1])
+    lb = LBFGSCoupled(len(lam0), m_lbfgs, restriction)
+    lam = np.array(lam0, dtype=np.float64)
+    mu = np.array(mu0, dtype=np.float64)
+    lam_pre = np.zeros_like(lam)
+    mu_pre = np.zeros_like(mu)
+    g_l = np.zeros_like(lam)
+    g_m = np.zeros_like(mu)
+    J = evaluate(lam, mu)                                         # :327-333
+    recs = [dict(iter=0, misfit=J, armijo=0, lam=lam.copy(), mu=mu.copy())]
+
+    def trial(a_l, a_m, it, p_l, p_m):
+        """VII (:597-628) + VIII + IX: the model of step sizes a_l, a_m."""
+        if bias_lambda and it < n_iter_bias:
+            W = 1.0 - float(it // n_iter_bias)                    # DBLE(Iter/NIterBias): integer division
+            pm_n = float(np.sqrt(p_m @ p_m))
+            pl_n = float(np.sqrt(p_l @ p_l))
+            fb_mu = W * pl_n / pm_n * a_l
+            fb_lam = (1.0 - W) * pl_n * a_l
+            new_l = lam_pre + (fb_mu * p_m + fb_lam * p_l)        # VecCopy + VecMAXPY
+        else:
+            new_l = a_l * p_l + lam_pre                           # VecWAXPY
+        new_m = a_m * p_m + mu_pre
+        return (_extend_and_clip(new_l, extend_to, *bounds_lambda),
+                _extend_and_clip(new_m, extend_to, *bounds_mu))
+
+    for it in range(iter_begin, iter_begin + n_iter):
+        J_pre = J                                                 # II (:384-392)
+        g_l_pre, g_m_pre = g_l.copy(), g_m.copy()
+        raw_l, raw_m = gradient()                                 # III (:398-409)
+        g_l = -np.asarray(raw_l, dtype=np.float64)                # :412-413
+        g_m = -np.asarray(raw_m, dtype=np.float64)
+        if tv is not None:                                        # IV (:418-450)
+            reg_l, reg_m, _, _ = tv(lam, mu)
+            f_l = reg_factor * float(np.sqrt(g_l @ g_l)) / float(np.sqrt(reg_l @ reg_l))
+            f_m = reg_factor * float(np.sqrt(g_m @ g_m)) / float(np.sqrt(reg_m @ reg_m))
+            if it != 1:
+                g_l = g_l + f_l * reg_l
+                g_m = g_m + f_m * reg_m
+        g_l = g_l * img                                           # :454-455
+        g_m = g_m * img
+        p_l, p_m = lb.direction(it, iter_begin, g_l, g_m, g_l_pre, g_m_pre, lam, mu, lam_pre, mu_pre)   # VI-2
+        lam_pre, mu_pre = lam.copy(), mu.copy()                   # VI-3 (:524-526)
+        gp_l = float(g_l @ p_l)                                   # VI-4 (:529-556)
+        chk_l = gp_l > 0
+        if chk_l:
+            p_l = -g_l
+            gp_l = float(g_l @ p_l)
+        gp_m = float(g_m @ p_m)
+        chk_m = gp_m > 0
+        if chk_m:
+            p_m = -g_m
+            gp_m = float(g_m @ p_m)
+        pl_max = float(np.abs(p_l).max())                         # VI-5 (:558-593)
+        pm_max = float(np.abs(p_m).max())
+        a_l, a_m = fac_l / pl_max, fac_m / pm_max
+        a_l_sd, a_m_sd = a_l, a_m
+        if it != iter_begin:
+            a_l = a_m = 1.0
+            if pl_max > fac_l:
+                a_l = fac_l / pl_max
+            if pm_max > fac_m:
+                a_m = fac_m / pm_max
+        if chk_l:
+            a_l = a_l_sd
+        if chk_m:
+            a_m = a_m_sd
+        lam, mu = trial(a_l, a_m, it, p_l, p_m)
+        J = evaluate(lam, mu)                                     # X-3, X-4
+        armijo = 1.0e-4 * abs(a_m) * gp_m + 1.0e-4 * abs(a_l) * gp_l
+        count = 0
+        while J > J_pre + armijo:                                 # X-5 (:737-896)
+            count += 1
+            if count == 3:
+                fac_l /= 6.0
+                fac_m /= 6.0
+            a_l *= 0.5
+            a_m *= 0.5
+            if count == 9:
+                a_l, a_m = -a_l, -a_m
+            lam, mu = trial(a_l, a_m, it, p_l, p_m)
+            J = evaluate(lam, mu)
+            armijo = 1.0e-4 * abs(a_m) * gp_m + 1.0e-4 * abs(a_l) * gp_l
+            if count == 10:
+                raise ArmijoStop(f"Armijo condition failure at iteration {it}")
+        recs.append(dict(iter=it, misfit=J, armijo=count, alpha_lambda=a_l, alpha_mu=a_m,
+                         lam=lam.copy(), mu=mu.copy()))
+    return recs

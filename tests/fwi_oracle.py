@@ -1,5 +1,7 @@
-"""Oracle backend of hirensi_b200.inversion.FWI: numpy vectors, the CPU
-restatement for assembly, time loops, gradient, TV and L-BFGS."""
+"""Oracle backend of hirensi_b200.inversion.FWI (numpy vectors, the CPU
+restatement for assembly, time loops, gradient, TV and L-BFGS), and the oracle
+primitives that drive oracle.inversion_loop, the independent restatement of the
+reference's step and line-search rules."""
 import numpy as np
 
 import oracle as O
@@ -80,3 +82,22 @@ class OracleBackend:
             a, b = O.control(self.om, self.nstep, self.dt, self.mesh.store_eq, h, pk)
             g_l += a
             g_m += b
+
+
+def loop_primitives(be: OracleBackend):
+    """evaluate / gradient / tv callables of oracle.inversion_loop over the oracle's
+    forward, misfit, adjoint, control and TV, plus img, restriction and the
+    extension map of the backend's mesh."""
+    def evaluate(lam, mu):
+        return be.forward(lam, mu)
+
+    def gradient():
+        gl, gm = np.zeros(be.n), np.zeros(be.n)
+        be.gradient(gl, gm)
+        return gl, gm
+
+    def tv(lam, mu):
+        return O.tv_reg(be.om, lam, mu)
+
+    img, restriction = O.inverse_gradient_mass(O.rmg(be.om))
+    return evaluate, gradient, tv, img, restriction, be.mesh.extend_to

@@ -1,5 +1,5 @@
 """Device model update (vector kernels, TV, gradient mass, coupled L-BFGS) and the
-FWI driver on the device against the oracle backend."""
+FWI driver on the device against the oracle's restatement of the inversion loop."""
 import numpy as np
 import pytest
 
@@ -68,7 +68,14 @@ def test_vector_kernels_tv_mass_and_lbfgs(gpu_lib):
     s.close()
 
 
-def test_fwi_iterations_match_oracle_backend(gpu_lib):
+@pytest.mark.parametrize("tv", ["TV", None])
+def test_fwi_iterations_match_the_reference_rules(gpu_lib, tv):
+    """The device driver (device forward, misfit, adjoint gradient, TV, gradient mass,
+    L-BFGS and vector kernels, with hirensi_b200.inversion's control flow) against
+    oracle.inversion_loop, the oracle's own restatement of S4/Program_Main.F90:379-896
+    driven by the CPU forward, adjoint and control: per iteration the step sizes, the
+    Armijo trials, the misfit and the model."""
+    from fwi_oracle import loop_primitives
     p = tiny(nshot=2, nstep=160)
     _, _, hist_t = oracle_forward(p, p["lam_t"], p["mu_t"])
     dis = [traces_from_history(p, h) for h in hist_t]
@@ -77,15 +84,24 @@ def test_fwi_iterations_match_oracle_backend(gpu_lib):
         b = np.zeros(p["mesh"].neq)
         b[p["src_eq"][k]] = 1.0
         shots.append((b, p["ftab"][k]))
-    cfg = InversionConfig(m_lbfgs=5, bounds_lambda=(10.0, 1000.0), bounds_mu=(10.0, 1000.0))
-    ref = FWI(OracleBackend(p["mesh"], shots, p["nstep"], p["dt"], p["eqdis"], p["eqdis_map"], dis), cfg)
-    h_ref = ref.run(p["lam"], p["mu"], n_iter=3)
+    cfg = InversionConfig(m_lbfgs=5, bounds_lambda=(10.0, 1000.0), bounds_mu=(10.0, 1000.0), regularization=tv)
+    be = OracleBackend(p["mesh"], shots, p["nstep"], p["dt"], p["eqdis"], p["eqdis_map"], dis)
+    evaluate, gradient, tvf, img, restriction, extend_to = loop_primitives(be)
+    ref = O.inversion_loop(evaluate, gradient, p["lam"], p["mu"], 3, img, restriction, extend_to, cfg.bounds_lambda,
+                           cfg.bounds_mu, m_lbfgs=cfg.m_lbfgs,
+                           fac_max_update=(cfg.fac_max_update_lambda, cfg.fac_max_update_mu),
+                           tv=tvf if tv else None, reg_factor=cfg.reg_factor, bias_lambda=cfg.bias_lambda,
+                           n_iter_bias=cfg.n_iter_bias, iter_begin=cfg.iter_begin)
     s = _device(p, dis)
     fwi = FWI(DeviceBackend(s, p["mesh"]), cfg)
     h_dev = fwi.run(p["lam"], p["mu"], n_iter=3)
-    assert [h["armijo"] for h in h_dev] == [h["armijo"] for h in h_ref]
-    for a, b in zip(h_dev, h_ref):
+    assert [h["armijo"] for h in h_dev] == [h["armijo"] for h in ref]
+    for a, b in zip(h_dev, ref):
         assert abs(a["misfit"] - b["misfit"]) <= 1e-8 * b["misfit"]
-    assert rel_l2(fwi.lam.cpu().numpy(), ref.lam) < 1e-9
-    assert rel_l2(fwi.mu.cpu().numpy(), ref.mu) < 1e-9
+        if b["iter"] > 0:
+            assert abs(a["alpha_lambda"] - b["alpha_lambda"]) <= 1e-8 * abs(b["alpha_lambda"])
+            assert abs(a["alpha_mu"] - b["alpha_mu"]) <= 1e-8 * abs(b["alpha_mu"])
+    assert ref[-1]["misfit"] < ref[0]["misfit"]
+    assert rel_l2(fwi.lam.cpu().numpy(), ref[-1]["lam"]) < 1e-9
+    assert rel_l2(fwi.mu.cpu().numpy(), ref[-1]["mu"]) < 1e-9
     s.close()

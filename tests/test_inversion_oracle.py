@@ -33,6 +33,27 @@ def test_lbfgs_iterations_reduce_the_misfit(reg):
     assert all(h["armijo"] < 10 for h in hist[1:])
 
 
+@pytest.mark.parametrize("reg", [None, "TV"])
+def test_driver_on_the_oracle_follows_the_oracle_loop(reg):
+    """hirensi_b200.inversion.FWI on the oracle backend and oracle.inversion_loop (the
+    oracle's own restatement of the step and line-search rules) on the same forward
+    problem: the same misfits, step sizes, Armijo trials and models."""
+    from fwi_oracle import loop_primitives
+    p, be = setup()
+    cfg = InversionConfig(m_lbfgs=5, bounds_lambda=(10.0, 1000.0), bounds_mu=(10.0, 1000.0), regularization=reg)
+    fwi = FWI(be, cfg)
+    hist = fwi.run(p["lam"], p["mu"], n_iter=2)
+    _, be2 = setup()
+    evaluate, gradient, tv, img, restriction, extend_to = loop_primitives(be2)
+    ref = O.inversion_loop(evaluate, gradient, p["lam"], p["mu"], 2, img, restriction, extend_to, cfg.bounds_lambda,
+                           cfg.bounds_mu, m_lbfgs=5, tv=tv if reg else None)
+    assert [h["armijo"] for h in hist] == [h["armijo"] for h in ref]
+    for a, b in zip(hist, ref):
+        assert abs(a["misfit"] - b["misfit"]) <= 1e-12 * b["misfit"]
+    assert np.allclose(fwi.lam, ref[-1]["lam"], rtol=1e-12, atol=0)
+    assert np.allclose(fwi.mu, ref[-1]["mu"], rtol=1e-12, atol=0)
+
+
 @pytest.mark.parametrize("memory", [1, 2, 10])
 def test_coupled_lbfgs_terminates_on_a_quadratic_with_exact_steps(memory):
     """Known answer of the two-loop recursion: on a strictly convex quadratic in the
