@@ -33,6 +33,8 @@ SIGNATURES = {
     "hrn_get_operator_csr": (C.c_int, [VP, C.c_int32, PI, PI, PD, PI64]),
     "hrn_get_diag_m": (C.c_int, [VP, PD]),
     "hrn_apply_operator": (C.c_int, [VP, C.c_int32, C.c_int32, PD, PD]),
+    "hrn_assemble_face_force": (C.c_int, [VP, PI, PD]),
+    "hrn_set_shots_face_force": (C.c_int, [VP, C.c_int32, C.c_int32, C.c_double, PD]),
     "hrn_set_history": (C.c_int, [VP, C.c_int32, PI]),
     "hrn_set_shots": (C.c_int, [VP, C.c_int32, C.c_int32, C.c_double, C.c_int32, PI, PD, PD]),
     "hrn_set_receivers": (C.c_int, [VP, C.c_int32, PI, PI]),

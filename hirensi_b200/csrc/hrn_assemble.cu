@@ -527,4 +527,151 @@ int assemble_device(hrn_ctx *c, bool discover_pattern)
     return launch_scale_operator(c);
 }
 
+// ----------------------------------------------------------------------------
+// Face traction: ASSEM_FORCE_PETSC_3D (S4/Assemble_PETSc_3D.F90:444-548) with
+// ELEMENT_FS_3D (S4/Element_Matrices_3D.F90:890-1096).  A unit vertical
+// traction (Tx = Ty = 0, Tz = 1) is integrated over the loaded face of every
+// regular-domain element with the 3-point GLL rule.  Every face point is a GLL
+// node, so the shape functions there are Kronecker deltas: node I at point q
+// receives w_i w_j |dx/dxi_L x dx/dxi_M| of that point alone, in its z entry.
+// DJ(:, L) and DJ(:, M) are summed over the 27 nodes in local order without
+// fused multiply-adds, as MATMUL(XT, DFXI); the normal is the reference's CROSS.
+
+__constant__ double a_gll_w[3];
+
+// One thread per loaded element: efs[k][27] (z entries) and an error flag when a
+// face point is off the surface (|z| > 1e-3), where the reference STOPs.
+__global__ void k_face_force(int nload, const int32_t *__restrict__ elem, const int32_t *__restrict__ face,
+                             const int32_t *__restrict__ inod, const double *__restrict__ xyz, double *__restrict__ efs,
+                             int *__restrict__ err)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= nload) return;
+    const int e = elem[k];
+    int nface = face[k];
+    if (nface == 6) nface = 5;                  // the reference's temporary adjustment (:945-948)
+    const int lface[6] = {2, 2, 3, 3, 1, 1};
+    const int fsign[6] = {1, -1, 1, -1, 1, -1};
+    const int iperm[3] = {2, 3, 1};
+    const int L = lface[nface - 1], M = iperm[L - 1], N = iperm[M - 1];
+    double xt[3][27];
+    for (int i = 0; i < 27; ++i) {
+        const int n = inod[size_t(e) * 27 + i];
+        xt[0][i] = xyz[3 * size_t(n) + 0];
+        xt[1][i] = xyz[3 * size_t(n) + 1];
+        xt[2][i] = xyz[3 * size_t(n) + 2];
+    }
+    double *out = efs + size_t(k) * 27;
+    for (int i = 0; i < 27; ++i) out[i] = 0.0;
+    int idx[3];
+    idx[N - 1] = fsign[nface - 1] > 0 ? 2 : 0;
+    for (int lj = 0; lj < 3; ++lj) {
+        idx[M - 1] = lj;
+        for (int li = 0; li < 3; ++li) {
+            idx[L - 1] = li;
+            const int q = 9 * idx[2] + 3 * idx[1] + idx[0];
+            const double wstar = mul(a_gll_w[li], a_gll_w[lj]);
+            double vr[3], vs[3];
+            for (int d = 0; d < 3; ++d) {
+                double sr = 0.0, ss = 0.0;
+                for (int I = 0; I < 27; ++I) {
+                    sr = add(sr, mul(xt[d][I], dfxi(I, L - 1, q)));
+                    ss = add(ss, mul(xt[d][I], dfxi(I, M - 1, q)));
+                }
+                vr[d] = sr;
+                vs[d] = ss;
+            }
+            const double vn0 = __dsub_rn(mul(vr[1], vs[2]), mul(vr[2], vs[1]));
+            const double vn1 = add(-mul(vr[0], vs[2]), mul(vr[2], vs[0]));
+            const double vn2 = __dsub_rn(mul(vr[0], vs[1]), mul(vr[1], vs[0]));
+            const double nrm = __dsqrt_rn(add(add(add(0.0, mul(vn0, vn0)), mul(vn1, vn1)), mul(vn2, vn2)));
+            const int I = a_node_at[q];
+            if (fabs(xt[2][I]) > 1.e-3) atomicExch(err, 5);
+            out[I] = add(out[I], mul(wstar, nrm));
+        }
+    }
+}
+
+// B of the loaded elements, added per equation in element order (VecSetValues
+// with ADD_VALUES, element by element): b[eq] = sum over its (slot, node) list.
+__global__ void k_face_force_add(int nrow, const int32_t *__restrict__ row_eq, const int32_t *__restrict__ ptr,
+                                 const int32_t *__restrict__ src, const double *__restrict__ efs, double *__restrict__ b)
+{
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= nrow) return;
+    double v = 0.0;
+    for (int t = ptr[r]; t < ptr[r + 1]; ++t) v = add(v, efs[src[t]]);
+    b[row_eq[r]] = v;
+}
+
+int face_force(hrn_ctx *c, const int32_t *nface)
+{
+    if (int rc = upload_asm_tables(c)) return rc;
+    const double w[3] = {0.33333333333333333333, 1.33333333333333333333, 0.33333333333333333333};
+    HRN_CUDA(c, cudaMemcpyToSymbol(a_gll_w, w, sizeof(w)));
+    // loaded regular-domain elements in element order, and per z equation of their
+    // nodes the (slot, local node) contributions in that order
+    std::vector<int32_t> elem, face;
+    for (int e = 0; e < c->nel; ++e) {
+        if (c->h_mtel[e] != 1 || nface[e] == 0) continue;
+        if (nface[e] < 1 || nface[e] > 6) return set_error(c, HRN_EARG, "nface must be 0 (no load) or 1..6");
+        elem.push_back(e);
+        face.push_back(nface[e]);
+    }
+    const int nload = int(elem.size());
+    std::vector<std::vector<int32_t>> per_eq;
+    std::vector<int32_t> eq_of, slot_of_eq(size_t(c->neq), -1);
+    for (int k = 0; k < nload; ++k)
+        for (int i = 0; i < 27; ++i) {
+            const int eq = c->h_id[size_t(c->h_inod[size_t(elem[k]) * 27 + i]) * 9 + 2];
+            if (eq < 0) continue;
+            if (slot_of_eq[eq] < 0) {
+                slot_of_eq[eq] = int(eq_of.size());
+                eq_of.push_back(eq);
+                per_eq.emplace_back();
+            }
+            per_eq[slot_of_eq[eq]].push_back(k * 27 + i);
+        }
+    std::vector<int32_t> ptr(1, 0), src;
+    for (auto &v : per_eq) {
+        src.insert(src.end(), v.begin(), v.end());
+        ptr.push_back(int32_t(src.size()));
+    }
+    HRN_CUDA(c, c->d_face_b.alloc(size_t(c->neq) * 8));
+    HRN_CUDA(c, cudaMemsetAsync(c->d_face_b.p, 0, size_t(c->neq) * 8, c->stream));
+    c->have_face_b = true;
+    if (nload == 0) return 0;
+    DevBuf d_elem, d_face, d_efs, d_eq, d_ptr, d_src, d_err;
+    HRN_CUDA(c, d_elem.alloc(size_t(nload) * 4));
+    HRN_CUDA(c, d_face.alloc(size_t(nload) * 4));
+    HRN_CUDA(c, d_efs.alloc(size_t(nload) * 27 * 8));
+    HRN_CUDA(c, d_eq.alloc(eq_of.size() * 4));
+    HRN_CUDA(c, d_ptr.alloc(ptr.size() * 4));
+    HRN_CUDA(c, d_src.alloc(src.size() * 4));
+    HRN_CUDA(c, d_err.alloc(4));
+    HRN_CUDA(c, cudaMemcpyAsync(d_elem.p, elem.data(), elem.size() * 4, cudaMemcpyHostToDevice, c->stream));
+    HRN_CUDA(c, cudaMemcpyAsync(d_face.p, face.data(), face.size() * 4, cudaMemcpyHostToDevice, c->stream));
+    HRN_CUDA(c, cudaMemcpyAsync(d_eq.p, eq_of.data(), eq_of.size() * 4, cudaMemcpyHostToDevice, c->stream));
+    HRN_CUDA(c, cudaMemcpyAsync(d_ptr.p, ptr.data(), ptr.size() * 4, cudaMemcpyHostToDevice, c->stream));
+    HRN_CUDA(c, cudaMemcpyAsync(d_src.p, src.data(), src.size() * 4, cudaMemcpyHostToDevice, c->stream));
+    HRN_CUDA(c, cudaMemsetAsync(d_err.p, 0, 4, c->stream));
+    k_face_force<<<(nload + 63) / 64, 64, 0, c->stream>>>(nload, d_elem.as<int32_t>(), d_face.as<int32_t>(),
+                                                          c->d_inod.as<int32_t>(), c->d_xyz.as<double>(),
+                                                          d_efs.as<double>(), d_err.as<int>()); ++c->launches;
+    HRN_CUDA(c, cudaGetLastError());
+    const int nrow = int(eq_of.size());
+    k_face_force_add<<<(nrow + 127) / 128, 128, 0, c->stream>>>(nrow, d_eq.as<int32_t>(), d_ptr.as<int32_t>(),
+                                                               d_src.as<int32_t>(), d_efs.as<double>(),
+                                                               c->d_face_b.as<double>()); ++c->launches;
+    HRN_CUDA(c, cudaGetLastError());
+    int err = 0;
+    HRN_CUDA(c, cudaMemcpyAsync(&err, d_err.p, 4, cudaMemcpyDeviceToHost, c->stream));
+    HRN_CUDA(c, cudaStreamSynchronize(c->stream));
+    if (err) {
+        c->have_face_b = false;
+        return set_error(c, HRN_EMESH, "loaded face not on the surface (|z| > 1e-3 at a face point)");
+    }
+    return 0;
+}
+
 }  // namespace hrn

@@ -588,6 +588,40 @@ int hrn_apply_operator(hrn_ctx *c, int32_t which, int32_t adjoint, const double 
     return HRN_OK;
 }
 
+int hrn_assemble_face_force(hrn_ctx *c, const int32_t *nface, double *b)
+{
+    if (!c || !nface) return HRN_EARG;
+    if (!c->have_mesh) return set_error(c, HRN_ESTATE, "no mesh: call hrn_set_mesh first");
+    cudaSetDevice(c->device);
+    if (int rc = face_force(c, nface)) return rc;
+    if (b) {
+        HRN_CUDA(c, cudaMemcpyAsync(b, c->d_face_b.p, size_t(c->neq) * 8, cudaMemcpyDeviceToHost, c->stream));
+        HRN_CUDA(c, cudaStreamSynchronize(c->stream));
+    }
+    return HRN_OK;
+}
+
+int hrn_set_shots_face_force(hrn_ctx *c, int32_t nshot, int32_t nstep, double dt, const double *ftab)
+{
+    if (!c || !ftab) return HRN_EARG;
+    if (!c->have_face_b) return set_error(c, HRN_ESTATE, "no face force: call hrn_assemble_face_force first");
+    if (nshot < 1 || nshot > HRN_MAX_SHOTS) return set_error(c, HRN_EARG, "nshot must be 1..HRN_MAX_SHOTS");
+    cudaSetDevice(c->device);
+    std::vector<double> bvec(size_t(c->neq));
+    HRN_CUDA(c, cudaMemcpyAsync(bvec.data(), c->d_face_b.p, size_t(c->neq) * 8, cudaMemcpyDeviceToHost, c->stream));
+    HRN_CUDA(c, cudaStreamSynchronize(c->stream));
+    // the entries of B that load the system; every shot carries the same B
+    std::vector<int32_t> eq;
+    std::vector<double> vals;
+    for (int32_t i = 0; i < c->neq; ++i)
+        if (bvec[i] != 0.0) {
+            eq.push_back(i);
+            for (int s = 0; s < nshot; ++s) vals.push_back(bvec[i]);
+        }
+    return hrn_set_shots(c, nshot, nstep, dt, int32_t(eq.size()), eq.empty() ? nullptr : eq.data(),
+                         vals.empty() ? nullptr : vals.data(), ftab);
+}
+
 int hrn_get_diag_m(hrn_ctx *c, double *diag_m)
 {
     if (!c || !diag_m) return HRN_EARG;

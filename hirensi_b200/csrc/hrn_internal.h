@@ -159,6 +159,8 @@ struct hrn_ctx {
     hrn::DevBuf d_lam, d_mu;      // nodal material (FP64)
     hrn::DevBuf d_touched;        // pattern discovery flags
     hrn::DevBuf d_asm_err;        // device error flag of the assembly kernels
+    hrn::DevBuf d_face_b;         // [neq] face-traction force vector B (FP64)
+    bool have_face_b = false;
     // matrix-free element operator (variants 90 and 91 of the stage kernels)
     bool op_from_mesh = false;    // the operator was assembled from the current mesh and material
     bool mf_only = false;         // assemble DIAG_M only: the operator is applied matrix-free (no CSR)
@@ -289,6 +291,7 @@ int run_time_stage(hrn_ctx *c, int adj, int nsteps, double *avg_ms);
 int run_pseudo_hessian(hrn_ctx *c, double *hl, double *hm);
 int build_rd_geometry(hrn_ctx *c);
 int assemble_device(hrn_ctx *c, bool discover_pattern);
+int face_force(hrn_ctx *c, const int32_t *nface);
 int finalize_pattern_from_keys(hrn_ctx *c, const std::vector<uint64_t> &keys);
 int vec_reduce(hrn_ctx *c, int kind, int n, const double *x, const double *y, double *out);
 int gt_ready(hrn_ctx *c, int adj);

@@ -39,6 +39,7 @@ class Solver:
         self.nstore = 0
         self.nrec3 = 0
         self.nj = 0
+        self.nel = 0
         self.neq = 0
         self.ckpt_interval = 0
 
@@ -111,6 +112,7 @@ class Solver:
         self._check(self._L.hrn_set_mesh(self.h, mesh.nj, mesh.nel, mesh.neq, dptr(xyz), iptr(inod), iptr(mtel),
                                          iptr(idm), dptr(rho_el), dptr(pml)))
         self.nj = mesh.nj
+        self.nel = mesh.nel
         self.neq = mesh.neq
 
     def set_operator_mode(self, matrix_free: bool):
@@ -176,6 +178,26 @@ class Solver:
         self._check(self._L.hrn_set_shots(self.h, nshot, nstep, float(dt), se.size, iptr(se) if se.size else None,
                                           dptr(np.ascontiguousarray(sb)) if se.size else None, dptr(ft)))
         self.nshot, self.nstep, self.dt = nshot, nstep, dt
+
+    def assemble_face_force(self, nface) -> np.ndarray:
+        """ASSEM_FORCE_PETSC_3D on the device: B [neq] of a unit vertical traction on
+        the loaded face nface[e] = ID_BC(e, 1) (0 = none) of each regular-domain element."""
+        nf = i32(nface)
+        if nf.size != self.nel:
+            raise ValueError("nface must have one entry per element")
+        b = np.zeros(self.neq)
+        self._check(self._L.hrn_assemble_face_force(self.h, iptr(nf), dptr(b)))
+        return b
+
+    def set_shots_face_force(self, nstep: int, dt: float, ftab):
+        """Shots loaded by the device face-force vector, ftab [nshot, nstep+1, 3]."""
+        ft = f64(ftab)
+        if ft.ndim == 2:
+            ft = ft[None]
+        if ft.shape[1:] != (nstep + 1, 3):
+            raise ValueError("ftab must be [nshot, nstep+1, 3]")
+        self._check(self._L.hrn_set_shots_face_force(self.h, ft.shape[0], nstep, float(dt), dptr(ft)))
+        self.nshot, self.nstep, self.dt = ft.shape[0], nstep, dt
 
     def set_receivers(self, eqdis, eqdis_map):
         e, m = i32(eqdis), i32(eqdis_map)

@@ -100,6 +100,20 @@ int hrn_get_diag_m(hrn_ctx *ctx, double *diag_m);
  * operator.  Not available for a matrix-free operator (HRN_ESTATE). */
 int hrn_apply_operator(hrn_ctx *ctx, int32_t which, int32_t adjoint, const double *x, double *y);
 
+/* Face-traction force vector B of ASSEM_FORCE_PETSC_3D (S4/Assemble_PETSc_3D.F90:444-548)
+ * with ELEMENT_FS_3D (S4/Element_Matrices_3D.F90:890-1096), built on the device: a unit
+ * vertical traction (Tx = Ty = 0, Tz = 1) integrated with the 3-point GLL rule over the
+ * loaded face of every regular-domain element.  nface[nel] = ID_BC(IEL, 1): 0 = no load,
+ * 1..6 = the loaded face (6 is taken as 5, as in the reference).  A face point off the
+ * surface (|z| > 1e-3) returns HRN_EMESH, where the reference STOPs.  B stays on the
+ * device for hrn_set_shots_face_force; b [neq] (may be NULL) receives a host copy. */
+int hrn_assemble_face_force(hrn_ctx *ctx, const int32_t *nface, double *b);
+
+/* hrn_set_shots with the device face-force vector of hrn_assemble_face_force as the B of
+ * every shot (the B argument of EXPLICIT_RK4_PETSC_PML_3D, S4/Solve_Forward.F90:117-119),
+ * each scaled by its own TIME_FUNCTION table ftab[nshot][nstep+1][3]. */
+int hrn_set_shots_face_force(hrn_ctx *ctx, int32_t nshot, int32_t nstep, double dt, const double *ftab);
+
 /* ---- problem description --------------------------------------------------- */
 
 /* History equations U_Store_Numbers_Global (S3/PIC_Inversion_Data_Structure.F90:255-300). */
