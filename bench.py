@@ -49,7 +49,12 @@ def parse_args():
     ap.add_argument("--no-fp32", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fwi", action="store_true", help="skip the FWI time-to-misfit leg")
-    ap.add_argument("--fwi-iters", type=int, default=10)
+    ap.add_argument("--fwi-iters", type=int, default=40,
+                    help="iteration cap of each FWI time-to-misfit leg")
+    ap.add_argument("--fwi-target", type=float, default=0.5,
+                    help="FWI legs stop once the misfit has fallen by this fraction")
+    ap.add_argument("--fwi-fac", type=float, default=20.0,
+                    help="Fac_Max_Update (largest model change per iteration) of the FWI legs")
     ap.add_argument("--profile-precision", choices=["fp64", "fp32"], default="fp64",
                     help="stepping precision of the --profile-case run")
     ap.add_argument("--variant", type=int, default=0,
@@ -64,6 +69,11 @@ def parse_args():
     ap.add_argument("--max-batches", type=int, default=0, help="uneven / xl: time at most this many batches")
     ap.add_argument("--length-scale", type=float, default=0.03,
                     help="uneven workload: record lengths scaled by this factor (a bounded sample)")
+    ap.add_argument("--no-batched", action="store_true",
+                    help="skip the batched FP32 leg (one full-length batch of 8 uneven shots on the "
+                         "80x80x40 + PML 4 mesh) of the default run")
+    ap.add_argument("--xl-error-steps", type=int, default=120,
+                    help="xl workload: steps of the FP32-against-FP64 error check (2 shots); 0 skips it")
     ap.add_argument("--inflight", type=int, default=2,
                     help="uneven workload: batches in flight at once, each on its own context and stream")
     return ap.parse_args()
@@ -358,20 +368,108 @@ def run_native(args, rank, world, local_rank):
             cb.pop("seconds", None)
             result["cpu_baseline"] = cb
         if not args.no_fwi and world == 1:
-            result["fwi"] = {}
-            for prec in (["fp64"] if args.no_fp32 else ["fp64", "fp32"]):
-                result["fwi"][prec] = fwi_leg(prec, prob, dis, local_rank, args.fwi_iters, variant=tuned.get(prec))
+            # time to a stated misfit reduction, each leg from the initial model
+            result["fwi"] = {"target_reduction": args.fwi_target, "iteration_cap": args.fwi_iters,
+                             "fac_max_update": args.fwi_fac}
+            legs = [("fp64", False)] if args.no_fp32 else [("fp64", False), ("fp32", False)]
             if not args.no_fp32 and os.path.exists(PRECOND_WEIGHTS):
-                # time for FP32 stepping + the learned preconditioner to reach the
-                # misfit reduction of the plain FP64 run
-                r64 = result["fwi"]["fp64"]["misfit_reduction"]
-                fl = fwi_leg("fp32", prob, dis, local_rank, args.fwi_iters, learned=True, target=r64,
-                             variant=tuned.get("fp32"))
-                result["fwi"]["fp32_learned"] = fl
-                if fl["reached_target"]:
-                    result["fwi"]["time_to_fp64_misfit_speedup"] = result["fwi"]["fp64"]["wall_s"] / fl["wall_s"]
+                legs.append(("fp32", True))
+            for prec, learned in legs:
+                name = prec + ("_learned" if learned else "")
+                result["fwi"][name] = fwi_leg(prec, prob, dis, local_rank, args.fwi_iters, learned=learned,
+                                              target=args.fwi_target, variant=tuned.get(prec), fac=args.fwi_fac)
+            f64, fl = result["fwi"]["fp64"], result["fwi"].get("fp32_learned")
+            if fl and f64["reached_target"] and fl["reached_target"]:
+                result["fwi"]["time_to_target_speedup_fp32_learned_vs_fp64"] = f64["wall_s"] / fl["wall_s"]
+            f32 = result["fwi"].get("fp32")
+            if f32 and f64["reached_target"] and f32["reached_target"]:
+                result["fwi"]["time_to_target_speedup_fp32_vs_fp64"] = f64["wall_s"] / f32["wall_s"]
     s64.close()
+    if not args.profile_case and not args.no_batched and world == 1:
+        result["batched_fp32"] = batched_leg(args, local_rank)
     return result
+
+
+def batched_leg(args, local_rank):
+    """One batch of the batched uneven-shot workload at full record length: 8 shots of
+    the 64-shot plan on the 80x80x40 + PML 4 mesh (12.7 M equations), the batch with the
+    shortest records (1500-2000 steps), FP32 stepping with FP64 reductions, forward with
+    checkpoints every 100 steps, misfit, adjoint with recomputed segments and the fused
+    gradient.  Warmed up on the same batch with its records scaled to 3 % (tuning,
+    tables), then timed once with CUDA events.  Counts each shot's own steps."""
+    import torch
+    from hirensi_b200 import batching as B
+    from hirensi_b200.configs import uneven_config
+    from hirensi_b200.solver import Solver
+    dev = torch.device("cuda", local_rank)
+    t_setup = time.perf_counter()
+    full = uneven_config(length_scale=1.0)
+    short = uneven_config(length_scale=0.03)
+    m = full.mesh
+    lengths = [sh.nstep for sh in full.shots]
+    ids = B.plan(lengths, 8)[-1]
+    sv = Solver("fp32", device=local_rank)
+    sv.set_graphs(False)   # launches are hidden behind millisecond stages; no capture in the timed batch
+    sv.set_mesh(m, full.rho_el)
+    sv.assemble(full.lam, full.mu)
+    sv.set_history(m.store_eq)
+    sv.set_checkpointing(100)
+
+    def run(prob):
+        b = B.pack(prob.shots, ids)
+        B.configure(sv, b, prob.dt, m.store_position)
+        sv.set_data(np.zeros((len(ids), len(b.eqdis), b.nstep + 1)))
+        sv.forward()
+        J = sv.misfit(None)
+        sv.adjoint_gradient(None, to_host=False)
+        return b, J
+
+    run(short)
+    b, _ = run(short)
+    torch.cuda.synchronize(dev)
+    setup_s = time.perf_counter() - t_setup
+    # the full-length batch: its buffers (checkpoints, traces, source tables) are
+    # allocated by the calls themselves, so the time is the device time the library
+    # measures with CUDA events around each time loop (forward, adjoint), plus the misfit
+    clk = ClockSampler(local_rank)
+    clk.start()
+    l0 = sv.launch_count()
+    b = B.pack(full.shots, ids)
+    B.configure(sv, b, full.dt, m.store_position)
+    sv.set_data(np.zeros((len(ids), len(b.eqdis), b.nstep + 1)))
+    sv.forward()
+    t_fwd = sv.last_timing()[0]
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    sv.misfit(None)
+    e1.record()
+    torch.cuda.synchronize(dev)
+    t_mis = e0.elapsed_time(e1)
+    sv.adjoint_gradient(None, to_host=False)
+    t_adj = sv.last_timing()[0]
+    torch.cuda.synchronize(dev)
+    ms = t_fwd + t_mis + t_adj
+    clocks = clk.stop()
+    launches = sv.launch_count() - l0
+    units = sum(full.dof * (2 * lengths[i] + 1) for i in ids)
+    st_f = sv.time_stage(adjoint=False, nsteps=20)
+    st_a = sv.time_stage(adjoint=True, nsteps=20)
+    nnz = [sv.operator_nnz(w) for w in range(3)]
+    bytes_launch = stage_bytes(sum(nnz), m.neq, len(ids), 4)
+    peak, peak_kind = measured_peaks()
+    st = 0.5 * (st_f + st_a)
+    out = {"value": units / (ms * 1e-3) / 1e9, "unit": UNIT, "ms": ms, "ms_forward_misfit_adjoint": [t_fwd, t_mis, t_adj],
+           "dtype": "f32 stepping, f64 reductions",
+           "workload": full.name, "shots_in_batch": len(ids), "record_lengths": [lengths[i] for i in ids],
+           "receivers_per_shot": [len(full.shots[i].eqdis) // 3 for i in ids], "checkpoint_interval": 100,
+           "equations": m.neq, "dof": full.dof, "nnz_CKG": nnz, "stage_variant_fwd_adj": list(sv.variant()),
+           "gpu_launches": int(launches), "setup_s": setup_s, "clocks": clocks,
+           "roofline": {"bound": "hbm", "achieved": bytes_launch / (st * 1e-3) / 1e9, "peak": peak,
+                        "peak_kind": peak_kind, "unit": "GB/s", "frac": bytes_launch / (st * 1e-3) / 1e9 / peak,
+                        "bytes_per_launch": bytes_launch, "avg_launch_us_fwd_adj": [st_f * 1e3, st_a * 1e3]},
+           "step": "forward (checkpoints every 100 steps) + misfit + adjoint with recomputed segments and gradient"}
+    sv.close()
+    return out
 
 
 PRECOND_WEIGHTS = os.path.join(ROOT, "hirensi_b200", "data", "precond_cnn6_16x16x8.npz")
@@ -536,15 +634,55 @@ def run_uneven(args, rank, world, local_rank):
               "clocks": clocks}
     for sv in solvers:
         sv.close()
+    if args.workload == "xl" and args.xl_error_steps > 0:
+        result["fp32_error_vs_fp64"] = xl_error(prob, args.xl_error_steps, local_rank)
     return result
 
 
-def fwi_leg(precision, prob, dis, local_rank, iters, learned=False, target=None, variant=None):
-    """Wall time of `iters` L-BFGS iterations (memory 5) of the inversion loop from
-    the initial model, all vectors on the device; misfit reduction reached.  With
-    `learned`, each iteration first tries the trained CNN's scaled direction, and the
-    run stops once the misfit reduction reaches `target`.  `variant` = the (forward,
-    adjoint) stage variants tuned earlier on the same operator, reused here."""
+def xl_error(prob, nsteps, local_rank):
+    """Seismogram and gradient error of FP32 stepping against FP64 stepping on the
+    extra-large mesh (matrix-free operator): the first two shots of the workload, their
+    records cut to `nsteps` steps, zero measured data (the residuals are the synthetics
+    themselves), checkpoints every nsteps / 3 steps; relative L2 over all traces and
+    over the whole gradient."""
+    from hirensi_b200 import batching as B
+    from hirensi_b200.solver import Solver
+    m = prob.mesh
+    shots = [B.Shot(sh.src_eq, sh.src_b, sh.ftab[: nsteps + 1], sh.eqdis) for sh in prob.shots[:2]]
+    b = B.pack(shots, [0, 1])
+    out = {}
+    for prec in ("fp32", "fp64"):
+        sv = Solver(prec, device=local_rank)
+        sv.set_mesh(m, prob.rho_el)
+        sv.set_operator_mode(True)
+        sv.assemble(prob.lam, prob.mu)
+        sv.set_history(m.store_eq)
+        sv.set_checkpointing(max(1, nsteps // 3))
+        B.configure(sv, b, prob.dt, m.store_position)
+        sv.set_data(np.zeros((2, len(b.eqdis), b.nstep + 1)))
+        sv.forward()
+        tr = sv.traces()
+        J = sv.misfit(None)
+        gl, gm = sv.adjoint_gradient(None)
+        out[prec] = (tr, J, gl, gm, list(sv.variant()))
+        sv.close()
+
+    def rel(a, b_):
+        return float(np.linalg.norm(a - b_) / np.linalg.norm(b_))
+    t32, J32, l32, m32, v32 = out["fp32"]
+    t64, J64, l64, m64, v64 = out["fp64"]
+    return {"shots": 2, "steps": nsteps, "receivers_per_shot": [len(sh.eqdis) // 3 for sh in shots],
+            "seismogram_rel_l2": rel(t32, t64), "misfit_rel": abs(J32 - J64) / J64,
+            "gradient_lambda_rel_l2": rel(l32, l64), "gradient_mu_rel_l2": rel(m32, m64),
+            "variants_fp32_fp64": [v32, v64]}
+
+
+def fwi_leg(precision, prob, dis, local_rank, iters, learned=False, target=None, variant=None, fac=5.0):
+    """Wall time of the inversion loop (L-BFGS memory 5, TV, the reference's step rules)
+    from the initial model until the misfit has fallen by `target` or `iters` iterations
+    have run, all vectors on the device; misfit reduction and model error reached.  With
+    `learned`, each iteration first tries the trained CNN's scaled direction.  `variant` =
+    the (forward, adjoint) stage variants tuned earlier on the same operator."""
     import torch
     from hirensi_b200.configs import RHO
     from hirensi_b200.inversion import FWI, DeviceBackend, InversionConfig
@@ -559,7 +697,8 @@ def fwi_leg(precision, prob, dis, local_rank, iters, learned=False, target=None,
     s.set_data(dis)
     if variant:
         s.set_variant(*variant)
-    cfg = InversionConfig(m_lbfgs=5, bounds_lambda=(10.0, 2000.0), bounds_mu=(10.0, 1000.0))
+    cfg = InversionConfig(m_lbfgs=5, bounds_lambda=(10.0, 2000.0), bounds_mu=(10.0, 1000.0),
+                          fac_max_update_lambda=fac, fac_max_update_mu=fac)
     backend = DeviceBackend(s, m)
     pre = None
     if learned:
@@ -571,23 +710,40 @@ def fwi_leg(precision, prob, dis, local_rank, iters, learned=False, target=None,
     FWI(backend, cfg, preconditioner=pre).run(prob.lam0, prob.mu0, n_iter=1)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    hist = FWI(backend, cfg, preconditioner=pre).run(prob.lam0, prob.mu0, n_iter=iters, target_reduction=target)
+    fwi = FWI(backend, cfg, preconditioner=pre)
+    failed = None
+    try:
+        hist = fwi.run(prob.lam0, prob.mu0, n_iter=iters, target_reduction=target)
+    except RuntimeError as exc:      # ArmijoFailure: the reference would STOP here
+        hist, failed = fwi.hist, str(exc)
     torch.cuda.synchronize()
     wall = time.perf_counter() - t0
     J0, J = hist[0]["misfit"], hist[-1]["misfit"]
-    t_half = next((h["wall_s"] for h in hist if h["misfit"] <= 0.5 * J0), None)
+    rd = m.node_mat_id == 0
+    err = {}
+    if failed is None:
+        mu_f = fwi.mu.cpu().numpy()
+        vs = np.sqrt(np.maximum(mu_f, 0.0) / RHO)
+        vs_t, vs_0 = np.sqrt(prob.mu_true / RHO), np.sqrt(prob.mu0 / RHO)
+        err = {"vs_rel_l2_error": float(np.linalg.norm((vs - vs_t)[rd]) / np.linalg.norm(vs_t[rd])),
+               "vs_rel_l2_error_initial": float(np.linalg.norm((vs_0 - vs_t)[rd]) / np.linalg.norm(vs_t[rd]))}
+    t_target = next((h["wall_s"] for h in hist if target is not None and h["misfit"] <= (1.0 - target) * J0), None)
     s.close()
-    out = {"iterations": len(hist) - 1, "wall_s": wall, "misfit_initial": J0, "misfit_final": J,
-           "misfit_reduction": 1.0 - J / J0, "time_to_50pct_reduction_s": t_half,
+    out = {"iterations": len(hist) - 1, "wall_s": wall, "time_to_target_s": t_target,
+           "misfit_initial": J0, "misfit_final": J, "misfit_reduction": 1.0 - J / J0,
+           "misfit_history": [h["misfit"] for h in hist],
            "forward_solves": sum(1 + h["armijo"] + (1 if h.get("learned") is False else 0) for h in hist[1:]) + 1,
-           "config": "L-BFGS memory 5, TV regularization, reference step rules, bounds lambda [10,2000] mu [10,1000]",
-           "warmup": "one inversion iteration (tables, buffers, captured time loops) before the timed inversion"}
+           "config": f"L-BFGS memory 5, TV regularization, reference step rules, Fac_Max_Update {fac}, "
+                     "bounds lambda [10,2000] mu [10,1000]",
+           "warmup": "one inversion iteration (tables, buffers, captured time loops) before the timed inversion", **err}
+    if failed:
+        out["armijo_failure"] = failed
     if learned:
         out["learned_steps_accepted"] = int(sum(1 for h in hist[1:] if h.get("learned")))
         out["weights"] = os.path.relpath(PRECOND_WEIGHTS, ROOT)
     if target is not None:
         out["target_reduction"] = target
-        out["reached_target"] = bool(1.0 - J / J0 >= target)
+        out["reached_target"] = bool(failed is None and 1.0 - J / J0 >= target)
     return out
 
 

@@ -1,146 +1,449 @@
-// hrn_cnn.cu -- 3-D convolution layers of the learned gradient preconditioner:
-// 3x3x3 kernels with zero padding on a [channel][z][y][x] grid, BF16 weights
-// and activations, FP32 accumulation; forward, data gradient and weight / bias
-// gradient (deterministic reductions).  At most 16 input and 16 output channels.
+// hrn_cnn.cu -- 3-D convolution layers of the learned gradient preconditioner on
+// the 5th-generation tensor cores: 3x3x3 kernels with zero padding, BF16 operands,
+// FP32 accumulation in tensor memory (TMEM), at most 16 input and 16 output
+// channels.  Activations are channels-last with a channel stride of 16: voxel v
+// holds channels 0..15 in 32 contiguous bytes.
+//
+// Each layer is an implicit GEMM over the 27 kernel taps:
+//   forward      y[v][co]  = b[co] + sum_tap sum_ci x[v + off(tap)][ci] w[co][ci][tap]
+//                D (128 voxels x 16 co) += A_tap (128 x 16 ci) B_tap (16 ci x 16 co)
+//   data grad.   gx[v][ci] = sum_tap sum_co gz[v - off(tap)][co] w[co][ci][tap]
+//                the same kernel with the neighbour offset negated and B_tap transposed
+//   weight grad. gw[co][ci][tap] = sum_v x[v + off(tap)][ci] gz[v][co]
+//                D ((8 taps x 16 ci) x 16 co) += A (128 x 16 voxels) B (16 voxels x 16 co),
+//                voxel chunks in parallel, partial sums added in a fixed order.
+// gz = gy masked by the ReLU of y and rounded to BF16 (the tensor-core operand).
+//
+// One elected thread issues tcgen05.mma (kind::f16, M = 128, N = 16, K = 16) on
+// operands staged in shared memory in the canonical no-swizzle core-matrix layout
+// (8 rows x 16 bytes per core matrix), commits to an mbarrier, and the CTA reads
+// the accumulator back with tcgen05.ld.  Every wait is bounded: on a timeout the
+// kernel flags an error, waits (bounded) once more and frees its TMEM.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
+
+#include <atomic>
+#include <mutex>
 
 #include "../../include/hirensi_b200.h"
 
 namespace {
 
-constexpr int kMaxC = 16;
+constexpr int kC = 16;            // channel stride of the activations (and the padded GEMM K and N)
+constexpr int kM = 128;           // voxels per tile (MMA M)
+constexpr int kTapsRound = 9;     // taps staged per round of the forward / data-gradient kernel
+constexpr int kThreads = 128;     // one warpgroup: warp w reads TMEM lanes 32w..32w+31
+constexpr int kTmemCols = 32;     // smallest TMEM allocation; the accumulator uses 16 columns
+constexpr int kWgSteps = 8;       // K steps (16 voxels each) staged per round of the weight-gradient kernel
+constexpr int kWgChunk = 1024;    // voxels of one weight-gradient CTA
 
 struct Grid {
     int nz, ny, nx;
-    __device__ __forceinline__ int size() const { return nz * ny * nx; }
+    __host__ __device__ int size() const { return nz * ny * nx; }
 };
 
-// offset of kernel tap k = 9 dz + 3 dy + dx (each in 0..2) from voxel (z, y, x); -1 if outside
-__device__ __forceinline__ int tap(const Grid &g, int z, int y, int x, int k, int sign)
+// voxel index of the neighbour of v at tap k (9 dz + 3 dy + dx, each 0..2), offset
+// multiplied by sign; -1 outside the grid
+__device__ __forceinline__ int neighbour(const Grid &g, int v, int k, int sign)
 {
+    const int x = v % g.nx, y = (v / g.nx) % g.ny, z = v / (g.nx * g.ny);
     const int zz = z + sign * (k / 9 - 1), yy = y + sign * ((k / 3) % 3 - 1), xx = x + sign * (k % 3 - 1);
     if (zz < 0 || zz >= g.nz || yy < 0 || yy >= g.ny || xx < 0 || xx >= g.nx) return -1;
     return (zz * g.ny + yy) * g.nx + xx;
 }
 
-// y[co][v] = act(b[co] + sum_ci sum_k w[co][ci][k] x[ci][v + off(k)])
-__global__ void k_conv_fwd(int cin, int cout, Grid g, const __nv_bfloat16 *__restrict__ x,
-                           const __nv_bfloat16 *__restrict__ w, const float *__restrict__ b, int relu,
-                           __nv_bfloat16 *__restrict__ y)
+__device__ __forceinline__ uint32_t smem_u32(const void *p) { return uint32_t(__cvta_generic_to_shared(p)); }
+
+// Shared-memory matrix descriptor, no swizzle: start address, leading-dimension
+// byte offset (between core matrices along K for K-major operands, along K groups
+// for MN-major ones), stride byte offset (between 8-row groups), version 1.
+__device__ __forceinline__ uint64_t smem_desc(const void *p, uint32_t lbo, uint32_t sbo)
 {
-    __shared__ float ws[kMaxC * kMaxC * 27];
-    for (int i = threadIdx.x; i < cout * cin * 27; i += blockDim.x) ws[i] = __bfloat162float(w[i]);
-    __syncthreads();
+    uint64_t d = uint64_t((smem_u32(p) >> 4) & 0x3FFFu);
+    d |= uint64_t((lbo >> 4) & 0x3FFFu) << 16;
+    d |= uint64_t((sbo >> 4) & 0x3FFFu) << 32;
+    d |= uint64_t(1) << 46;
+    return d;
+}
+
+// Instruction descriptor of kind::f16: BF16 A and B, FP32 D, M x N, operand majors.
+constexpr uint32_t instr_desc(int M, int N, int a_mn_major, int b_mn_major)
+{
+    return (1u << 4) | (1u << 7) | (1u << 10) | (uint32_t(a_mn_major) << 15) | (uint32_t(b_mn_major) << 16) |
+           (uint32_t(N >> 3) << 17) | (uint32_t(M >> 4) << 24);
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bar)) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+// bounded wait for the phase with the given parity; false on timeout
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity)
+{
+    const uint32_t addr = smem_u32(bar);
+    for (int i = 0; i < (1 << 20); ++i) {
+        uint32_t done;
+        asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+                     : "=r"(done) : "r"(addr), "r"(parity) : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+__device__ __forceinline__ void tmem_alloc(uint32_t *dst)   // whole warp
+{
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(dst)), "r"(kTmemCols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+}
+
+__device__ __forceinline__ void tmem_dealloc(uint32_t taddr)   // whole warp
+{
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(kTmemCols) : "memory");
+}
+
+__device__ __forceinline__ void fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+// generic-proxy shared-memory writes become visible to the tensor core (async proxy)
+__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+__device__ __forceinline__ void mma_bf16(uint32_t taddr, uint64_t adesc, uint64_t bdesc, uint32_t idesc, int accumulate)
+{
+    asm volatile("{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+                 " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}"
+                 ::"r"(taddr), "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate) : "memory");
+}
+
+__device__ __forceinline__ void mma_commit(uint64_t *bar)
+{
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+                 : "memory");
+}
+
+// 16 FP32 accumulator columns of this thread's TMEM lane (warp w: lanes 32w..32w+31)
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&o)[16])
+{
+    uint32_t r[16];
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+                   "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+                 : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 16; ++i) o[i] = __uint_as_float(r[i]);
+}
+
+__device__ __forceinline__ uint32_t pack2(float a, float b)
+{
+    const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
+    return *reinterpret_cast<const uint32_t *>(&h);
+}
+
+// Eight channels (one 16-byte core-matrix row) of the A operand at voxel u:
+// the activations (forward) or gz = gy masked by ReLU(y), rounded to BF16 (data gradient).
+template <bool GRAD>
+__device__ __forceinline__ uint4 channels8(const void *src, const __nv_bfloat16 *y, int relu, int u, int half)
+{
+    if (u < 0) return make_uint4(0, 0, 0, 0);
+    if constexpr (!GRAD) {
+        return __ldg(reinterpret_cast<const uint4 *>(static_cast<const __nv_bfloat16 *>(src) + size_t(u) * kC) + half);
+    } else {
+        const float4 *g = reinterpret_cast<const float4 *>(static_cast<const float *>(src) + size_t(u) * kC + 8 * half);
+        const float4 a = __ldg(g), b = __ldg(g + 1);
+        float f[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+        if (relu) {
+            const uint4 yy = __ldg(reinterpret_cast<const uint4 *>(y + size_t(u) * kC) + half);
+            const __nv_bfloat16 *yh = reinterpret_cast<const __nv_bfloat16 *>(&yy);
+#pragma unroll
+            for (int i = 0; i < 8; ++i)
+                if (!(__bfloat162float(yh[i]) > 0.f)) f[i] = 0.f;
+        }
+        return make_uint4(pack2(f[0], f[1]), pack2(f[2], f[3]), pack2(f[4], f[5]), pack2(f[6], f[7]));
+    }
+}
+
+// Forward (GRAD = false) and data gradient (GRAD = true) of one 128-voxel tile.
+//   forward: src = x (BF16 [V][16]), B_tap[n = co][k = ci] = w[co][ci][tap], out = y (BF16 [V][16]);
+//   data gradient: src = gy (FP32 [V][16]) masked by y, B_tap[n = ci][k = co] = w[co][ci][tap],
+//   neighbour offset negated, out = gx (FP32 [V][16]).
+// Shared memory: B for all taps (27 x 512 B), A for the taps of one round (9 x 4 KB).
+template <bool GRAD>
+__global__ void __launch_bounds__(kThreads) k_conv_tc(int cin, int cout, Grid g, const void *__restrict__ src,
+                                                      const __nv_bfloat16 *__restrict__ y_act,
+                                                      const __nv_bfloat16 *__restrict__ w,
+                                                      const float *__restrict__ bias, int relu, void *__restrict__ out,
+                                                      int *__restrict__ err)
+{
+    extern __shared__ __align__(1024) unsigned char smem[];
+    unsigned char *Bs = smem;                         // 27 x 512
+    unsigned char *As = smem + 27 * 512;              // 9 x 4096
+    uint64_t *bar = reinterpret_cast<uint64_t *>(As + kTapsRound * 4096);
+    uint32_t *s_taddr = reinterpret_cast<uint32_t *>(bar + 1);
     const int V = g.size();
-    const int v = blockIdx.x * blockDim.x + threadIdx.x;
-    if (v >= V) return;
-    const int xx = v % g.nx, yy = (v / g.nx) % g.ny, zz = v / (g.nx * g.ny);
-    float acc[kMaxC];
+    const int v0 = blockIdx.x * kM;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int nrow = GRAD ? cin : cout, ncol = GRAD ? cout : cin;   // B rows (N) and columns (K)
+
+    // B operand of every tap: core matrix (n / 8, k / 8) at ((n / 8) * 2 + k / 8) * 128, row n % 8
+    for (int i = threadIdx.x; i < 27 * kC * kC; i += kThreads) {
+        const int tap = i / (kC * kC), n = (i / kC) % kC, k = i % kC;
+        float val = 0.f;
+        if (n < nrow && k < ncol) {
+            const int co = GRAD ? k : n, ci = GRAD ? n : k;
+            val = __bfloat162float(w[(size_t(co) * cin + ci) * 27 + tap]);
+        }
+        *reinterpret_cast<__nv_bfloat16 *>(Bs + tap * 512 + ((n >> 3) * 2 + (k >> 3)) * 128 + (n & 7) * 16 + (k & 7) * 2) =
+            __float2bfloat16_rn(val);
+    }
+    if (threadIdx.x == 0) mbar_init(bar);
+    if (warp == 0) tmem_alloc(s_taddr);
+    fence_before();
+    __syncthreads();
+    fence_after();
+    const uint32_t taddr = *s_taddr;
+    constexpr uint32_t idesc = instr_desc(kM, kC, 0, 0);
+    bool ok = true;
+    int issued = 0;
+    for (int r = 0; r < 27 / kTapsRound && ok; ++r) {
+        // A operand of the round's taps: voxel m, channels 8h..8h+7 -> core (m / 8, h), row m % 8
+        for (int i = threadIdx.x; i < kTapsRound * kM * 2; i += kThreads) {
+            const int t = i / (kM * 2), m = (i >> 1) % kM, h = i & 1;
+            const int v = v0 + m;
+            const int u = v < V ? neighbour(g, v, r * kTapsRound + t, GRAD ? -1 : 1) : -1;
+            *reinterpret_cast<uint4 *>(As + t * 4096 + ((m >> 3) * 2 + h) * 128 + (m & 7) * 16) =
+                channels8<GRAD>(src, y_act, relu, u, h);
+        }
+        fence_async_smem();
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            fence_after();
+            for (int t = 0; t < kTapsRound; ++t)
+                mma_bf16(taddr, smem_desc(As + t * 4096, 128, 256), smem_desc(Bs + (r * kTapsRound + t) * 512, 128, 256),
+                         idesc, (r | t) != 0);
+            mma_commit(bar);
+        }
+        ++issued;
+        ok = mbar_wait(bar, uint32_t(r & 1));   // the MMAs read A before the next round overwrites it
+        ok = __syncthreads_and(ok);
+    }
+    if (!ok) {
+        if (threadIdx.x == 0) {
+            atomicExch(err, 1);
+            mbar_wait(bar, uint32_t((issued - 1) & 1));
+        }
+    } else {
+        fence_after();
+        float acc[16];
+        tmem_ld16(taddr + (uint32_t(32 * warp) << 16), acc);
+        const int v = v0 + 32 * warp + lane;
+        if (v < V) {
+            if constexpr (!GRAD) {
+                uint32_t o[8];
 #pragma unroll
-    for (int co = 0; co < kMaxC; ++co) acc[co] = co < cout ? b[co] : 0.f;
-    for (int k = 0; k < 27; ++k) {
-        const int u = tap(g, zz, yy, xx, k, 1);
-        if (u < 0) continue;
-        for (int ci = 0; ci < cin; ++ci) {
-            const float xv = __bfloat162float(x[size_t(ci) * V + u]);
+                for (int c = 0; c < 16; c += 2) {
+                    float a = c < cout ? acc[c] + bias[c] : 0.f, b = c + 1 < cout ? acc[c + 1] + bias[c + 1] : 0.f;
+                    if (relu) { a = fmaxf(a, 0.f); b = fmaxf(b, 0.f); }
+                    o[c / 2] = pack2(a, b);
+                }
+                uint4 *dst = reinterpret_cast<uint4 *>(static_cast<__nv_bfloat16 *>(out) + size_t(v) * kC);
+                dst[0] = make_uint4(o[0], o[1], o[2], o[3]);
+                dst[1] = make_uint4(o[4], o[5], o[6], o[7]);
+            } else {
+                float4 *dst = reinterpret_cast<float4 *>(static_cast<float *>(out) + size_t(v) * kC);
 #pragma unroll
-            for (int co = 0; co < kMaxC; ++co)
-                if (co < cout) acc[co] = fmaf(ws[(co * cin + ci) * 27 + k], xv, acc[co]);
+                for (int c = 0; c < 16; c += 4)
+                    dst[c / 4] = make_float4(c < cin ? acc[c] : 0.f, c + 1 < cin ? acc[c + 1] : 0.f,
+                                             c + 2 < cin ? acc[c + 2] : 0.f, c + 3 < cin ? acc[c + 3] : 0.f);
+            }
         }
     }
-    for (int co = 0; co < cout; ++co) {
-        const float a = relu ? fmaxf(acc[co], 0.f) : acc[co];
-        y[size_t(co) * V + v] = __float2bfloat16_rn(a);
-    }
-}
-
-// gradient at the pre-activation: gy masked by the activation's derivative
-__device__ __forceinline__ float gz_at(const float *__restrict__ gy, const __nv_bfloat16 *__restrict__ y, int relu, size_t i)
-{
-    const float g = gy[i];
-    if (!relu) return g;
-    return __bfloat162float(y[i]) > 0.f ? g : 0.f;
-}
-
-// gx[ci][v] = sum_co sum_k w[co][ci][k] gz[co][v - off(k)]
-__global__ void k_conv_bwd_data(int cin, int cout, Grid g, const __nv_bfloat16 *__restrict__ w,
-                                const __nv_bfloat16 *__restrict__ y, int relu, const float *__restrict__ gy,
-                                float *__restrict__ gx)
-{
-    __shared__ float ws[kMaxC * kMaxC * 27];
-    for (int i = threadIdx.x; i < cout * cin * 27; i += blockDim.x) ws[i] = __bfloat162float(w[i]);
+    fence_before();
     __syncthreads();
-    const int V = g.size();
-    const int v = blockIdx.x * blockDim.x + threadIdx.x;
-    if (v >= V) return;
-    const int xx = v % g.nx, yy = (v / g.nx) % g.ny, zz = v / (g.nx * g.ny);
-    float acc[kMaxC];
-#pragma unroll
-    for (int ci = 0; ci < kMaxC; ++ci) acc[ci] = 0.f;
-    for (int k = 0; k < 27; ++k) {
-        const int u = tap(g, zz, yy, xx, k, -1);
-        if (u < 0) continue;
-        for (int co = 0; co < cout; ++co) {
-            const float gz = gz_at(gy, y, relu, size_t(co) * V + u);
-#pragma unroll
-            for (int ci = 0; ci < kMaxC; ++ci)
-                if (ci < cin) acc[ci] = fmaf(ws[(co * cin + ci) * 27 + k], gz, acc[ci]);
-        }
-    }
-    for (int ci = 0; ci < cin; ++ci) gx[size_t(ci) * V + v] = acc[ci];
+    if (warp == 0) tmem_dealloc(taddr);
 }
 
-// one block per (co, ci): gw[co][ci][k] = sum_v gz[co][v] x[ci][v + off(k)];
-// the ci = 0 block also writes gb[co] = sum_v gz[co][v]
-constexpr int kWThreads = 256;
-
-__global__ void __launch_bounds__(kWThreads) k_conv_bwd_weight(int cin, int cout, Grid g, const __nv_bfloat16 *__restrict__ x,
-                                                               const __nv_bfloat16 *__restrict__ y, int relu,
-                                                               const float *__restrict__ gy, float *__restrict__ gw,
-                                                               float *__restrict__ gb)
+// Weight gradient, partial sums of one chunk of voxels for one M tile of 8 taps:
+//   part[chunk][mt * 128 + (tap - 8 mt) * 16 + ci][co] = sum_v x[v + off(tap)][ci] gz[v][co]
+// Both operands are MN-major (the GEMM's K runs over voxels): core matrix
+// (8 M or N elements) x (8 voxels), row = voxel, at (group * 2 + voxel / 8) * 128.
+__global__ void __launch_bounds__(kThreads) k_conv_wgrad_tc(Grid g, const __nv_bfloat16 *__restrict__ x,
+                                                            const float *__restrict__ gy,
+                                                            const __nv_bfloat16 *__restrict__ y_act, int relu,
+                                                            float *__restrict__ part, int *__restrict__ err)
 {
-    const int co = blockIdx.x / cin, ci = blockIdx.x % cin;
+    extern __shared__ __align__(1024) unsigned char smem[];
+    unsigned char *As = smem;                         // kWgSteps x 4096
+    unsigned char *Bs = smem + kWgSteps * 4096;       // kWgSteps x 512
+    uint64_t *bar = reinterpret_cast<uint64_t *>(Bs + kWgSteps * 512);
+    uint32_t *s_taddr = reinterpret_cast<uint32_t *>(bar + 1);
     const int V = g.size();
-    float acc[28];
-#pragma unroll
-    for (int k = 0; k < 28; ++k) acc[k] = 0.f;
-    for (int v = threadIdx.x; v < V; v += kWThreads) {
-        const float gz = gz_at(gy, y, relu, size_t(co) * V + v);
-        if (gz == 0.f) continue;
-        const int xx = v % g.nx, yy = (v / g.nx) % g.ny, zz = v / (g.nx * g.ny);
-#pragma unroll
-        for (int k = 0; k < 27; ++k) {
-            const int u = tap(g, zz, yy, xx, k, 1);
-            if (u >= 0) acc[k] = fmaf(gz, __bfloat162float(x[size_t(ci) * V + u]), acc[k]);
-        }
-        acc[27] += gz;
-    }
-    // fixed-order reduction: warp shuffles, then the warps' partials in order
-    __shared__ float part[kWThreads / 32][28];
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-#pragma unroll
-    for (int k = 0; k < 28; ++k) {
-        float s = acc[k];
-#pragma unroll
-        for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
-        if (lane == 0) part[wid][k] = s;
-    }
+    const int mt = blockIdx.x, chunk = blockIdx.y;
+    const int c0 = chunk * kWgChunk;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (threadIdx.x == 0) mbar_init(bar);
+    if (warp == 0) tmem_alloc(s_taddr);
+    fence_before();
     __syncthreads();
-    if (threadIdx.x < 28) {
-        float s = 0.f;
-        for (int i = 0; i < kWThreads / 32; ++i) s += part[i][threadIdx.x];
-        if (threadIdx.x < 27) gw[(size_t(co) * cin + ci) * 27 + threadIdx.x] = s;
-        else if (ci == 0) gb[co] = s;
+    fence_after();
+    const uint32_t taddr = *s_taddr;
+    constexpr uint32_t idesc = instr_desc(kM, kC, 1, 1);
+    constexpr int kRoundVox = kWgSteps * 16;
+    const int nround = kWgChunk / kRoundVox;
+    bool ok = true;
+    int issued = 0;
+    for (int r = 0; r < nround && ok; ++r) {
+        const int vr = c0 + r * kRoundVox;
+        if (vr >= V) break;
+        // A: 16 M groups (tap, channel half) x 16 voxels per step; B: 2 N groups x 16 voxels
+        for (int i = threadIdx.x; i < kWgSteps * 16 * 16; i += kThreads) {
+            const int s = i / 256, mg = (i / 16) % 16, kv = i % 16;
+            const int v = vr + s * 16 + kv, tap = mt * 8 + (mg >> 1), h = mg & 1;
+            const int u = (v < V && tap < 27) ? neighbour(g, v, tap, 1) : -1;
+            *reinterpret_cast<uint4 *>(As + s * 4096 + (mg * 2 + (kv >> 3)) * 128 + (kv & 7) * 16) =
+                channels8<false>(x, nullptr, 0, u, h);
+        }
+        for (int i = threadIdx.x; i < kWgSteps * 2 * 16; i += kThreads) {
+            const int s = i / 32, ng = (i / 16) % 2, kv = i % 16;
+            const int v = vr + s * 16 + kv;
+            *reinterpret_cast<uint4 *>(Bs + s * 512 + (ng * 2 + (kv >> 3)) * 128 + (kv & 7) * 16) =
+                channels8<true>(gy, y_act, relu, v < V ? v : -1, ng);
+        }
+        fence_async_smem();
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            fence_after();
+            for (int s = 0; s < kWgSteps; ++s)
+                mma_bf16(taddr, smem_desc(As + s * 4096, 128, 256), smem_desc(Bs + s * 512, 128, 256), idesc,
+                         (r | s) != 0);
+            mma_commit(bar);
+        }
+        ++issued;
+        ok = mbar_wait(bar, uint32_t(r & 1));
+        ok = __syncthreads_and(ok);
+    }
+    float *dst = part + (size_t(chunk) * 4 * kM + size_t(mt) * kM + 32 * warp + lane) * kC;
+    if (!ok) {
+        if (threadIdx.x == 0) {
+            atomicExch(err, 1);
+            mbar_wait(bar, uint32_t((issued - 1) & 1));
+        }
+    } else if (issued == 0) {
+#pragma unroll
+        for (int c = 0; c < 16; ++c) dst[c] = 0.f;
+    } else {
+        fence_after();
+        float acc[16];
+        tmem_ld16(taddr + (uint32_t(32 * warp) << 16), acc);
+#pragma unroll
+        for (int c = 0; c < 16; c += 4) reinterpret_cast<float4 *>(dst)[c / 4] = make_float4(acc[c], acc[c + 1], acc[c + 2], acc[c + 3]);
+    }
+    fence_before();
+    __syncthreads();
+    if (warp == 0) tmem_dealloc(taddr);
+}
+
+// gw[co][ci][tap] = sum over chunks, in chunk order, of the partial sums
+__global__ void k_conv_wgrad_sum(int cin, int cout, int nchunk, const float *__restrict__ part, float *__restrict__ gw)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= cout * cin * 27) return;
+    const int co = i / (cin * 27), ci = (i / 27) % cin, tap = i % 27;
+    const size_t row = size_t(tap) * kC + ci;        // = mt * 128 + (tap - 8 mt) * 16 + ci
+    float s = 0.f;
+    for (int c = 0; c < nchunk; ++c) s += part[(size_t(c) * 4 * kM + row) * kC + co];
+    gw[i] = s;
+}
+
+// gb[co] = sum_v gz[v][co] (FP32 gz), one block per output channel, fixed-order reduction
+constexpr int kBThreads = 256;
+__global__ void __launch_bounds__(kBThreads) k_conv_bias_grad(Grid g, const float *__restrict__ gy,
+                                                              const __nv_bfloat16 *__restrict__ y_act, int relu,
+                                                              float *__restrict__ gb)
+{
+    const int co = blockIdx.x;
+    const int V = g.size();
+    float s = 0.f;
+    for (int v = threadIdx.x; v < V; v += kBThreads) {
+        const float gz = gy[size_t(v) * kC + co];
+        if (!relu || __bfloat162float(y_act[size_t(v) * kC + co]) > 0.f) s += gz;
+    }
+    __shared__ float part[kBThreads / 32];
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
+    if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        float t = 0.f;
+        for (int i = 0; i < kBThreads / 32; ++i) t += part[i];
+        gb[co] = t;
     }
 }
+
+constexpr size_t kConvSmem = 27 * 512 + kTapsRound * 4096 + 16;
+constexpr size_t kWgSmem = kWgSteps * (4096 + 512) + 16;
 
 int check(int cin, int cout, int nz, int ny, int nx)
 {
-    if (cin < 1 || cin > kMaxC || cout < 1 || cout > kMaxC || nz < 1 || ny < 1 || nx < 1) return HRN_EARG;
+    if (cin < 1 || cin > kC || cout < 1 || cout > kC || nz < 1 || ny < 1 || nx < 1) return HRN_EARG;
     if (int64_t(nz) * ny * nx > (int64_t(1) << 30)) return HRN_EARG;
     return HRN_OK;
+}
+
+// Per-device scratch of the layers (the error flag and the weight-gradient partial
+// sums), grown on demand and kept until the process exits.
+struct Scratch {
+    int *err = nullptr;
+    float *part = nullptr;
+    size_t part_bytes = 0;
+};
+
+int scratch(int dev, size_t part_bytes, Scratch &out)
+{
+    static std::mutex mu;
+    static Scratch per[64];
+    if (dev < 0 || dev >= 64) return HRN_EARG;
+    std::lock_guard<std::mutex> lock(mu);
+    Scratch &s = per[dev];
+    if (!s.err) {
+        if (cudaMalloc(&s.err, sizeof(int)) != cudaSuccess) return HRN_EOOM;
+        if (cudaMemset(s.err, 0, sizeof(int)) != cudaSuccess) return HRN_ECUDA;
+    }
+    if (part_bytes > s.part_bytes) {
+        if (s.part) cudaFree(s.part);
+        s.part = nullptr;
+        s.part_bytes = 0;
+        if (cudaMalloc(&s.part, part_bytes) != cudaSuccess) return HRN_EOOM;
+        s.part_bytes = part_bytes;
+    }
+    out = s;
+    return HRN_OK;
+}
+
+int check_err(const Scratch &s, cudaStream_t st)
+{
+    int e = 0;
+    if (cudaMemcpyAsync(&e, s.err, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess) return HRN_ECUDA;
+    if (cudaStreamSynchronize(st) != cudaSuccess) return HRN_ECUDA;
+    if (e) {
+        cudaMemsetAsync(s.err, 0, sizeof(int), st);
+        return HRN_ECUDA;
+    }
+    return HRN_OK;
+}
+
+template <bool GRAD>
+void set_smem_once()
+{
+    static std::atomic<uint64_t> done{0};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const uint64_t bit = dev >= 0 && dev < 64 ? (uint64_t(1) << dev) : 0;
+    if (bit && (done.load() & bit)) return;
+    cudaFuncSetAttribute(k_conv_tc<GRAD>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kConvSmem));
+    done.fetch_or(bit);
 }
 
 }  // namespace
@@ -150,12 +453,17 @@ extern "C" int hrn_cnn_conv3d_forward(int32_t cin, int32_t cout, int32_t nz, int
 {
     if (int rc = check(cin, cout, nz, ny, nx)) return rc;
     if (!x || !w || !bias || !y) return HRN_EARG;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return HRN_ECUDA;
+    Scratch s;
+    if (int rc = scratch(dev, 0, s)) return rc;
     const Grid g{nz, ny, nx};
-    const int V = nz * ny * nx, th = 128;
-    k_conv_fwd<<<(V + th - 1) / th, th, 0, static_cast<cudaStream_t>(stream)>>>(
-        cin, cout, g, static_cast<const __nv_bfloat16 *>(x), static_cast<const __nv_bfloat16 *>(w), bias, relu,
-        static_cast<__nv_bfloat16 *>(y));
-    return cudaGetLastError() == cudaSuccess ? HRN_OK : HRN_ECUDA;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    set_smem_once<false>();
+    k_conv_tc<false><<<(g.size() + kM - 1) / kM, kThreads, kConvSmem, st>>>(
+        cin, cout, g, x, nullptr, static_cast<const __nv_bfloat16 *>(w), bias, relu, y, s.err);
+    if (cudaGetLastError() != cudaSuccess) return HRN_ECUDA;
+    return check_err(s, st);
 }
 
 extern "C" int hrn_cnn_conv3d_backward(int32_t cin, int32_t cout, int32_t nz, int32_t ny, int32_t nx, const void *x,
@@ -164,13 +472,24 @@ extern "C" int hrn_cnn_conv3d_backward(int32_t cin, int32_t cout, int32_t nz, in
 {
     if (int rc = check(cin, cout, nz, ny, nx)) return rc;
     if (!x || !w || !y || !gy || !gw || !gb) return HRN_EARG;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return HRN_ECUDA;
     const Grid g{nz, ny, nx};
-    const int V = nz * ny * nx, th = 128;
+    const int V = g.size();
+    const int nchunk = (V + kWgChunk - 1) / kWgChunk;
+    Scratch s;
+    if (int rc = scratch(dev, size_t(nchunk) * 4 * kM * kC * sizeof(float), s)) return rc;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
-    if (gx)
-        k_conv_bwd_data<<<(V + th - 1) / th, th, 0, st>>>(cin, cout, g, static_cast<const __nv_bfloat16 *>(w),
-                                                          static_cast<const __nv_bfloat16 *>(y), relu, gy, gx);
-    k_conv_bwd_weight<<<cin * cout, kWThreads, 0, st>>>(cin, cout, g, static_cast<const __nv_bfloat16 *>(x),
-                                                        static_cast<const __nv_bfloat16 *>(y), relu, gy, gw, gb);
-    return cudaGetLastError() == cudaSuccess ? HRN_OK : HRN_ECUDA;
+    const __nv_bfloat16 *yb = static_cast<const __nv_bfloat16 *>(y);
+    if (gx) {
+        set_smem_once<true>();
+        k_conv_tc<true><<<(V + kM - 1) / kM, kThreads, kConvSmem, st>>>(
+            cin, cout, g, gy, yb, static_cast<const __nv_bfloat16 *>(w), nullptr, relu, gx, s.err);
+    }
+    k_conv_wgrad_tc<<<dim3(4, nchunk), kThreads, kWgSmem, st>>>(g, static_cast<const __nv_bfloat16 *>(x), gy, yb, relu,
+                                                                 s.part, s.err);
+    k_conv_wgrad_sum<<<(cout * cin * 27 + 127) / 128, 128, 0, st>>>(cin, cout, nchunk, s.part, gw);
+    k_conv_bias_grad<<<cout, kBThreads, 0, st>>>(g, gy, yb, relu, gb);
+    if (cudaGetLastError() != cudaSuccess) return HRN_ECUDA;
+    return check_err(s, st);
 }

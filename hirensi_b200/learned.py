@@ -210,7 +210,9 @@ class DeviceNet:
         V = int(np.prod(shape))
         self.V = V
         self.ch = net.ch
-        self.act = [torch.zeros(c * V, dtype=torch.int16, device=self.dev) for c in self.ch]   # BF16 bits
+        # channels-last activations with a channel stride of 16 ([V][16] BF16 bits); the
+        # channels past a layer's count stay zero
+        self.act = [torch.zeros(16 * V, dtype=torch.int16, device=self.dev) for _ in self.ch]
         self.sync_weights()
 
     def _ck(self, rc):
@@ -227,25 +229,29 @@ class DeviceNet:
         t = self.torch
         CH = self.ch
         nz, ny, nx = self.shape
-        self.act[0].copy_(t.from_numpy(to_bf16_bits(x).view(np.int16).ravel()))
+        xl = np.zeros((self.V, 16))
+        xl[:, :CH[0]] = np.asarray(x).reshape(CH[0], self.V).T
+        self.act[0].copy_(t.from_numpy(to_bf16_bits(xl).view(np.int16).ravel()))
         for i in range(4):
             self._ck(self.L.hrn_cnn_conv3d_forward(CH[i], CH[i + 1], nz, ny, nx, C.c_void_p(self.act[i].data_ptr()),
                                                    C.c_void_p(self.wd[i].data_ptr()), C.c_void_p(self.bd[i].data_ptr()),
                                                    int(i < 3), C.c_void_p(self.act[i + 1].data_ptr()), C.c_void_p(self.stream)))
-        z = self.act[4].cpu().numpy().view(np.uint16)
-        return from_bf16_bits(z).astype(np.float64).reshape((CH[4],) + self.shape)
+        z = self.act[4].cpu().numpy().view(np.uint16).reshape(self.V, 16)[:, :CH[4]]
+        return from_bf16_bits(np.ascontiguousarray(z.T)).astype(np.float64).reshape((CH[4],) + self.shape)
 
     def backward(self, gz: np.ndarray):
         """Weight and bias gradients for dL/dz = gz (after a forward of the same input)."""
         t = self.torch
         CH = self.ch
         nz, ny, nx = self.shape
-        gy = t.from_numpy(np.ascontiguousarray(gz, dtype=np.float32).ravel()).to(self.dev)
+        gl = np.zeros((self.V, 16), dtype=np.float32)
+        gl[:, :CH[4]] = np.asarray(gz, dtype=np.float32).reshape(CH[4], self.V).T
+        gy = t.from_numpy(gl.ravel()).to(self.dev)
         gws, gbs = [None] * 4, [None] * 4
         for i in range(3, -1, -1):
             gw = t.zeros(CH[i + 1] * CH[i] * 27, dtype=t.float32, device=self.dev)
             gb = t.zeros(CH[i + 1], dtype=t.float32, device=self.dev)
-            gx = t.zeros(CH[i] * self.V, dtype=t.float32, device=self.dev) if i > 0 else None
+            gx = t.zeros(16 * self.V, dtype=t.float32, device=self.dev) if i > 0 else None
             self._ck(self.L.hrn_cnn_conv3d_backward(CH[i], CH[i + 1], nz, ny, nx, C.c_void_p(self.act[i].data_ptr()),
                                                     C.c_void_p(self.wd[i].data_ptr()), C.c_void_p(self.act[i + 1].data_ptr()),
                                                     int(i < 3), C.c_void_p(gy.data_ptr()),

@@ -314,15 +314,21 @@ int hrn_illumination(hrn_ctx *ctx, double *d_out);
  * arrays [nj], overwritten.  Needs the whole forward history. */
 int hrn_pseudo_hessian(hrn_ctx *ctx, double *d_h_lambda, double *d_h_mu);
 
-/* 3x3x3 convolution with zero padding on a [channel][nz][ny][nx] grid, BF16 x, w
- * and y, FP32 bias and accumulation: y = act(b + w * x), act = ReLU when relu != 0.
- * w is [cout][cin][27] (tap k = 9 dz + 3 dy + dx).  At most 16 channels in and out.
- * All pointers are device pointers; stream is a cudaStream_t or NULL. */
+/* 3x3x3 convolution with zero padding on the 5th-generation tensor cores (tcgen05.mma,
+ * BF16 operands, FP32 accumulation in tensor memory): y = act(b + w * x), act = ReLU
+ * when relu != 0.  Activations are channels-last with a channel stride of 16:
+ * x [nz][ny][nx][16] BF16 with channels >= cin zero, y [nz][ny][nx][16] BF16 with
+ * channels >= cout written as zero.  w is [cout][cin][27] BF16 (tap k = 9 dz + 3 dy + dx),
+ * bias [cout] FP32.  At most 16 channels in and out.  All pointers are device pointers;
+ * stream is a cudaStream_t or NULL.  Returns once the layer has run (the kernels' error
+ * flag is read back). */
 int hrn_cnn_conv3d_forward(int32_t cin, int32_t cout, int32_t nz, int32_t ny, int32_t nx, const void *x,
                            const void *w, const float *bias, int32_t relu, void *y, void *stream);
-/* Gradients of that layer from gy = dL/dy (FP32): gx = dL/dx (FP32, skipped when
- * NULL), gw = dL/dw [cout][cin][27] and gb = dL/db [cout] (FP32, overwritten).
- * y is the forward output (for the ReLU mask). */
+/* Gradients of that layer from gy = dL/dy (FP32 [nz][ny][nx][16]): gx = dL/dx (FP32
+ * [nz][ny][nx][16], channels >= cin zero; skipped when NULL), gw = dL/dw [cout][cin][27]
+ * and gb = dL/db [cout] (FP32, overwritten).  y is the forward output (for the ReLU mask).
+ * The masked gy is rounded to BF16 as the tensor-core operand of gx and gw; gb sums it in
+ * FP32.  Partial sums over voxel chunks are added in a fixed order. */
 int hrn_cnn_conv3d_backward(int32_t cin, int32_t cout, int32_t nz, int32_t ny, int32_t nx, const void *x,
                             const void *w, const void *y, int32_t relu, const float *gy, float *gx, float *gw,
                             float *gb, void *stream);

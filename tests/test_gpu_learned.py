@@ -1,6 +1,7 @@
 """Device kernels of the learned preconditioner against the host oracle: the BF16
-3-D convolution forward and backward (FP32 accumulation), the source illumination
-of the forward history, and a few training steps lowering the loss."""
+3-D convolution forward and backward on the tensor cores (FP32 accumulation), the
+source illumination of the forward history, and a few training steps lowering the
+loss."""
 import ctypes as C
 
 import numpy as np
@@ -16,38 +17,62 @@ def _bits(t, a):
     return t.from_numpy(Lr.to_bf16_bits(a).view(np.int16).ravel()).cuda()
 
 
-@pytest.mark.parametrize("cin,cout,shape,relu", [(4, 16, (5, 7, 9), 1), (16, 16, (6, 5, 8), 1), (16, 2, (4, 6, 5), 0)])
+def _last(a):
+    """[c, nz, ny, nx] -> channels-last [V, 16] with the channels past c zero."""
+    c = a.shape[0]
+    out = np.zeros((a[0].size, 16), dtype=a.dtype)
+    out[:, :c] = a.reshape(c, -1).T
+    return out
+
+
+def _first(a, c, shape):
+    """channels-last [V, 16] -> [c, nz, ny, nx]."""
+    return np.ascontiguousarray(a.reshape(-1, 16)[:, :c].T).reshape((c,) + shape)
+
+
+@pytest.mark.parametrize("cin,cout,shape,relu", [(4, 16, (5, 7, 9), 1), (16, 16, (6, 5, 8), 1), (16, 2, (4, 6, 5), 0),
+                                                 (6, 16, (17, 33, 33), 1), (16, 16, (3, 40, 47), 1)])
 def test_conv3d_kernels_match_oracle(gpu_lib, cin, cout, shape, relu):
+    """The tensor-core layers against the numpy oracle: the forward within one BF16
+    rounding of the FP64 result; the gradients at FP32-accumulation accuracy against
+    the oracle fed the same BF16-rounded masked gy (the tensor-core operand); gb from
+    the FP32 gy.  The shapes include tiles cut by the grid's end and more than one
+    weight-gradient voxel chunk."""
     import torch
     rng = np.random.default_rng(cin * 100 + cout)
     x = Lr.round_bf16(rng.standard_normal((cin,) + shape))
     w = Lr.round_bf16(rng.standard_normal((cout, cin, 27)) * 0.2)
     b = (rng.standard_normal(cout) * 0.1).astype(np.float32).astype(np.float64)
     V = int(np.prod(shape))
-    xd, wd = _bits(torch, x), _bits(torch, w)
+    xd, wd = _bits(torch, _last(x)), _bits(torch, w)
     bd = torch.from_numpy(b.astype(np.float32)).cuda()
-    yd = torch.zeros(cout * V, dtype=torch.int16, device="cuda")
+    yd = torch.full((16 * V,), 0x7FC0, dtype=torch.int16, device="cuda")   # NaN bits: every channel is written
     nz, ny, nx = shape
     rc = gpu_lib.hrn_cnn_conv3d_forward(cin, cout, nz, ny, nx, C.c_void_p(xd.data_ptr()), C.c_void_p(wd.data_ptr()),
                                         C.c_void_p(bd.data_ptr()), relu, C.c_void_p(yd.data_ptr()), None)
     assert rc == 0
-    y = Lr.from_bf16_bits(yd.cpu().numpy().view(np.uint16)).astype(np.float64).reshape((cout,) + shape)
+    yl = Lr.from_bf16_bits(yd.cpu().numpy().view(np.uint16)).astype(np.float64).reshape(V, 16)
+    assert np.all(yl[:, cout:] == 0.0)
+    y = _first(yl, cout, shape)
     yr = Lr.conv_ref(x, w, b, relu)
     # BF16 output: within one rounding of the FP64 result
     assert np.all(np.abs(y - yr) <= 2.0 ** -7 * np.abs(yr) + 1e-6)
-    gy = rng.standard_normal(y.shape)
-    gyd = torch.from_numpy(gy.astype(np.float32).ravel()).cuda()
-    gx = torch.zeros(cin * V, dtype=torch.float32, device="cuda")
+    gy = rng.standard_normal(y.shape).astype(np.float32).astype(np.float64)
+    gyd = torch.from_numpy(_last(gy).astype(np.float32).ravel()).cuda()
+    gx = torch.full((16 * V,), float("nan"), dtype=torch.float32, device="cuda")
     gw = torch.zeros(cout * cin * 27, dtype=torch.float32, device="cuda")
     gb = torch.zeros(cout, dtype=torch.float32, device="cuda")
     rc = gpu_lib.hrn_cnn_conv3d_backward(cin, cout, nz, ny, nx, C.c_void_p(xd.data_ptr()), C.c_void_p(wd.data_ptr()),
                                          C.c_void_p(yd.data_ptr()), relu, C.c_void_p(gyd.data_ptr()),
                                          C.c_void_p(gx.data_ptr()), C.c_void_p(gw.data_ptr()), C.c_void_p(gb.data_ptr()), None)
     assert rc == 0
-    gxr, gwr, gbr = Lr.conv_ref_backward(x, w, y, relu, gy.astype(np.float32).astype(np.float64))
+    gxl = gx.cpu().numpy().reshape(V, 16)
+    assert np.all(gxl[:, cin:] == 0.0)
+    gxr, gwr, _ = Lr.conv_ref_backward(x, w, y, relu, Lr.round_bf16(gy * ((y > 0) if relu else 1.0)))
+    _, _, gbr = Lr.conv_ref_backward(x, w, y, relu, gy)
     rel = lambda a, r: np.linalg.norm(a.ravel() - r.ravel()) / np.linalg.norm(r.ravel())
-    assert rel(gx.cpu().numpy(), gxr) < 1e-5
-    assert rel(gw.cpu().numpy(), gwr) < 1e-5
+    assert rel(_first(gxl, cin, shape), gxr) < 1e-5
+    assert rel(gw.cpu().numpy().reshape(cout, cin, 27), gwr) < 1e-5
     assert rel(gb.cpu().numpy(), gbr) < 1e-5
     # invalid sizes are refused without a launch
     assert gpu_lib.hrn_cnn_conv3d_forward(17, cout, nz, ny, nx, C.c_void_p(xd.data_ptr()), C.c_void_p(wd.data_ptr()),
