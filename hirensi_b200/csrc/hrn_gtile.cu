@@ -1,5 +1,6 @@
 // hrn_gtile.cu -- RK4 stage kernel over spatially compact row tiles whose
-// gathered stage inputs are staged in shared memory (variants 44, 45, 84, 85).
+// gathered stage inputs are staged in shared memory (variants 44, 45, 84, 85,
+// and 46, 86 with the staged records moved by bulk copies).
 //
 // The row-parallel stage kernel gathers one row record ([S] shots of the stage
 // input of the entry's matrix) per stored entry: about 18 gathers per row on the
@@ -18,6 +19,14 @@
 //      history, kb or the next-stage inputs, or the RK4 update).
 // Entries keep their order within a row and the lane split of the row-parallel
 // kernel, so the row sums equal that kernel's bit for bit.
+//
+// A tile's distinct keys, sorted, fall into runs of consecutive columns of one
+// matrix (about 1.5 runs per row and 6 records per run on the 27-node meshes), and
+// a run is contiguous both in the stage-input array and in the staged set.  With
+// materialized stage inputs and records of a multiple of 16 bytes, variants 46
+// and 86 move each run with one 1-D bulk copy (the tensor memory accelerator)
+// into shared memory, completing on the tile's mbarrier together with the entry
+// slab, so the gathered records take no load/store-unit instructions at all.
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -53,6 +62,7 @@ struct GtArgs {
     const uint32_t *__restrict__ ukey;
     const uint16_t *__restrict__ lidx;
     const T *__restrict__ val;
+    const int4 *__restrict__ runs;      // [nruns] staged index, matrix, first column, records (variants 46, 86)
     int *__restrict__ err;
 };
 
@@ -132,12 +142,14 @@ __device__ __forceinline__ void staged_input(const StageArgs<T> &a, uint32_t key
     }
 }
 
-template <typename T, int S, int STAGE, int G, int MAT>
+template <typename T, int S, int STAGE, int G, int MAT, bool RUNS = false>
 __global__ void __launch_bounds__(kGtThreads) rk4_stage_gt(const StageArgs<T> a, const GtArgs<T> g)
 {
+    static_assert(!RUNS || (MAT == 1 && (S * sizeof(T)) % 16 == 0), "bulk-copied runs need materialized inputs and 16-byte records");
     extern __shared__ __align__(128) unsigned char gt_smem[];
     const int4 ti0 = __ldg(g.tinfo + 2 * blockIdx.x), ti1 = __ldg(g.tinfo + 2 * blockIdx.x + 1);
     const int row_off = ti0.x, nrows = ti0.y, ent_off = ti0.z, nent = ti0.w, u_off = ti1.x, nu = ti1.y;
+    const int run_off = ti1.z, nruns = ti1.w;
     uint64_t *bar = reinterpret_cast<uint64_t *>(gt_smem);
     size_t off = 16;
     int32_t *s_row = reinterpret_cast<int32_t *>(gt_smem + off); off += a16(size_t(nrows) * 4);
@@ -149,19 +161,28 @@ __global__ void __launch_bounds__(kGtThreads) rk4_stage_gt(const StageArgs<T> a,
     T *s_val = reinterpret_cast<T *>(gt_smem + off); off += a16(size_t(nent) * sizeof(T));
     T *sx = reinterpret_cast<T *>(gt_smem + off);
 
-    // 1. entry slab by bulk copies (sizes and addresses are multiples of 16 bytes)
+    constexpr size_t kRec = S * sizeof(T);
+    // 1. entry slab by bulk copies (sizes and addresses are multiples of 16 bytes); with
+    //    RUNS the staged records too, one bulk copy per run of consecutive columns, all
+    //    completing on the same barrier, whose byte count is set before any copy starts
     if (threadIdx.x == 0) {
         mbar_init(bar, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        const uint32_t bytes = uint32_t(nent) * uint32_t(2 + sizeof(T)) + (RUNS ? uint32_t(nu) * uint32_t(kRec) : 0u);
+        if (bytes > 0) mbar_expect_tx(bar, bytes);
+        else asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
     }
     __syncthreads();
-    if (threadIdx.x == 0) {
-        if (nent > 0) {
-            mbar_expect_tx(bar, uint32_t(nent) * uint32_t(2 + sizeof(T)));
-            bulk_g2s(s_lidx, g.lidx + ent_off, uint32_t(nent) * 2u, bar);
-            bulk_g2s(s_val, g.val + ent_off, uint32_t(nent) * uint32_t(sizeof(T)), bar);
-        } else {
-            asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+    if (threadIdx.x == 0 && nent > 0) {
+        bulk_g2s(s_lidx, g.lidx + ent_off, uint32_t(nent) * 2u, bar);
+        bulk_g2s(s_val, g.val + ent_off, uint32_t(nent) * uint32_t(sizeof(T)), bar);
+    }
+    if constexpr (RUNS) {
+        for (int q = threadIdx.x; q < nruns; q += kGtThreads) {
+            const int4 rn = __ldg(g.runs + run_off + q);   // staged index, matrix, first column, records
+            const T *src = STAGE == 1 ? (rn.y == 0 ? a.x3 : (rn.y == 1 ? a.x2 : a.x1))
+                                      : (rn.y == 0 ? a.in_m : (rn.y == 1 ? a.in_t : a.in_h));
+            bulk_g2s(sx + size_t(rn.x) * S, src + size_t(rn.z) * S, uint32_t(rn.w) * uint32_t(kRec), bar);
         }
     }
     // 2. rows of the tile with their source slot and history position
@@ -173,8 +194,9 @@ __global__ void __launch_bounds__(kGtThreads) rk4_stage_gt(const StageArgs<T> a,
         s_pos[r] = (STAGE == 1 && a.hist) ? __ldg(a.store_pos + row) : -1;
     }
     //    staged set, ascending keys, adjacent threads on adjacent keys
-    constexpr size_t kRec = S * sizeof(T);
-    if constexpr (MAT == 1 && STAGE > 1 && kRec % 16 == 0) {
+    if constexpr (RUNS) {
+        // the records arrive by the bulk copies above
+    } else if constexpr (MAT == 1 && STAGE > 1 && kRec % 16 == 0) {
         // materialized inputs: asynchronous 16-byte copies straight into shared memory,
         // eight keys per thread in flight before their copies are issued
         for (int u = threadIdx.x; u < nu; u += 8 * kGtThreads) {
@@ -387,6 +409,7 @@ static int gt_build(hrn_ctx *c, int adj, size_t rec_bytes)
     std::vector<uint32_t> h_ukey;
     std::vector<uint16_t> h_lidx;
     std::vector<int32_t> h_perm;
+    std::vector<int32_t> h_runs;   // [nruns][4] staged index, matrix, first column, records
     std::vector<uint32_t> keys;
     size_t smem = 0;
     bool fit = true;
@@ -417,8 +440,18 @@ static int gt_build(hrn_ctx *c, int adj, size_t rec_bytes)
         const int64_t ne = int64_t(h_lidx.size()) - e0;
         h_lidx.resize(size_t(e0 + pad8(ne)), 0);
         h_perm.resize(size_t(e0 + pad8(ne)), -1);
+        // runs of consecutive keys: consecutive columns of one matrix, contiguous in the
+        // stage-input array and in the staged set
+        const int32_t r0 = int32_t(h_runs.size() / 4);
+        for (size_t q = 0; q < keys.size();) {
+            size_t q1 = q + 1;
+            while (q1 < keys.size() && keys[q1] == keys[q1 - 1] + 1u) ++q1;
+            const int32_t rn[4] = {int32_t(q), int32_t(keys[q] >> kTagBits), int32_t(keys[q] & kColMask), int32_t(q1 - q)};
+            h_runs.insert(h_runs.end(), rn, rn + 4);
+            q = q1;
+        }
         const int32_t ti[8] = {gstart[g0], gstart[g1] - gstart[g0], int32_t(e0), int32_t(pad8(ne)),
-                               int32_t(h_ukey.size()), int32_t(keys.size()), 0, 0};
+                               int32_t(h_ukey.size()), int32_t(keys.size()), r0, int32_t(h_runs.size() / 4) - r0};
         h_tinfo.insert(h_tinfo.end(), ti, ti + 8);
         h_ukey.insert(h_ukey.end(), keys.begin(), keys.end());
     };
@@ -470,6 +503,8 @@ static int gt_build(hrn_ctx *c, int adj, size_t rec_bytes)
     HRN_CUDA(c, gs.d_ukey.alloc(std::max<size_t>(h_ukey.size(), 1) * 4));
     HRN_CUDA(c, gs.d_lidx.alloc(h_lidx.size() * 2));
     HRN_CUDA(c, gs.d_perm.alloc(h_perm.size() * 4));
+    HRN_CUDA(c, gs.d_runs.alloc(std::max<size_t>(h_runs.size(), 4) * 4));
+    if (!h_runs.empty()) HRN_CUDA(c, cudaMemcpy(gs.d_runs.p, h_runs.data(), h_runs.size() * 4, cudaMemcpyHostToDevice));
     if (!h_tinfo.empty()) HRN_CUDA(c, cudaMemcpy(gs.d_tinfo.p, h_tinfo.data(), h_tinfo.size() * 4, cudaMemcpyHostToDevice));
     if (!order.empty()) HRN_CUDA(c, cudaMemcpy(gs.d_row.p, order.data(), order.size() * 4, cudaMemcpyHostToDevice));
     HRN_CUDA(c, cudaMemcpy(gs.d_ent.p, h_ent.data(), h_ent.size() * 4, cudaMemcpyHostToDevice));
@@ -480,6 +515,7 @@ static int gt_build(hrn_ctx *c, int adj, size_t rec_bytes)
     gs.smem = smem;
     gs.nu = int64_t(h_ukey.size());
     gs.nent = total;
+    gs.nruns = int64_t(h_runs.size() / 4);
     gs.rec_bytes = rec_bytes;
     gs.val_version = -1;
     gs.built = true;
@@ -519,12 +555,12 @@ int gt_ready(hrn_ctx *c, int adj)
 // ----------------------------------------------------------------------------
 // launch
 
-template <typename T, int S, int STAGE, int G, int MAT>
+template <typename T, int S, int STAGE, int G, int MAT, bool RUNS = false>
 static void launch_gt(const StageArgs<T> &a, const GtArgs<T> &g, int ntiles, size_t smem, cudaStream_t st)
 {
     static std::atomic<uint64_t> smem_done{0};
-    smem_limit_once(rk4_stage_gt<T, S, STAGE, G, MAT>, int(kGtBudget), smem_done);
-    rk4_stage_gt<T, S, STAGE, G, MAT><<<ntiles, kGtThreads, smem, st>>>(a, g);
+    smem_limit_once(rk4_stage_gt<T, S, STAGE, G, MAT, RUNS>, int(kGtBudget), smem_done);
+    rk4_stage_gt<T, S, STAGE, G, MAT, RUNS><<<ntiles, kGtThreads, smem, st>>>(a, g);
 }
 
 template <typename T, int S, int STAGE>
@@ -535,6 +571,13 @@ static void launch_gt_variant(const StageArgs<T> &a, const GtArgs<T> &g, int nti
     case 44: launch_gt<T, S, STAGE, 4, 0>(a, g, ntiles, smem, st); break;
     case 45: launch_gt<T, S, STAGE, 4, 1>(a, g, ntiles, smem, st); break;
     case 84: launch_gt<T, S, STAGE, 8, 0>(a, g, ntiles, smem, st); break;
+    case 46:
+    case 86:
+        if constexpr ((S * sizeof(T)) % 16 == 0) {
+            if (variant == 46) launch_gt<T, S, STAGE, 4, 1, true>(a, g, ntiles, smem, st);
+            else launch_gt<T, S, STAGE, 8, 1, true>(a, g, ntiles, smem, st);
+        }
+        break;
     default: launch_gt<T, S, STAGE, 8, 1>(a, g, ntiles, smem, st); break;
     }
 }
@@ -551,8 +594,13 @@ static int gt_stage_t(hrn_ctx *c, const StageArgs<T> &a, int stage, int adj, int
         return set_error(c, HRN_ESTATE, "staged-gather tables not built");
     }
     if (gs.ntiles == 0) return 0;   // no rows
+    if ((variant == 46 || variant == 86) && (S * sizeof(T)) % 16 != 0) {
+        static const int two = 2;
+        cudaMemcpyAsync(c->d_step_err.p, &two, sizeof(int), cudaMemcpyHostToDevice, c->stream);
+        return set_error(c, HRN_EARG, "variants 46 / 86 need records of a multiple of 16 bytes");
+    }
     const GtArgs<T> g{gs.d_tinfo.as<int4>(), gs.d_row.as<int32_t>(), gs.d_ent.as<int32_t>(), gs.d_ukey.as<uint32_t>(),
-                      gs.d_lidx.as<uint16_t>(), gs.d_val.as<T>(), c->d_step_err.as<int>()};
+                      gs.d_lidx.as<uint16_t>(), gs.d_val.as<T>(), gs.d_runs.as<int4>(), c->d_step_err.as<int>()};
     switch (stage) {
     case 1: launch_gt_variant<T, S, 1>(a, g, gs.ntiles, gs.smem, variant, c->stream); break;
     case 2: launch_gt_variant<T, S, 2>(a, g, gs.ntiles, gs.smem, variant, c->stream); break;

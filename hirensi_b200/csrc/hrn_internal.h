@@ -85,7 +85,7 @@ struct LoopGraph {
     ~LoopGraph() { reset(); }
 };
 
-// Row tiles of the staged-gather stage kernel (variants 44, 45, 84, 85) for one
+// Row tiles of the staged-gather stage kernel (variants 44-46, 84-86) for one
 // operator direction: spatially compact sets of rows whose gathered (matrix,
 // column) pairs, entries and row data fit in one CTA's shared memory.
 struct GtSet {
@@ -102,6 +102,8 @@ struct GtSet {
     DevBuf d_lidx;              // [nent] uint16 position of the entry's key in its tile's set
     DevBuf d_perm;              // [nent] int32 entry of the scaled value array (-1: padding)
     DevBuf d_val;               // [nent] scaled values in tile order (T)
+    DevBuf d_runs;              // [nruns][4] staged index, matrix, first column, records of each run of consecutive keys
+    int64_t nruns = 0;
     int64_t val_version = -1;   // value version d_val was built from
     size_t val_elem = 0;
 };
@@ -296,7 +298,9 @@ int finalize_pattern_from_keys(hrn_ctx *c, const std::vector<uint64_t> &keys);
 int vec_reduce(hrn_ctx *c, int kind, int n, const double *x, const double *y, double *out);
 int gt_ready(hrn_ctx *c, int adj);
 int gt_stage(hrn_ctx *c, const void *stage_args, int stage, int adj, int variant);
-inline bool is_gt_variant(int v) { return v == 44 || v == 45 || v == 84 || v == 85; }
+inline bool is_gt_variant(int v) { return v == 44 || v == 45 || v == 84 || v == 85 || v == 46 || v == 86; }
+// staged-gather variants whose records move by bulk copies: records of a multiple of 16 bytes
+inline bool gt_runs_valid(int v, int nshot, size_t elem) { return (v != 46 && v != 86) || (size_t(nshot) * elem) % 16 == 0; }
 int elem_prepare(hrn_ctx *c);
 int elem_ready(hrn_ctx *c);
 int elem_stage(hrn_ctx *c, const void *stage_args, int stage, int adj, int acc, int shots_per_thread, int mat);

@@ -873,7 +873,8 @@ static int autotune_lanes(hrn_ctx *c, StageArgs<T> a, T *X, T *Y, const TileArgs
     std::vector<int> cand;
     if (c->have_pattern) cand.assign(kVariants, kVariants + 10);   // none with a matrix-free operator
     if (c->have_pattern && gt_ready(c, adj) == 0)
-        for (int v : {44, 45, 84, 85}) cand.push_back(v);
+        for (int v : {44, 45, 84, 85, 46, 86})
+            if (gt_runs_valid(v, c->nshot, c->elem_bytes())) cand.push_back(v);
     if (c->op_from_mesh) {
         if (int rc = elem_ready(c)) return rc;
         for (int v : {90, 91, 92, 93, 94, 95, 100, 101, 102, 103, 104, 105})
@@ -1032,6 +1033,8 @@ static int forward_t(hrn_ctx *c)
         if (!elem_variant_valid(c, c->lanes_f)) return set_error(c, HRN_EARG, "matrix-free variant not available for this shot count and precision");
         if (int rc = elem_ready(c)) return rc;
     } else if (is_gt_variant(c->lanes_f)) {
+        if (!gt_runs_valid(c->lanes_f, c->nshot, c->elem_bytes()))
+            return set_error(c, HRN_EARG, "variants 46 / 86 need records (shots x value size) of a multiple of 16 bytes");
         if (int rc = gt_ready(c, 0)) return rc;
     }
     cudaEvent_t t0, t1;
@@ -1135,6 +1138,8 @@ static int adjoint_t(hrn_ctx *c, int lambda_2mu, int keep_p)
         if (!elem_variant_valid(c, c->lanes_a)) return set_error(c, HRN_EARG, "matrix-free variant not available for this shot count and precision");
         if (int rc = elem_ready(c)) return rc;
     } else if (is_gt_variant(c->lanes_a)) {
+        if (!gt_runs_valid(c->lanes_a, c->nshot, c->elem_bytes()))
+            return set_error(c, HRN_EARG, "variants 46 / 86 need records (shots x value size) of a multiple of 16 bytes");
         if (int rc = gt_ready(c, 1)) return rc;
     }
     if (c->ckpt > 0 && is_gt_variant(c->lanes_f))   // the recomputed forward segments
@@ -1319,6 +1324,7 @@ static int time_stage_t(hrn_ctx *c, int adj, int nsteps, double *avg_ms)
     if (is_elem_variant(lanes)) {
         if (int rc = elem_ready(c)) return rc;
     } else if (is_gt_variant(lanes)) {
+        if (!gt_runs_valid(lanes, c->nshot, c->elem_bytes())) return set_error(c, HRN_EARG, "variant needs 16-byte records");
         if (int rc = gt_ready(c, adj)) return rc;
     }
     HRN_CUDA(c, cudaMemsetAsync(X0, 0, 6 * vn * sizeof(T), c->stream));

@@ -1,9 +1,10 @@
-"""Staged-gather stage kernels (variants 44, 45, 84, 85) through the C ABI.
+"""Staged-gather stage kernels (variants 44, 45, 84, 85, 46, 86) through the C ABI.
 
 The rows are cut into compact tiles whose gathered stage inputs are loaded once
 into shared memory.  Entries keep their order inside a row, so with the same
 lane count and stage-input mode the row sums are those of the row-parallel
-kernel: 44 = 40, 45 = 41, 84 = 80, 85 = 81 bit for bit.  Parity against the FP64
+kernel: 44 = 40, 45 = 41, 84 = 80, 85 = 81 bit for bit; 46 and 86 stage the same
+records by bulk copies of runs of consecutive columns, so 46 = 41 and 86 = 81.  Parity against the FP64
 oracle uses the bars of the other stage kernels (1e-10 FP64, 1e-4 FP32).
 """
 import numpy as np
@@ -139,3 +140,66 @@ def test_staged_tiles_odd_shot_counts(gpu_lib, nshot, precision):
     for k in range(nshot):
         assert np.abs(out[41][k]).max() > 0
         assert np.array_equal(out[45][k], out[41][k])
+
+
+@pytest.mark.parametrize("nshot,precision,variant,row_parallel",
+                         [(2, "fp64", 46, 41), (4, "fp64", 86, 81), (4, "fp32", 46, 41), (8, "fp32", 86, 81)])
+def test_bulk_copied_runs_equal_row_parallel_kernel(gpu_lib, nshot, precision, variant, row_parallel):
+    """Records of a multiple of 16 bytes moved by one bulk copy per run of
+    consecutive columns: histories and adjoint histories equal the row-parallel
+    kernel's bit for bit, in every stage (stage 1 copies from the state, stages
+    2-4 from the materialized inputs)."""
+    p = tiny(nshot=nshot, nstep=120)
+    _, _, hist_t = oracle_forward(p, p["lam_t"], p["mu_t"])
+    dis = np.stack([traces_from_history(p, h) for h in hist_t])
+    out = {}
+    for v in (variant, row_parallel):
+        with _assembled_solver(p, p["lam"], p["mu"], precision) as s:
+            s.set_variant(v, v)
+            s.forward()
+            assert s.variant() == (v, v)
+            s.adjoint_gradient(dis, keep_p=True)
+            out[v] = ([s.history(k) for k in range(nshot)], [s.adjoint_history(k) for k in range(nshot)])
+    for k in range(nshot):
+        assert np.abs(out[row_parallel][0][k]).max() > 0
+        assert np.array_equal(out[variant][0][k], out[row_parallel][0][k])
+        assert np.array_equal(out[variant][1][k], out[row_parallel][1][k])
+
+
+def test_bulk_copied_runs_on_split_tiles(gpu_lib):
+    """Eight FP64 shots (64-byte records) on the 16 x 16 x 8 mesh: halved tiles, runs
+    of 64-byte records; equal to the row-parallel kernel."""
+    from hirensi_b200 import configs
+    from hirensi_b200.solver import Solver
+    shots = [(x, y) for x in (-15.0, -5.0, 5.0, 15.0) for y in (-10.0, 10.0)]
+    prob = configs.inversion_config(nstep=12, shots=shots)
+    m = prob.mesh
+    hists = {}
+    for v in (86, 81):
+        with Solver("fp64") as s:
+            s.set_mesh(m, RHO)
+            s.assemble(prob.lam0, prob.mu0)
+            s.set_history(m.store_eq)
+            s.set_shots(prob.nstep, prob.dt, prob.src_eq, prob.src_b, prob.ftab)
+            s.set_receivers(prob.eqdis, prob.eqdis_map)
+            s.set_variant(v, v)
+            s.forward()
+            hists[v] = [s.history(k) for k in range(prob.nshot)]
+    for k in range(prob.nshot):
+        assert np.abs(hists[81][k]).max() > 0
+        assert np.array_equal(hists[86][k], hists[81][k])
+
+
+def test_bulk_copied_runs_refuse_unaligned_records(gpu_lib):
+    """Three FP64 shots make 24-byte records, which a bulk copy cannot move: the
+    forward fails with HRN_EARG and the tuner never picks 46 / 86 for them."""
+    from hirensi_b200.capi import HrnError
+    p = tiny(nshot=3, nstep=20)
+    with _assembled_solver(p, p["lam"], p["mu"]) as s:
+        s.set_variant(46, 46)
+        with pytest.raises(HrnError) as ei:
+            s.forward()
+        assert ei.value.code == 1
+    with _assembled_solver(p, p["lam"], p["mu"]) as s:
+        s.forward()
+        assert s.variant()[0] not in (46, 86)
