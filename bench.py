@@ -51,8 +51,11 @@ def parse_args():
     ap.add_argument("--no-fwi", action="store_true", help="skip the FWI time-to-misfit leg")
     ap.add_argument("--fwi-iters", type=int, default=40,
                     help="iteration cap of each FWI time-to-misfit leg")
-    ap.add_argument("--fwi-target", type=float, default=0.5,
+    ap.add_argument("--fwi-target", type=float, default=0.9,
                     help="FWI legs stop once the misfit has fallen by this fraction")
+    ap.add_argument("--fwi-tv", action="store_true",
+                    help="add the TV regularization to the gradient in the FWI legs (off: with it the plain "
+                         "legs stall near a 6 %% reduction)")
     ap.add_argument("--fwi-fac", type=float, default=20.0,
                     help="Fac_Max_Update (largest model change per iteration) of the FWI legs")
     ap.add_argument("--profile-precision", choices=["fp64", "fp32"], default="fp64",
@@ -61,11 +64,12 @@ def parse_args():
                     help="stage-kernel variant for forward and adjoint (0 = chosen by timing on first use)")
     ap.add_argument("--no-graphs", action="store_true",
                     help="launch every kernel directly instead of replaying the captured time loops")
-    ap.add_argument("--workload", choices=["inversion", "uneven", "xl"], default="inversion",
+    ap.add_argument("--workload", choices=["inversion", "uneven", "xl", "shot-scaling"], default="inversion",
                     help="inversion: the 16x16x8 plain inversion loop (default); uneven: batched uneven "
                          "shots on the 80x80x40 + PML 4 mesh, FP32 stepping, checkpointed adjoint; "
                          "xl: the same on the 160x160x80 + PML 6 mesh (86.6 M equations) with the "
-                         "matrix-free operator")
+                         "matrix-free operator; shot-scaling: stage-kernel time per shot for 1, 2, 4 and 8 "
+                         "shots per pass over the 80x80x40 + PML 4 operator (FP32)")
     ap.add_argument("--max-batches", type=int, default=0, help="uneven / xl: time at most this many batches")
     ap.add_argument("--length-scale", type=float, default=0.03,
                     help="uneven workload: record lengths scaled by this factor (a bounded sample)")
@@ -370,20 +374,23 @@ def run_native(args, rank, world, local_rank):
         if not args.no_fwi and world == 1:
             # time to a stated misfit reduction, each leg from the initial model
             result["fwi"] = {"target_reduction": args.fwi_target, "iteration_cap": args.fwi_iters,
-                             "fac_max_update": args.fwi_fac}
+                             "fac_max_update": args.fwi_fac, "regularization": "TV" if args.fwi_tv else None}
             legs = [("fp64", False)] if args.no_fp32 else [("fp64", False), ("fp32", False)]
             if not args.no_fp32 and os.path.exists(PRECOND_WEIGHTS):
                 legs.append(("fp32", True))
             for prec, learned in legs:
                 name = prec + ("_learned" if learned else "")
                 result["fwi"][name] = fwi_leg(prec, prob, dis, local_rank, args.fwi_iters, learned=learned,
-                                              target=args.fwi_target, variant=tuned.get(prec), fac=args.fwi_fac)
+                                              target=args.fwi_target, variant=tuned.get(prec), fac=args.fwi_fac,
+                                              tv=args.fwi_tv)
             f64, fl = result["fwi"]["fp64"], result["fwi"].get("fp32_learned")
             if fl and f64["reached_target"] and fl["reached_target"]:
-                result["fwi"]["time_to_target_speedup_fp32_learned_vs_fp64"] = f64["wall_s"] / fl["wall_s"]
+                result["fwi"]["time_to_target_speedup_fp32_learned_vs_fp64"] = f64["time_to_target_s"] / fl["time_to_target_s"]
             f32 = result["fwi"].get("fp32")
             if f32 and f64["reached_target"] and f32["reached_target"]:
-                result["fwi"]["time_to_target_speedup_fp32_vs_fp64"] = f64["wall_s"] / f32["wall_s"]
+                result["fwi"]["time_to_target_speedup_fp32_vs_fp64"] = f64["time_to_target_s"] / f32["time_to_target_s"]
+            if fl and f64["time_to_50pct_s"] and fl["time_to_50pct_s"]:
+                result["fwi"]["time_to_50pct_speedup_fp32_learned_vs_fp64"] = f64["time_to_50pct_s"] / fl["time_to_50pct_s"]
     s64.close()
     if not args.profile_case and not args.no_batched and world == 1:
         result["batched_fp32"] = batched_leg(args, local_rank)
@@ -639,6 +646,47 @@ def run_uneven(args, rank, world, local_rank):
     return result
 
 
+def run_shot_scaling(args, local_rank):
+    """How the cost of a stage grows with the shots that share one pass over the
+    operator: on the 80x80x40 + PML 4 mesh (12.7 M equations, 312.6 M stored entries),
+    FP32 stepping, for 1, 2, 4 and 8 shots the tuned stage variant is timed alone
+    (hrn_time_stage, 50 RK4 steps per direction).  Per-shot time falling slowly with
+    the shot count means the matrix stream is a small part of a stage, so batches
+    larger than 8 would gain little."""
+    import torch
+    from hirensi_b200 import batching as B
+    from hirensi_b200 import build
+    from hirensi_b200.configs import uneven_config
+    from hirensi_b200.solver import Solver
+    build.build()
+    torch.cuda.set_device(local_rank)
+    prob = uneven_config(length_scale=0.01)
+    m = prob.mesh
+    rows = []
+    for S in (1, 2, 4, 8):
+        sv = Solver("fp32", device=local_rank)
+        sv.set_mesh(m, prob.rho_el)
+        sv.assemble(prob.lam, prob.mu)
+        sv.set_history(m.store_eq)
+        sv.set_checkpointing(10)
+        b = B.pack(prob.shots, list(range(S)))
+        B.configure(sv, b, prob.dt, m.store_position)
+        sv.set_data(np.zeros((S, len(b.eqdis), b.nstep + 1)))
+        sv.forward()
+        sv.adjoint_gradient(None, to_host=False)
+        f, a = sv.time_stage(False, 50), sv.time_stage(True, 50)
+        rows.append({"shots": S, "variant_fwd_adj": list(sv.variant()), "stage_us_fwd_adj": [f * 1e3, a * 1e3],
+                     "stage_us_per_shot": 0.5 * (f + a) * 1e3 / S})
+        sv.close()
+    base = rows[0]["stage_us_per_shot"]
+    for r in rows:
+        r["per_shot_vs_one_shot"] = r["stage_us_per_shot"] / base
+    return {"metric": "stage-kernel time per shot against shots per pass", "unit": "us per shot-stage",
+            "value": rows[-1]["stage_us_per_shot"], "higher_is_better": False, "n_gpus": 1, "dtype": "f32",
+            "data": "synthetic", "config": {"workload": prob.name.replace("_64shots", ""), "equations": m.neq,
+                                            "dof": prob.dof}, "rows": rows}
+
+
 def xl_error(prob, nsteps, local_rank):
     """Seismogram and gradient error of FP32 stepping against FP64 stepping on the
     extra-large mesh (matrix-free operator): the first two shots of the workload, their
@@ -677,8 +725,8 @@ def xl_error(prob, nsteps, local_rank):
             "variants_fp32_fp64": [v32, v64]}
 
 
-def fwi_leg(precision, prob, dis, local_rank, iters, learned=False, target=None, variant=None, fac=5.0):
-    """Wall time of the inversion loop (L-BFGS memory 5, TV, the reference's step rules)
+def fwi_leg(precision, prob, dis, local_rank, iters, learned=False, target=None, variant=None, fac=5.0, tv=False):
+    """Wall time of the inversion loop (L-BFGS memory 5, the reference's step rules, TV optional)
     from the initial model until the misfit has fallen by `target` or `iters` iterations
     have run, all vectors on the device; misfit reduction and model error reached.  With
     `learned`, each iteration first tries the trained CNN's scaled direction.  `variant` =
@@ -698,7 +746,7 @@ def fwi_leg(precision, prob, dis, local_rank, iters, learned=False, target=None,
     if variant:
         s.set_variant(*variant)
     cfg = InversionConfig(m_lbfgs=5, bounds_lambda=(10.0, 2000.0), bounds_mu=(10.0, 1000.0),
-                          fac_max_update_lambda=fac, fac_max_update_mu=fac)
+                          fac_max_update_lambda=fac, fac_max_update_mu=fac, regularization="TV" if tv else None)
     backend = DeviceBackend(s, m)
     pre = None
     if learned:
@@ -728,13 +776,16 @@ def fwi_leg(precision, prob, dis, local_rank, iters, learned=False, target=None,
         err = {"vs_rel_l2_error": float(np.linalg.norm((vs - vs_t)[rd]) / np.linalg.norm(vs_t[rd])),
                "vs_rel_l2_error_initial": float(np.linalg.norm((vs_0 - vs_t)[rd]) / np.linalg.norm(vs_t[rd]))}
     t_target = next((h["wall_s"] for h in hist if target is not None and h["misfit"] <= (1.0 - target) * J0), None)
+    t_half = next((h["wall_s"] for h in hist if h["misfit"] <= 0.5 * J0), None)
+    it_half = next((h["iter"] for h in hist if h["misfit"] <= 0.5 * J0), None)
     s.close()
     out = {"iterations": len(hist) - 1, "wall_s": wall, "time_to_target_s": t_target,
+           "time_to_50pct_s": t_half, "iterations_to_50pct": it_half,
            "misfit_initial": J0, "misfit_final": J, "misfit_reduction": 1.0 - J / J0,
            "misfit_history": [h["misfit"] for h in hist],
            "forward_solves": sum(1 + h["armijo"] + (1 if h.get("learned") is False else 0) for h in hist[1:]) + 1,
-           "config": f"L-BFGS memory 5, TV regularization, reference step rules, Fac_Max_Update {fac}, "
-                     "bounds lambda [10,2000] mu [10,1000]",
+           "config": f"L-BFGS memory 5, {'TV regularization' if tv else 'no regularization'}, reference step "
+                     f"rules (lambda bias on), Fac_Max_Update {fac}, bounds lambda [10,2000] mu [10,1000]",
            "warmup": "one inversion iteration (tables, buffers, captured time loops) before the timed inversion", **err}
     if failed:
         out["armijo_failure"] = failed
@@ -848,6 +899,8 @@ def main():
         res = run_reference(args, rank, world)
     elif args.workload in ("uneven", "xl"):
         res = run_uneven(args, rank, world, local_rank)
+    elif args.workload == "shot-scaling":
+        res = run_shot_scaling(args, local_rank) if rank == 0 else None
     else:
         res = run_native(args, rank, world, local_rank)
     if rank == 0 and res is not None:
