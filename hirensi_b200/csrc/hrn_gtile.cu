@@ -285,6 +285,281 @@ __global__ void __launch_bounds__(kGtThreads) rk4_stage_gt(const StageArgs<T> a,
     }
 }
 
+// ----------------------------------------------------------------------------
+// Pipelined staged tiles (variants 47, 87): persistent CTAs of four consumer warps
+// and one producer warp with two shared-memory buffers.  For its next tile the
+// producer waits until the consumers have released that buffer, sets the byte count
+// on the buffer's mbarrier and starts 1-D bulk copies of everything the tile needs:
+// its header, the row metadata (entry range, source slot, history position, row),
+// the entry slab, the staged records (one copy per run of consecutive columns) and
+// the epilogue's row operands (x1, x2, x3 and the stage's inputs or kb, one copy per
+// run of consecutive rows and operand).  Meanwhile the consumers sum and finish the
+// previous tile from shared memory alone, so no phase of a tile waits on a global
+// load.  The row sums and the epilogue use the arithmetic of the other stage kernels
+// (equal to variants 41 / 81 bit for bit).
+
+constexpr int kGtpConsumers = 128;
+constexpr int kGtpThreads = kGtpConsumers + 32;
+constexpr int kGtpHdr = 64;               // tile header: tinfo (32 B) and tinfo2 (16 B)
+constexpr int kGtpRows = kGtRows;         // rows of a tile, at most
+
+// buffer: header | meta [kGtpRows][4] int32 | operands [6][kGtpRows][S] | lidx | values | records
+__host__ __device__ constexpr size_t gtp_fixed(size_t rec) { return kGtpHdr + size_t(kGtpRows) * 16 + 6 * size_t(kGtpRows) * rec; }
+__host__ __device__ constexpr size_t gtp_buffer(size_t rec) { return gtp_fixed(rec) + kGtBudget; }
+__host__ __device__ constexpr size_t gtp_smem(size_t rec) { return 64 + 2 * gtp_buffer(rec) + size_t(kGtpRows) * rec; }
+
+template <typename T>
+struct GtpArgs {
+    const int32_t *__restrict__ tinfo;    // [ntiles][8]
+    const int32_t *__restrict__ tinfo2;   // [ntiles][4] first operand run, runs
+    const int4 *__restrict__ meta;        // [rows in tile order] entry range, slot, history position, row
+    const int4 *__restrict__ eruns;       // [n] first tile row, first row (equation), rows
+    const int4 *__restrict__ runs;        // record runs (as variants 46, 86)
+    const uint16_t *__restrict__ lidx;
+    const T *__restrict__ val;
+    int ntiles;
+    int *__restrict__ err;
+};
+
+__device__ __forceinline__ void bar_named_consumers() { asm volatile("bar.sync 1, 128;" ::: "memory"); }
+
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+// the stage's epilogue operands: x1, x2, x3, then (stages 2, 3) in_t, in_m or (stage 4) kb1, kb2, kb3
+template <typename T, int STAGE>
+__device__ __forceinline__ const T *gtp_operand(const StageArgs<T> &a, int v)
+{
+    if (v == 0) return a.x1;
+    if (v == 1) return a.x2;
+    if (v == 2) return a.x3;
+    if constexpr (STAGE == 4) return v == 3 ? a.kb1 : (v == 4 ? a.kb2 : a.kb3);
+    else return v == 3 ? a.in_t : a.in_m;
+}
+
+template <typename T, int STAGE>
+constexpr int gtp_noperands() { return STAGE == 1 ? 3 : (STAGE == 4 ? 6 : 5); }
+
+// Row epilogue of finish_row_sp with the row's operands read from shared memory
+// (op(v) = operand v of this row); the same arithmetic, so the same bits.
+template <typename T, int S, int STAGE>
+__device__ __forceinline__ void gtp_finish(const StageArgs<T> &a, int row, int sl, int pos, const T (&acc)[S],
+                                           const T *ops, int r)
+{
+    auto op = [&](int v, T (&o)[S]) { lds_rec<T, S>(ops + (size_t(v) * kGtpRows + r) * S, o); };
+    const size_t o = size_t(row) * S;
+    T kb[S];
+    if (sl >= 0) {
+        T sv[S];
+        ldv<T, S>(a.srcv + (size_t(STAGE - 1) * a.nslot + sl) * S, sv);
+#pragma unroll
+        for (int s = 0; s < S; ++s) kb[s] = sv[s] + acc[s];
+    } else {
+#pragma unroll
+        for (int s = 0; s < S; ++s) kb[s] = acc[s];
+    }
+    T x1[S], x2[S], x3[S];
+    op(0, x1);
+    op(1, x2);
+    op(2, x3);
+    if constexpr (STAGE == 1) {
+        if (a.hist && pos >= 0) stv<T, S>(a.hist + size_t(pos) * S, x2);
+    }
+    if constexpr (STAGE < 4) {
+        stv<T, S>(a.kb_out + o, kb);
+        T kt[S], km[S], nt[S], nm[S], nh[S];
+        if constexpr (STAGE == 1) {
+#pragma unroll
+            for (int s = 0; s < S; ++s) { kt[s] = x2[s]; km[s] = x3[s]; }
+        } else {
+            op(3, kt);
+            op(4, km);
+        }
+        const T cc = STAGE == 3 ? a.D : a.c;
+#pragma unroll
+        for (int s = 0; s < S; ++s) {
+            nt[s] = fmaT(cc, km[s], x2[s]);
+            nm[s] = fmaT(cc, kb[s], x3[s]);
+            nh[s] = fmaT(cc, kt[s], x1[s]);
+        }
+        stv<T, S>(a.out_t + o, nt);
+        stv<T, S>(a.out_m + o, nm);
+        stv<T, S>(a.out_h + o, nh);
+    } else {
+        T k1[S], k2[S], k3[S], n1[S], n2[S], n3[S];
+        op(3, k1);
+        op(4, k2);
+        op(5, k3);
+#pragma unroll
+        for (int s = 0; s < S; ++s) {
+            const T km2 = fmaT(a.c, k1[s], x3[s]);
+            const T km3 = fmaT(a.c, k2[s], x3[s]);
+            const T km4 = fmaT(a.D, k3[s], x3[s]);
+            const T kt2 = fmaT(a.c, x3[s], x2[s]);
+            const T kt3 = fmaT(a.c, km2, x2[s]);
+            const T kt4 = fmaT(a.D, km3, x2[s]);
+            const T ht = ((x2[s] + T(2) * kt2) + T(2) * kt3) + kt4;
+            const T hm = ((x3[s] + T(2) * km2) + T(2) * km3) + km4;
+            const T hb = ((k1[s] + T(2) * k2[s]) + T(2) * k3[s]) + kb[s];
+            n1[s] = fmaT(a.d6, ht, x1[s]);
+            n2[s] = fmaT(a.d6, hm, x2[s]);
+            n3[s] = fmaT(a.d6, hb, x3[s]);
+        }
+        stv<T, S>(a.y1 + o, n1);
+        stv<T, S>(a.y2 + o, n2);
+        stv<T, S>(a.y3 + o, n3);
+    }
+}
+
+template <typename T, int S, int STAGE, int G>
+__global__ void __launch_bounds__(kGtpThreads) rk4_stage_gtp(const StageArgs<T> a, const GtpArgs<T> g)
+{
+    constexpr size_t kRec = S * sizeof(T);
+    static_assert(kRec % 16 == 0, "pipelined tiles need 16-byte records");
+    constexpr int NV = gtp_noperands<T, STAGE>();
+    extern __shared__ __align__(128) unsigned char gtp_shm[];
+    uint64_t *full = reinterpret_cast<uint64_t *>(gtp_shm);
+    uint64_t *empty = full + 2;
+    int *s_fail = reinterpret_cast<int *>(full + 4);
+    unsigned char *buf0 = gtp_shm + 64;
+    T *s_acc = reinterpret_cast<T *>(buf0 + 2 * gtp_buffer(kRec));
+    const int tid = threadIdx.x;
+    if (tid == 0) {
+        mbar_init(&full[0], 1);
+        mbar_init(&full[1], 1);
+        mbar_init(&empty[0], 1);
+        mbar_init(&empty[1], 1);
+        *s_fail = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    const int ntiles = g.ntiles;
+    if (tid >= kGtpConsumers) {
+        // ---- producer warp
+        const int lane = tid - kGtpConsumers;
+        int i = 0;
+        for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++i) {
+            const int b = i & 1, k = i >> 1;
+            if (k >= 1 && !mbar_wait(&empty[b], uint32_t((k - 1) & 1))) {
+                if (lane == 0) atomicExch(g.err, 1);
+                break;
+            }
+            unsigned char *buf = buf0 + size_t(b) * gtp_buffer(kRec);
+            const int4 ti0 = __ldg(reinterpret_cast<const int4 *>(g.tinfo) + 2 * t);
+            const int4 ti1 = __ldg(reinterpret_cast<const int4 *>(g.tinfo) + 2 * t + 1);
+            const int4 ti2 = __ldg(reinterpret_cast<const int4 *>(g.tinfo2) + t);
+            const int row_off = ti0.x, nrows = ti0.y, ent_off = ti0.z, nent = ti0.w, nu = ti1.y;
+            const int run_off = ti1.z, nruns = ti1.w, erun_off = ti2.x, neruns = ti2.y;
+            uint16_t *s_lidx = reinterpret_cast<uint16_t *>(buf + gtp_fixed(kRec));
+            T *s_val = reinterpret_cast<T *>(buf + gtp_fixed(kRec) + a16(size_t(nent) * 2));
+            T *sx = reinterpret_cast<T *>(reinterpret_cast<unsigned char *>(s_val) + a16(size_t(nent) * sizeof(T)));
+            T *ops = reinterpret_cast<T *>(buf + kGtpHdr + size_t(kGtpRows) * 16);
+            if (lane == 0) {
+                const uint32_t bytes = 48u + uint32_t(nrows) * 16u + uint32_t(nent) * uint32_t(2 + sizeof(T)) +
+                                       uint32_t(nu) * uint32_t(kRec) + uint32_t(NV) * uint32_t(nrows) * uint32_t(kRec);
+                mbar_expect_tx(&full[b], bytes);
+            }
+            __syncwarp();
+            if (lane == 0) {
+                bulk_g2s(buf, g.tinfo + 8 * size_t(t), 32u, &full[b]);
+                bulk_g2s(buf + 32, g.tinfo2 + 4 * size_t(t), 16u, &full[b]);
+                bulk_g2s(buf + kGtpHdr, g.meta + row_off, uint32_t(nrows) * 16u, &full[b]);
+            } else if (lane == 1 && nent > 0) {
+                bulk_g2s(s_lidx, g.lidx + ent_off, uint32_t(nent) * 2u, &full[b]);
+            } else if (lane == 2 && nent > 0) {
+                bulk_g2s(s_val, g.val + ent_off, uint32_t(nent) * uint32_t(sizeof(T)), &full[b]);
+            }
+            for (int q = lane; q < nruns; q += 32) {
+                const int4 rn = __ldg(g.runs + run_off + q);
+                const T *src = STAGE == 1 ? (rn.y == 0 ? a.x3 : (rn.y == 1 ? a.x2 : a.x1))
+                                          : (rn.y == 0 ? a.in_m : (rn.y == 1 ? a.in_t : a.in_h));
+                bulk_g2s(sx + size_t(rn.x) * S, src + size_t(rn.z) * S, uint32_t(rn.w) * uint32_t(kRec), &full[b]);
+            }
+            for (int q = lane; q < neruns * NV; q += 32) {
+                const int v = q / neruns;
+                const int4 er = __ldg(g.eruns + erun_off + (q - v * neruns));   // first tile row, first row, rows
+                bulk_g2s(ops + (size_t(v) * kGtpRows + er.x) * S, gtp_operand<T, STAGE>(a, v) + size_t(er.y) * S,
+                         uint32_t(er.z) * uint32_t(kRec), &full[b]);
+            }
+        }
+        return;
+    }
+    // ---- consumer warps
+    int i = 0;
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++i) {
+        const int b = i & 1, k = i >> 1;
+        const bool ok = mbar_wait(&full[b], uint32_t(k & 1));
+        if (!ok) *s_fail = 1;
+        bar_named_consumers();
+        if (*s_fail) {
+            if (tid == 0) {
+                atomicExch(g.err, 1);
+                mbar_wait(&full[b], uint32_t(k & 1));   // the copies in flight into this buffer
+            }
+            break;
+        }
+        const unsigned char *buf = buf0 + size_t(b) * gtp_buffer(kRec);
+        const int4 ti0 = *reinterpret_cast<const int4 *>(buf);
+        const int nrows = ti0.y, nent = ti0.w;
+        const int4 *meta = reinterpret_cast<const int4 *>(buf + kGtpHdr);
+        const uint16_t *s_lidx = reinterpret_cast<const uint16_t *>(buf + gtp_fixed(kRec));
+        const T *s_val = reinterpret_cast<const T *>(buf + gtp_fixed(kRec) + a16(size_t(nent) * 2));
+        const T *sx = reinterpret_cast<const T *>(reinterpret_cast<const unsigned char *>(s_val) + a16(size_t(nent) * sizeof(T)));
+        const T *ops = reinterpret_cast<const T *>(buf + kGtpHdr + size_t(kGtpRows) * 16);
+        // row sums, G lanes per row, from shared memory
+        const int lane = tid & (G - 1);
+        const unsigned gmask = (G == 32) ? 0xffffffffu : (((1u << G) - 1u) << ((tid & 31) & ~(G - 1)));
+        for (int r = tid / G; r < nrows; r += kGtpConsumers / G) {
+            const uint32_t pe = uint32_t(meta[r].x);
+            const int k0 = int(pe & 0xffffu), k3 = k0 + int(pe >> 16);
+            T acc[S];
+#pragma unroll
+            for (int s = 0; s < S; ++s) acc[s] = T(0);
+            for (int kk0 = k0 + lane; kk0 < k3; kk0 += 4 * G) {
+#pragma unroll
+                for (int uu = 0; uu < 4; ++uu) {
+                    const int kk = kk0 + uu * G;
+                    if (kk < k3) {
+                        T x[S];
+                        lds_rec<T, S>(sx + size_t(s_lidx[kk]) * S, x);
+                        const T w = s_val[kk];
+#pragma unroll
+                        for (int s = 0; s < S; ++s) acc[s] = fmaT(w, x[s], acc[s]);
+                    }
+                }
+            }
+#pragma unroll
+            for (int off2 = G / 2; off2 > 0; off2 >>= 1)
+#pragma unroll
+                for (int s = 0; s < S; ++s) acc[s] += __shfl_xor_sync(gmask, acc[s], off2, G);
+            if (lane == 0) sts_rec<T, S>(s_acc + size_t(r) * S, acc);
+        }
+        bar_named_consumers();
+        // epilogue, one thread per row, operands from shared memory
+        for (int r = tid; r < nrows; r += kGtpConsumers) {
+            const int4 mt = meta[r];   // entry range, source slot, history position, row
+            T acc[S];
+            lds_rec<T, S>(s_acc + size_t(r) * S, acc);
+            gtp_finish<T, S, STAGE>(a, mt.w, mt.y, mt.z, acc, ops, r);
+        }
+        bar_named_consumers();
+        if (tid == 0) mbar_arrive(&empty[b]);
+    }
+}
+
+// Row metadata of the pipelined tiles in tile order: entry range, source slot,
+// history position, row (the slots and positions of the direction's current set-up).
+__global__ void k_gtp_meta(int n, const int32_t *__restrict__ row, const int32_t *__restrict__ ent,
+                           const int32_t *__restrict__ slot, const int32_t *__restrict__ store_pos, int4 *__restrict__ meta)
+{
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= n) return;
+    const int q = row[r];
+    meta[r] = make_int4(ent[r], slot[q], store_pos[q], q);
+}
+
 template <typename T>
 __global__ void k_gt_values(int64_t nnz, const int32_t *__restrict__ perm, const T *__restrict__ src, T *__restrict__ dst)
 {
@@ -410,6 +685,9 @@ static int gt_build(hrn_ctx *c, int adj, size_t rec_bytes)
     std::vector<uint16_t> h_lidx;
     std::vector<int32_t> h_perm;
     std::vector<int32_t> h_runs;   // [nruns][4] staged index, matrix, first column, records
+    std::vector<int32_t> h_eruns;  // [n][4] first tile row, first row, rows: runs of consecutive rows of a tile
+    std::vector<int32_t> h_tinfo2; // [ntiles][4] first operand run, operand runs
+    int max_rows = 0;
     std::vector<uint32_t> keys;
     size_t smem = 0;
     bool fit = true;
@@ -452,6 +730,18 @@ static int gt_build(hrn_ctx *c, int adj, size_t rec_bytes)
         }
         const int32_t ti[8] = {gstart[g0], gstart[g1] - gstart[g0], int32_t(e0), int32_t(pad8(ne)),
                                int32_t(h_ukey.size()), int32_t(keys.size()), r0, int32_t(h_runs.size() / 4) - r0};
+        // runs of consecutive rows (equations) among the tile's rows, for the epilogue's operand copies
+        const int32_t er0 = int32_t(h_eruns.size() / 4);
+        for (int r = gstart[g0]; r < gstart[g1];) {
+            int r1 = r + 1;
+            while (r1 < gstart[g1] && order[r1] == order[r1 - 1] + 1) ++r1;
+            const int32_t er[4] = {r - gstart[g0], order[r], r1 - r, 0};
+            h_eruns.insert(h_eruns.end(), er, er + 4);
+            r = r1;
+        }
+        const int32_t ti2[4] = {er0, int32_t(h_eruns.size() / 4) - er0, 0, 0};
+        h_tinfo2.insert(h_tinfo2.end(), ti2, ti2 + 4);
+        max_rows = std::max(max_rows, gstart[g1] - gstart[g0]);
         h_tinfo.insert(h_tinfo.end(), ti, ti + 8);
         h_ukey.insert(h_ukey.end(), keys.begin(), keys.end());
     };
@@ -504,6 +794,11 @@ static int gt_build(hrn_ctx *c, int adj, size_t rec_bytes)
     HRN_CUDA(c, gs.d_lidx.alloc(h_lidx.size() * 2));
     HRN_CUDA(c, gs.d_perm.alloc(h_perm.size() * 4));
     HRN_CUDA(c, gs.d_runs.alloc(std::max<size_t>(h_runs.size(), 4) * 4));
+    HRN_CUDA(c, gs.d_eruns.alloc(std::max<size_t>(h_eruns.size(), 4) * 4));
+    HRN_CUDA(c, gs.d_tinfo2.alloc(std::max<size_t>(h_tinfo2.size(), 4) * 4));
+    HRN_CUDA(c, gs.d_meta.alloc(std::max<size_t>(order.size(), 1) * 16));
+    if (!h_eruns.empty()) HRN_CUDA(c, cudaMemcpy(gs.d_eruns.p, h_eruns.data(), h_eruns.size() * 4, cudaMemcpyHostToDevice));
+    if (!h_tinfo2.empty()) HRN_CUDA(c, cudaMemcpy(gs.d_tinfo2.p, h_tinfo2.data(), h_tinfo2.size() * 4, cudaMemcpyHostToDevice));
     if (!h_runs.empty()) HRN_CUDA(c, cudaMemcpy(gs.d_runs.p, h_runs.data(), h_runs.size() * 4, cudaMemcpyHostToDevice));
     if (!h_tinfo.empty()) HRN_CUDA(c, cudaMemcpy(gs.d_tinfo.p, h_tinfo.data(), h_tinfo.size() * 4, cudaMemcpyHostToDevice));
     if (!order.empty()) HRN_CUDA(c, cudaMemcpy(gs.d_row.p, order.data(), order.size() * 4, cudaMemcpyHostToDevice));
@@ -516,6 +811,7 @@ static int gt_build(hrn_ctx *c, int adj, size_t rec_bytes)
     gs.nu = int64_t(h_ukey.size());
     gs.nent = total;
     gs.nruns = int64_t(h_runs.size() / 4);
+    gs.max_rows = max_rows;
     gs.rec_bytes = rec_bytes;
     gs.val_version = -1;
     gs.built = true;
@@ -541,6 +837,21 @@ static int gt_values(hrn_ctx *c, int adj)
     return 0;
 }
 
+int gtp_prepare(hrn_ctx *c, int adj)
+{
+    GtSet &gs = c->gt[adj];
+    if (!gs.built) return set_error(c, HRN_ESTATE, "staged-gather tables not built");
+    if (gs.max_rows > kGtpRows) return set_error(c, HRN_EARG, "a tile has more rows than the pipelined tiles hold");
+    const int n = c->neq;
+    if (n == 0) return 0;
+    k_gtp_meta<<<(n + 255) / 256, 256, 0, c->stream>>>(n, gs.d_row.as<int32_t>(), gs.d_ent.as<int32_t>(),
+                                                       (adj ? c->d_slot_a : c->d_slot_f).as<int32_t>(),
+                                                       c->d_store_pos.as<int32_t>(), gs.d_meta.as<int4>());
+    ++c->launches;
+    HRN_CUDA(c, cudaGetLastError());
+    return 0;
+}
+
 int gt_ready(hrn_ctx *c, int adj)
 {
     if (!c->have_pattern || !c->have_operator) return set_error(c, HRN_ESTATE, "no operator");
@@ -561,6 +872,19 @@ static void launch_gt(const StageArgs<T> &a, const GtArgs<T> &g, int ntiles, siz
     static std::atomic<uint64_t> smem_done{0};
     smem_limit_once(rk4_stage_gt<T, S, STAGE, G, MAT, RUNS>, int(kGtBudget), smem_done);
     rk4_stage_gt<T, S, STAGE, G, MAT, RUNS><<<ntiles, kGtThreads, smem, st>>>(a, g);
+}
+
+template <typename T, int S, int STAGE, int G>
+static void launch_gtp(const StageArgs<T> &a, const GtpArgs<T> &g, int num_sms, cudaStream_t st)
+{
+    if constexpr ((S * sizeof(T)) % 16 == 0) {
+        static std::atomic<uint64_t> smem_done{0};
+        constexpr size_t smem = gtp_smem(S * sizeof(T));
+        smem_limit_once(rk4_stage_gtp<T, S, STAGE, G>, int(smem), smem_done);
+        const int per_sm = std::max(1, int((227 * 1024) / smem));
+        const int grid = std::min(g.ntiles, num_sms * per_sm);
+        rk4_stage_gtp<T, S, STAGE, G><<<grid, kGtpThreads, smem, st>>>(a, g);
+    }
 }
 
 template <typename T, int S, int STAGE>
@@ -594,10 +918,25 @@ static int gt_stage_t(hrn_ctx *c, const StageArgs<T> &a, int stage, int adj, int
         return set_error(c, HRN_ESTATE, "staged-gather tables not built");
     }
     if (gs.ntiles == 0) return 0;   // no rows
-    if ((variant == 46 || variant == 86) && (S * sizeof(T)) % 16 != 0) {
+    if ((variant == 46 || variant == 86 || variant == 47 || variant == 87) && (S * sizeof(T)) % 16 != 0) {
         static const int two = 2;
         cudaMemcpyAsync(c->d_step_err.p, &two, sizeof(int), cudaMemcpyHostToDevice, c->stream);
-        return set_error(c, HRN_EARG, "variants 46 / 86 need records of a multiple of 16 bytes");
+        return set_error(c, HRN_EARG, "variants 46, 47, 86, 87 need records of a multiple of 16 bytes");
+    }
+    if (variant == 47 || variant == 87) {
+        const GtpArgs<T> gp{gs.d_tinfo.as<int32_t>(), gs.d_tinfo2.as<int32_t>(), gs.d_meta.as<int4>(), gs.d_eruns.as<int4>(),
+                            gs.d_runs.as<int4>(), gs.d_lidx.as<uint16_t>(), gs.d_val.as<T>(), gs.ntiles, c->d_step_err.as<int>()};
+        switch (stage * 100 + variant) {
+        case 147: launch_gtp<T, S, 1, 4>(a, gp, c->num_sms, c->stream); break;
+        case 247: launch_gtp<T, S, 2, 4>(a, gp, c->num_sms, c->stream); break;
+        case 347: launch_gtp<T, S, 3, 4>(a, gp, c->num_sms, c->stream); break;
+        case 447: launch_gtp<T, S, 4, 4>(a, gp, c->num_sms, c->stream); break;
+        case 187: launch_gtp<T, S, 1, 8>(a, gp, c->num_sms, c->stream); break;
+        case 287: launch_gtp<T, S, 2, 8>(a, gp, c->num_sms, c->stream); break;
+        case 387: launch_gtp<T, S, 3, 8>(a, gp, c->num_sms, c->stream); break;
+        default: launch_gtp<T, S, 4, 8>(a, gp, c->num_sms, c->stream); break;
+        }
+        return 0;
     }
     const GtArgs<T> g{gs.d_tinfo.as<int4>(), gs.d_row.as<int32_t>(), gs.d_ent.as<int32_t>(), gs.d_ukey.as<uint32_t>(),
                       gs.d_lidx.as<uint16_t>(), gs.d_val.as<T>(), gs.d_runs.as<int4>(), c->d_step_err.as<int>()};

@@ -104,6 +104,10 @@ struct GtSet {
     DevBuf d_val;               // [nent] scaled values in tile order (T)
     DevBuf d_runs;              // [nruns][4] staged index, matrix, first column, records of each run of consecutive keys
     int64_t nruns = 0;
+    DevBuf d_eruns;             // [n][4] first tile row, first row, rows: runs of consecutive rows inside a tile
+    DevBuf d_tinfo2;            // [ntiles][4] first operand run, operand runs
+    DevBuf d_meta;              // [neq] int4 per tile row: entry range, source slot, history position, row (pipelined tiles)
+    int max_rows = 0;           // rows of the largest tile
     int64_t val_version = -1;   // value version d_val was built from
     size_t val_elem = 0;
 };
@@ -297,10 +301,13 @@ int face_force(hrn_ctx *c, const int32_t *nface);
 int finalize_pattern_from_keys(hrn_ctx *c, const std::vector<uint64_t> &keys);
 int vec_reduce(hrn_ctx *c, int kind, int n, const double *x, const double *y, double *out);
 int gt_ready(hrn_ctx *c, int adj);
+int gtp_prepare(hrn_ctx *c, int adj);
 int gt_stage(hrn_ctx *c, const void *stage_args, int stage, int adj, int variant);
-inline bool is_gt_variant(int v) { return v == 44 || v == 45 || v == 84 || v == 85 || v == 46 || v == 86; }
+inline bool is_gt_variant(int v) { return v == 44 || v == 45 || v == 84 || v == 85 || v == 46 || v == 86 || v == 47 || v == 87; }
+// pipelined staged tiles: persistent CTAs, producer warp, per-call row metadata
+inline bool is_gtp_variant(int v) { return v == 47 || v == 87; }
 // staged-gather variants whose records move by bulk copies: records of a multiple of 16 bytes
-inline bool gt_runs_valid(int v, int nshot, size_t elem) { return (v != 46 && v != 86) || (size_t(nshot) * elem) % 16 == 0; }
+inline bool gt_runs_valid(int v, int nshot, size_t elem) { return (v != 46 && v != 86 && v != 47 && v != 87) || (size_t(nshot) * elem) % 16 == 0; }
 int elem_prepare(hrn_ctx *c);
 int elem_ready(hrn_ctx *c);
 int elem_stage(hrn_ctx *c, const void *stage_args, int stage, int adj, int acc, int shots_per_thread, int mat);

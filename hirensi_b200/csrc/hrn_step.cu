@@ -873,8 +873,9 @@ static int autotune_lanes(hrn_ctx *c, StageArgs<T> a, T *X, T *Y, const TileArgs
     std::vector<int> cand;
     if (c->have_pattern) cand.assign(kVariants, kVariants + 10);   // none with a matrix-free operator
     if (c->have_pattern && gt_ready(c, adj) == 0)
-        for (int v : {44, 45, 84, 85, 46, 86})
-            if (gt_runs_valid(v, c->nshot, c->elem_bytes())) cand.push_back(v);
+        for (int v : {44, 45, 84, 85, 46, 86, 47, 87})
+            if (gt_runs_valid(v, c->nshot, c->elem_bytes()) && (!is_gtp_variant(v) || gtp_prepare(c, adj) == 0))
+                cand.push_back(v);
     if (c->op_from_mesh) {
         if (int rc = elem_ready(c)) return rc;
         for (int v : {90, 91, 92, 93, 94, 95, 100, 101, 102, 103, 104, 105})
@@ -1034,8 +1035,10 @@ static int forward_t(hrn_ctx *c)
         if (int rc = elem_ready(c)) return rc;
     } else if (is_gt_variant(c->lanes_f)) {
         if (!gt_runs_valid(c->lanes_f, c->nshot, c->elem_bytes()))
-            return set_error(c, HRN_EARG, "variants 46 / 86 need records (shots x value size) of a multiple of 16 bytes");
+            return set_error(c, HRN_EARG, "variants 46, 47, 86, 87 need records (shots x value size) of a multiple of 16 bytes");
         if (int rc = gt_ready(c, 0)) return rc;
+        if (is_gtp_variant(c->lanes_f))
+            if (int rc = gtp_prepare(c, 0)) return rc;
     }
     cudaEvent_t t0, t1;
     cudaEventCreate(&t0);
@@ -1139,11 +1142,16 @@ static int adjoint_t(hrn_ctx *c, int lambda_2mu, int keep_p)
         if (int rc = elem_ready(c)) return rc;
     } else if (is_gt_variant(c->lanes_a)) {
         if (!gt_runs_valid(c->lanes_a, c->nshot, c->elem_bytes()))
-            return set_error(c, HRN_EARG, "variants 46 / 86 need records (shots x value size) of a multiple of 16 bytes");
+            return set_error(c, HRN_EARG, "variants 46, 47, 86, 87 need records (shots x value size) of a multiple of 16 bytes");
         if (int rc = gt_ready(c, 1)) return rc;
+        if (is_gtp_variant(c->lanes_a))
+            if (int rc = gtp_prepare(c, 1)) return rc;
     }
-    if (c->ckpt > 0 && is_gt_variant(c->lanes_f))   // the recomputed forward segments
+    if (c->ckpt > 0 && is_gt_variant(c->lanes_f)) {   // the recomputed forward segments
         if (int rc = gt_ready(c, 0)) return rc;
+        if (is_gtp_variant(c->lanes_f))
+            if (int rc = gtp_prepare(c, 0)) return rc;
+    }
     cudaEvent_t t0, t1;
     cudaEventCreate(&t0);
     cudaEventCreate(&t1);
@@ -1326,6 +1334,8 @@ static int time_stage_t(hrn_ctx *c, int adj, int nsteps, double *avg_ms)
     } else if (is_gt_variant(lanes)) {
         if (!gt_runs_valid(lanes, c->nshot, c->elem_bytes())) return set_error(c, HRN_EARG, "variant needs 16-byte records");
         if (int rc = gt_ready(c, adj)) return rc;
+        if (is_gtp_variant(lanes))
+            if (int rc = gtp_prepare(c, adj)) return rc;
     }
     HRN_CUDA(c, cudaMemsetAsync(X0, 0, 6 * vn * sizeof(T), c->stream));
     launch_step<T, S>(c, a, X0, X1, nullptr, lanes, ta, adj);   // warm-up

@@ -1,10 +1,13 @@
-"""Staged-gather stage kernels (variants 44, 45, 84, 85, 46, 86) through the C ABI.
+"""Staged-gather stage kernels (variants 44-47, 84-87) through the C ABI.
 
 The rows are cut into compact tiles whose gathered stage inputs are loaded once
 into shared memory.  Entries keep their order inside a row, so with the same
 lane count and stage-input mode the row sums are those of the row-parallel
 kernel: 44 = 40, 45 = 41, 84 = 80, 85 = 81 bit for bit; 46 and 86 stage the same
-records by bulk copies of runs of consecutive columns, so 46 = 41 and 86 = 81.  Parity against the FP64
+records by bulk copies of runs of consecutive columns, so 46 = 41 and 86 = 81; 47 and 87
+run the same sums and epilogue in persistent CTAs whose producer warp moves each tile's
+data by bulk copies while the consumer warps work on the previous tile, so 47 = 41 and
+87 = 81.  Parity against the FP64
 oracle uses the bars of the other stage kernels (1e-10 FP64, 1e-4 FP32).
 """
 import numpy as np
@@ -143,7 +146,9 @@ def test_staged_tiles_odd_shot_counts(gpu_lib, nshot, precision):
 
 
 @pytest.mark.parametrize("nshot,precision,variant,row_parallel",
-                         [(2, "fp64", 46, 41), (4, "fp64", 86, 81), (4, "fp32", 46, 41), (8, "fp32", 86, 81)])
+                         [(2, "fp64", 46, 41), (4, "fp64", 86, 81), (4, "fp32", 46, 41), (8, "fp32", 86, 81),
+                          (2, "fp64", 47, 41), (4, "fp64", 47, 41), (4, "fp64", 87, 81), (4, "fp32", 47, 41),
+                          (8, "fp32", 87, 81)])
 def test_bulk_copied_runs_equal_row_parallel_kernel(gpu_lib, nshot, precision, variant, row_parallel):
     """Records of a multiple of 16 bytes moved by one bulk copy per run of
     consecutive columns: histories and adjoint histories equal the row-parallel
@@ -166,7 +171,8 @@ def test_bulk_copied_runs_equal_row_parallel_kernel(gpu_lib, nshot, precision, v
         assert np.array_equal(out[variant][1][k], out[row_parallel][1][k])
 
 
-def test_bulk_copied_runs_on_split_tiles(gpu_lib):
+@pytest.mark.parametrize("variant", [86, 87])
+def test_bulk_copied_runs_on_split_tiles(gpu_lib, variant):
     """Eight FP64 shots (64-byte records) on the 16 x 16 x 8 mesh: halved tiles, runs
     of 64-byte records; equal to the row-parallel kernel."""
     from hirensi_b200 import configs
@@ -175,7 +181,7 @@ def test_bulk_copied_runs_on_split_tiles(gpu_lib):
     prob = configs.inversion_config(nstep=12, shots=shots)
     m = prob.mesh
     hists = {}
-    for v in (86, 81):
+    for v in (variant, 81):
         with Solver("fp64") as s:
             s.set_mesh(m, RHO)
             s.assemble(prob.lam0, prob.mu0)
@@ -187,7 +193,7 @@ def test_bulk_copied_runs_on_split_tiles(gpu_lib):
             hists[v] = [s.history(k) for k in range(prob.nshot)]
     for k in range(prob.nshot):
         assert np.abs(hists[81][k]).max() > 0
-        assert np.array_equal(hists[86][k], hists[81][k])
+        assert np.array_equal(hists[variant][k], hists[81][k])
 
 
 def test_bulk_copied_runs_refuse_unaligned_records(gpu_lib):
@@ -203,3 +209,20 @@ def test_bulk_copied_runs_refuse_unaligned_records(gpu_lib):
     with _assembled_solver(p, p["lam"], p["mu"]) as s:
         s.forward()
         assert s.variant()[0] not in (46, 86)
+
+
+def test_pipelined_tiles_with_checkpointed_adjoint(gpu_lib):
+    """Variant 47 in the checkpointed adjoint, whose recomputed forward segments and
+    adjoint steps both run the pipelined tiles: the gradient equals variant 41's."""
+    p = tiny(nshot=4, nstep=90)
+    _, _, hist_t = oracle_forward(p, p["lam_t"], p["mu_t"])
+    dis = np.stack([traces_from_history(p, h) for h in hist_t])
+    g = {}
+    for v in (47, 41):
+        with _assembled_solver(p, p["lam"], p["mu"]) as s:
+            s.set_variant(v, v)
+            s.set_checkpointing(20)
+            s.forward()
+            g[v] = s.adjoint_gradient(dis)
+    assert np.abs(g[41][1]).max() > 0
+    assert np.array_equal(g[47][0], g[41][0]) and np.array_equal(g[47][1], g[41][1])

@@ -99,7 +99,7 @@ def test_gradient_fp32_within_1e4(gpu_lib):
         assert rel_l2(gm, gm_ref) < TOL32_GRAD
 
 
-@pytest.mark.parametrize("variant", [40, 80, 160, 41, 81, 161, 42, 43, 82, 83, 44, 45, 84, 85, 46, 86])
+@pytest.mark.parametrize("variant", [40, 80, 160, 41, 81, 161, 42, 43, 82, 83, 44, 45, 84, 85, 46, 86, 47, 87])
 def test_every_stage_kernel_variant_matches_oracle(gpu_lib, variant):
     p = tiny(nshot=2, nstep=120)
     _, _, hist_t = oracle_forward(p, p["lam_t"], p["mu_t"])
