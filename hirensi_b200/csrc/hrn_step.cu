@@ -873,9 +873,10 @@ static int autotune_lanes(hrn_ctx *c, StageArgs<T> a, T *X, T *Y, const TileArgs
     std::vector<int> cand;
     if (c->have_pattern) cand.assign(kVariants, kVariants + 10);   // none with a matrix-free operator
     if (c->have_pattern && gt_ready(c, adj) == 0)
-        for (int v : {44, 45, 84, 85, 46, 86, 47, 87})
-            if (gt_runs_valid(v, c->nshot, c->elem_bytes()) && (!is_gtp_variant(v) || gtp_prepare(c, adj) == 0))
-                cand.push_back(v);
+        // 47 / 87 (pipelined tiles) stay selectable but are not timed here: their many
+        // small bulk copies are limited by the copy engine's rate (about 2x slower)
+        for (int v : {44, 45, 84, 85, 46, 86})
+            if (gt_runs_valid(v, c->nshot, c->elem_bytes())) cand.push_back(v);
     if (c->op_from_mesh) {
         if (int rc = elem_ready(c)) return rc;
         for (int v : {90, 91, 92, 93, 94, 95, 100, 101, 102, 103, 104, 105})

@@ -423,6 +423,51 @@ def default_inversion_config():
     return InversionConfig(m_lbfgs=5, bounds_lambda=(10.0, 2000.0), bounds_mu=(10.0, 1000.0))
 
 
+def study_inversion_config(fac: float = 20.0, tv: bool = False):
+    """The inversion settings of the time-to-misfit comparison (bench.py's FWI legs):
+    L-BFGS memory 5, the reference's step rules with the lambda bias, Fac_Max_Update
+    `fac`, no TV regularization unless `tv` (with it the plain path stalls)."""
+    from .inversion import InversionConfig
+    return InversionConfig(m_lbfgs=5, bounds_lambda=(10.0, 2000.0), bounds_mu=(10.0, 1000.0),
+                           fac_max_update_lambda=fac, fac_max_update_mu=fac, regularization="TV" if tv else None)
+
+
+def _to_targets(h, targets):
+    """Iterations and wall time at which the misfit first fell by each target fraction."""
+    J0 = h[0]["misfit"]
+    out = {}
+    for r in targets:
+        hit = next((x for x in h if x["misfit"] <= (1.0 - r) * J0), None)
+        out[f"{int(round(r * 100))}pct"] = None if hit is None else {"iterations": hit["iter"], "wall_s": hit["wall_s"]}
+    return out
+
+
+def time_to_targets(runner: _Runner, dnet: DeviceNet, seeds, cap: int = 30, targets=(0.5, 0.9), cfg=None,
+                    unit_scale_seeds=()):
+    """Per held-out model: iterations and wall time to each misfit-reduction target for
+    plain L-BFGS and for the network's proposals (and the unit-scale ablation on
+    `unit_scale_seeds`), each run stopped at the last target or after `cap` iterations."""
+    cfg = cfg or study_inversion_config()
+    pre = LearnedPreconditioner(dnet, runner.prob.mesh, runner.rho)
+    rows = []
+    for sd in seeds:
+        rng = np.random.default_rng(int(sd))
+        lam_t, mu_t = random_true_model(runner.prob, rng)
+        runner.set_true(lam_t, mu_t)
+        row = {"seed": int(sd)}
+        runs = [("plain", None), ("learned", pre)]
+        if int(sd) in set(int(x) for x in unit_scale_seeds):
+            runs.append(("unit_scale", UnitScale()))
+        for name, p in runs:
+            h = runner.fwi(cap, cfg=cfg, preconditioner=p, target_reduction=max(targets))
+            row[name] = {"reduction": 1.0 - h[-1]["misfit"] / h[0]["misfit"], "iterations": len(h) - 1,
+                         "wall_s": h[-1]["wall_s"], **_to_targets(h, targets)}
+            if p is not None:
+                row[name]["accepted"] = int(sum(1 for x in h[1:] if x.get("learned")))
+        rows.append(row)
+    return rows
+
+
 def generate_samples(runner: _Runner, seeds, iters: int = 3, log=None, inputs: int = 4):
     """(x, q, dm) of the first `iters` iterations of a plain inversion of each seeded model."""
     out = []
@@ -495,10 +540,41 @@ def main(argv=None):
     ap.add_argument("--eval-only", help="skip training: evaluate these weights")
     ap.add_argument("--inputs", type=int, choices=[4, 6], default=6,
                     help="input channels: 4 = gradients, illumination, Vs; 6 = also the pseudo-Hessian diagonals")
+    ap.add_argument("--study", help="held-out study of these weights: time to 50 %% and 90 %% misfit reduction "
+                                    "(writes a .json beside the weights with the suffix _study)")
+    ap.add_argument("--study-models", type=int, default=32)
+    ap.add_argument("--study-cap", type=int, default=30)
+    ap.add_argument("--fac", type=float, default=20.0, help="Fac_Max_Update of the study's inversions")
     a = ap.parse_args(argv)
     t0 = time.time()
     prob = inversion_config(nstep=a.nstep)
     runner = _Runner(prob, "fp32")
+    if a.study:
+        dnet = DeviceNet(Net.load(a.study), runner.lat.shape)
+        seeds = list(range(5000, 5000 + a.study_models))
+        rows = time_to_targets(runner, dnet, seeds, cap=a.study_cap, cfg=study_inversion_config(a.fac),
+                               unit_scale_seeds=seeds[:8])
+
+        def med(key, tgt, field):
+            v = [r[key][tgt][field] for r in rows if r[key].get(tgt)]
+            return (float(np.median(v)) if v else None), len(v)
+        summary = {"models": len(rows), "cap": a.study_cap, "fac_max_update": a.fac, "precision": "fp32",
+                   "mesh": "16x16x8 + PML 3, 4 shots, 2000 steps", "lattice": list(runner.lat.shape)}
+        for key in ("plain", "learned"):
+            for tgt in ("50pct", "90pct"):
+                (mi, n), (mw, _) = med(key, tgt, "iterations"), med(key, tgt, "wall_s")
+                summary[f"{key}_{tgt}"] = {"reached": n, "median_iterations": mi, "median_wall_s": mw}
+        both = [r for r in rows if r["plain"].get("90pct") and r["learned"].get("90pct")]
+        summary["median_speedup_to_90pct"] = (float(np.median([r["plain"]["90pct"]["wall_s"] / r["learned"]["90pct"]["wall_s"]
+                                                               for r in both])) if both else None)
+        both50 = [r for r in rows if r["plain"].get("50pct") and r["learned"].get("50pct")]
+        summary["median_speedup_to_50pct"] = (float(np.median([r["plain"]["50pct"]["wall_s"] / r["learned"]["50pct"]["wall_s"]
+                                                               for r in both50])) if both50 else None)
+        summary["rows"] = rows
+        with open(a.study.replace(".npz", "_study.json"), "w") as f:
+            json.dump(summary, f, indent=1)
+        print(json.dumps({k: v for k, v in summary.items() if k != "rows"}), flush=True)
+        return
     if a.eval_only:
         dnet = DeviceNet(Net.load(a.eval_only), runner.lat.shape)
         for g in fwi_gain(runner, dnet, range(5000, 5000 + a.eval_models), a.fwi_iters):
