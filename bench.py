@@ -98,6 +98,10 @@ def measured_peaks():
 def stage_kernel_name(variant: int):
     """Kernel of a stage variant (FP64, 4 shots) and the committed ncu summary holding
     its DRAM traffic per launch."""
+    if variant in (46, 86):
+        return "rk4_stage_gt<double,4,runs>", "rk4_stage_gt46_fp64_inversion.md"
+    if variant in (47, 87):
+        return "rk4_stage_gtp<double,4>", "rk4_stage_gtp_fp64_inversion.md"
     if variant in (44, 45, 84, 85):
         return "rk4_stage_gt<double,4>", "rk4_stage_gt_fp64_inversion.md"
     if variant in (42, 43, 82, 83):
