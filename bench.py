@@ -64,12 +64,13 @@ def parse_args():
                     help="stage-kernel variant for forward and adjoint (0 = chosen by timing on first use)")
     ap.add_argument("--no-graphs", action="store_true",
                     help="launch every kernel directly instead of replaying the captured time loops")
-    ap.add_argument("--workload", choices=["inversion", "uneven", "xl", "shot-scaling"], default="inversion",
+    ap.add_argument("--workload", choices=["inversion", "uneven", "xl", "xl-fwi", "shot-scaling"], default="inversion",
                     help="inversion: the 16x16x8 plain inversion loop (default); uneven: batched uneven "
                          "shots on the 80x80x40 + PML 4 mesh, FP32 stepping, checkpointed adjoint; "
                          "xl: the same on the 160x160x80 + PML 6 mesh (86.6 M equations) with the "
-                         "matrix-free operator; shot-scaling: stage-kernel time per shot for 1, 2, 4 and 8 "
-                         "shots per pass over the 80x80x40 + PML 4 operator (FP32)")
+                         "matrix-free operator; xl-fwi: inversion iterations on that mesh (8 shots in two "
+                         "batches, records scaled by --length-scale); shot-scaling: stage-kernel time per shot "
+                         "for 1, 2, 4 and 8 shots per pass over the 80x80x40 + PML 4 operator (FP32)")
     ap.add_argument("--max-batches", type=int, default=0, help="uneven / xl: time at most this many batches")
     ap.add_argument("--length-scale", type=float, default=0.03,
                     help="uneven workload: record lengths scaled by this factor (a bounded sample)")
@@ -511,15 +512,10 @@ def run_uneven(args, rank, world, local_rank):
     dev = torch.device("cuda", local_rank)
     t_setup = time.perf_counter()
     if args.workload == "xl":
-        # 8 shots of 6000-8000 steps and 2500 receivers; dt at 0.15 of the GLL-spacing
-        # CFL limit of the fastest P wave of the model distribution (Vs 600, nu 0.40).
         # The CSR of this mesh would exceed the 2^31 entry range: C, K, G are applied
         # element by element.  Four FP32 shots per batch hold about 40 GB of segment
         # history (50 steps) and 25 GB of checkpoints.
-        vp_max = 600.0 * np.sqrt(2.0 * (1.0 - 0.40) / (1.0 - 2.0 * 0.40))
-        dt = 0.15 * (0.5 * 2.5) / vp_max
-        prob = uneven_config(nx=160, ny=160, nz=80, npml=6, nshot=8, dt=dt, lengths=(6000, 8000),
-                             receivers=(2500, 2500), length_scale=args.length_scale)
+        prob = xl_problem(args.length_scale)
         per_batch, ckpt = 4, 50
     else:
         prob = uneven_config(length_scale=args.length_scale)
@@ -648,6 +644,98 @@ def run_uneven(args, rank, world, local_rank):
     if args.workload == "xl" and args.xl_error_steps > 0:
         result["fp32_error_vs_fp64"] = xl_error(prob, args.xl_error_steps, local_rank)
     return result
+
+
+def xl_problem(length_scale):
+    """The extra-large workload: 160x160x80 + PML 6, 8 shots of 6000-8000 steps scaled by
+    length_scale, 2500 receivers, dt at 0.15 of the GLL-spacing CFL limit of the model
+    distribution's fastest P wave (Vs 600 m/s, nu 0.40)."""
+    from hirensi_b200.configs import uneven_config
+    vp_max = 600.0 * np.sqrt(2.0 * (1.0 - 0.40) / (1.0 - 2.0 * 0.40))
+    dt = 0.15 * (0.5 * 2.5) / vp_max
+    return uneven_config(nx=160, ny=160, nz=80, npml=6, nshot=8, dt=dt, lengths=(6000, 8000),
+                         receivers=(2500, 2500), length_scale=length_scale)
+
+
+def run_xl_fwi(args, local_rank):
+    """Inversion iterations on the extra-large mesh: the seeded model (layers + ellipsoidal
+    inclusions) is the true model, its depth average (each level's mean lambda and mu) the
+    initial one; 8 shots in two batches of four (hirensi_b200.inversion.BatchedBackend),
+    FP32 stepping with FP64 reductions and L-BFGS, matrix-free operator, checkpointed
+    adjoint; L-BFGS memory 5, the reference's step rules, Fac_Max_Update 20, no TV."""
+    import torch
+    from hirensi_b200 import batching as B
+    from hirensi_b200 import build
+    from hirensi_b200.configs import extend_into_pml
+    from hirensi_b200.inversion import FWI, BatchedBackend, InversionConfig
+    from hirensi_b200.solver import Solver
+    build.build()
+    torch.cuda.set_device(local_rank)
+    t_setup = time.perf_counter()
+    prob = xl_problem(args.length_scale)
+    m = prob.mesh
+    zlev = np.round(m.xyz[:, 2] / 1.25).astype(np.int64)
+    _, inv = np.unique(zlev, return_inverse=True)
+    cnt = np.bincount(inv)
+    lam0 = extend_into_pml(m, (np.bincount(inv, prob.lam) / cnt)[inv])
+    mu0 = extend_into_pml(m, (np.bincount(inv, prob.mu) / cnt)[inv])
+    lengths = [sh.nstep for sh in prob.shots]
+    plan = B.plan(lengths, 4)
+    sv = Solver("fp32", device=local_rank)
+    sv.set_mesh(m, prob.rho_el)
+    sv.set_operator_mode(True)
+    sv.assemble(prob.lam, prob.mu)
+    sv.set_history(m.store_eq)
+    sv.set_checkpointing(max(10, max(lengths) // 4))
+    shots = list(prob.shots)
+    for ids in plan:                        # measured data: the true model's traces
+        b = B.pack(shots, ids)
+        B.configure(sv, b, prob.dt, m.store_position)
+        sv.forward()
+        for k, tr in zip(ids, B.unpack_traces(b, sv.traces())):
+            sh = shots[k]
+            shots[k] = B.Shot(sh.src_eq, sh.src_b, sh.ftab, sh.eqdis, tr)
+    batches = [B.pack(shots, ids) for ids in plan]
+    cfg = InversionConfig(m_lbfgs=5, bounds_lambda=(1.0, 5000.0), bounds_mu=(1.0, 2000.0), regularization=None,
+                          fac_max_update_lambda=20.0, fac_max_update_mu=20.0)
+    backend = BatchedBackend(sv, m, batches, prob.dt, m.store_position)
+    torch.cuda.synchronize()
+    setup_s = time.perf_counter() - t_setup
+    clk = ClockSampler(local_rank)
+    clk.start()
+    t0 = time.perf_counter()
+    fwi = FWI(backend, cfg)
+    failed = None
+    try:
+        hist = fwi.run(lam0, mu0, n_iter=args.fwi_iters)
+    except RuntimeError as exc:     # ArmijoFailure: the reference would STOP here
+        hist, failed = fwi.hist, str(exc)
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    clocks = clk.stop()
+    J0 = hist[0]["misfit"]
+    rd = m.node_mat_id == 0
+    err = {}
+    if failed is None:
+        mu_f = fwi.mu.cpu().numpy()
+        err = {"mu_rel_l2_error": float(np.linalg.norm((mu_f - prob.mu)[rd]) / np.linalg.norm(prob.mu[rd])),
+               "mu_rel_l2_error_initial": float(np.linalg.norm((mu0 - prob.mu)[rd]) / np.linalg.norm(prob.mu[rd]))}
+    sv.close()
+    out = {"metric": "FWI iterations on the extra-large mesh", "unit": "s", "value": wall, "higher_is_better": False,
+           "n_gpus": 1, "dtype": "f32 stepping, f64 reductions and L-BFGS", "data": "synthetic (seeded true model)",
+           "config": {"workload": prob.name.replace("_8shots", "") + "_fwi", "equations": m.neq, "dof": prob.dof,
+                      "nodes": m.nj, "shots": len(shots), "batches": len(batches),
+                      "record_lengths": [min(lengths), max(lengths)], "length_scale": args.length_scale,
+                      "receivers_per_shot": 2500, "operator": "matrix-free",
+                      "inversion": "L-BFGS memory 5, reference step rules, Fac_Max_Update 20, no TV; initial model = "
+                                   "depth average of the true model"},
+           "iterations": len(hist) - 1, "armijo_trials": [h["armijo"] for h in hist[1:]],
+           "misfit_history": [h["misfit"] / J0 for h in hist], "misfit_reduction": 1.0 - hist[-1]["misfit"] / J0,
+           "setup_s": setup_s, "clocks": clocks}
+    if failed:
+        out["armijo_failure"] = failed
+    out.update(err)
+    return out
 
 
 def run_shot_scaling(args, local_rank):
@@ -903,6 +991,8 @@ def main():
         res = run_reference(args, rank, world)
     elif args.workload in ("uneven", "xl"):
         res = run_uneven(args, rank, world, local_rank)
+    elif args.workload == "xl-fwi":
+        res = run_xl_fwi(args, local_rank) if rank == 0 else None
     elif args.workload == "shot-scaling":
         res = run_shot_scaling(args, local_rank) if rank == 0 else None
     else:

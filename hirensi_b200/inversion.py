@@ -337,3 +337,55 @@ class DeviceBackend:
             self._ck(self.L.hrn_pseudo_hessian(self.h, C.c_void_p(self._p(out[0])), C.c_void_p(self._p(out[1]))))
             h = out.cpu().numpy()
         return h[0], h[1]
+
+
+class BatchedBackend(DeviceBackend):
+    """DeviceBackend over many shots advanced in batches on one context: the misfit of a
+    model is the sum over batches (each batch configured in turn, hirensi_b200.batching),
+    and the gradient the sum of the batches' adjoint gradients.  The batch left resident by
+    the last misfit evaluation takes its adjoint first; the others run their forward again
+    before their adjoint (with checkpointing this is the usual recompute).  The reference
+    solves one source per call and sums over its sources the same way
+    (S4/Program_Main.F90:379-470).  batches: packed batches with their measured data
+    (Batch.dis, [nshot][nrec3][nstep+1]); store_position maps receiver equations to
+    history positions (Mesh.store_position)."""
+
+    def __init__(self, solver, mesh, batches, dt, store_position, device=None):
+        super().__init__(solver, mesh, device)
+        self.batches = batches
+        self.dt = dt
+        self.store_position = store_position
+        self.resident = None
+        self._g = self.torch.zeros(2, self.n, dtype=self.torch.float64, device=self.dev)
+
+    def _use(self, k):
+        from . import batching
+        b = self.batches[k]
+        batching.configure(self.s, b, self.dt, self.store_position)
+        self.s.set_data(b.dis)
+        self.resident = k
+
+    def forward(self, lam, mu):
+        self.s.assemble_device(self._p(lam), self._p(mu))
+        J = 0.0
+        for k in range(len(self.batches)):
+            self._use(k)
+            self.s.forward()
+            J += self.s.misfit(None)
+        return J
+
+    def gradient(self, g_l, g_m):
+        order = list(range(len(self.batches)))
+        if self.resident is not None:
+            order.remove(self.resident)
+            order.insert(0, self.resident)
+        self.axpby(0.0, g_l, 0.0, None, g_l)
+        self.axpby(0.0, g_m, 0.0, None, g_m)
+        for i, k in enumerate(order):
+            if i > 0:
+                self._use(k)
+                self.s.forward()
+            self.s.adjoint_gradient(None, to_host=False)
+            self.s.gradient_device(self._p(self._g[0]), self._p(self._g[1]))
+            self.axpby(1.0, g_l, 1.0, self._g[0], g_l)
+            self.axpby(1.0, g_m, 1.0, self._g[1], g_m)

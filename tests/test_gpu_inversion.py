@@ -105,3 +105,37 @@ def test_fwi_iterations_match_the_reference_rules(gpu_lib, tv):
     assert rel_l2(fwi.lam.cpu().numpy(), ref[-1]["lam"]) < 1e-9
     assert rel_l2(fwi.mu.cpu().numpy(), ref[-1]["mu"]) < 1e-9
     s.close()
+
+
+def test_batched_backend_equals_one_batch(gpu_lib):
+    """FWI over shots advanced in two batches (hirensi_b200.inversion.BatchedBackend) equals
+    FWI with all shots in one batch: the misfit and the gradient are sums over shots, only
+    the order of the gradient sum changes."""
+    from hirensi_b200 import batching as B
+    from hirensi_b200.inversion import BatchedBackend
+    from hirensi_b200.solver import Solver
+    p = tiny(nshot=4, nstep=120)
+    _, _, hist_t = oracle_forward(p, p["lam_t"], p["mu_t"])
+    dis = [traces_from_history(p, h) for h in hist_t]
+    cfg = InversionConfig(m_lbfgs=5, bounds_lambda=(10.0, 1000.0), bounds_mu=(10.0, 1000.0), regularization=None)
+    s = _device(p, dis)
+    one = FWI(DeviceBackend(s, p["mesh"]), cfg)
+    h1 = one.run(p["lam"], p["mu"], n_iter=3)
+    lam1, mu1 = one.lam.cpu().numpy(), one.mu.cpu().numpy()
+    s.close()
+    shots = [B.Shot(np.array([p["src_eq"][k]], np.int32), np.ones(1), p["ftab"][k], p["eqdis"], dis[k]) for k in range(4)]
+    batches = [B.pack(shots, ids) for ids in ([0, 1], [2, 3])]
+    for b in batches:
+        assert b.dis is not None and b.dis.shape[0] == 2
+    sb = Solver("fp64")
+    sb.set_mesh(p["mesh"], RHO)
+    sb.assemble(p["lam"], p["mu"])
+    sb.set_history(p["mesh"].store_eq)
+    two = FWI(BatchedBackend(sb, p["mesh"], batches, p["dt"], p["mesh"].store_position), cfg)
+    h2 = two.run(p["lam"], p["mu"], n_iter=3)
+    assert [h["armijo"] for h in h1] == [h["armijo"] for h in h2]
+    for a, b in zip(h1, h2):
+        assert abs(a["misfit"] - b["misfit"]) <= 1e-10 * b["misfit"]
+    assert h2[-1]["misfit"] < h2[0]["misfit"]
+    assert rel_l2(two.lam.cpu().numpy(), lam1) < 1e-9 and rel_l2(two.mu.cpu().numpy(), mu1) < 1e-9
+    sb.close()
