@@ -126,6 +126,56 @@ __device__ __forceinline__ void lds_rec(const T *p, T (&o)[S])
     }
 }
 
+// 32-byte staged records placed with their two 16-byte halves swapped when bit 2 of
+// the record's index is set.  Eight lanes reading eight random records then spread over
+// all eight 16-byte bank groups instead of the four even (or odd) ones, which cuts the
+// shared-memory bank conflicts of the row sums; the values and the order of the sums
+// are unchanged.
+template <typename T, int S>
+constexpr bool kSwizzleRec = (S * sizeof(T)) == 32;
+
+__device__ __forceinline__ uint32_t rec_swz(uint32_t idx) { return ((idx >> 2) & 1u) * 16u; }
+
+template <typename T, int S>
+__device__ __forceinline__ void sts_rec_swz(T *base, uint32_t idx, const T (&v)[S])
+{
+    if constexpr (kSwizzleRec<T, S>) {
+        char *rec = reinterpret_cast<char *>(base) + size_t(idx) * 32;
+        const uint32_t sw = rec_swz(idx);
+        const T *lo = v, *hi = v + S / 2;
+        if constexpr (sizeof(T) == 8) {
+            *reinterpret_cast<double2 *>(rec + sw) = make_double2(lo[0], lo[1]);
+            *reinterpret_cast<double2 *>(rec + (16u ^ sw)) = make_double2(hi[0], hi[1]);
+        } else {
+            *reinterpret_cast<float4 *>(rec + sw) = make_float4(lo[0], lo[1], lo[2], lo[3]);
+            *reinterpret_cast<float4 *>(rec + (16u ^ sw)) = make_float4(hi[0], hi[1], hi[2], hi[3]);
+        }
+    } else {
+        sts_rec<T, S>(base + size_t(idx) * S, v);
+    }
+}
+
+template <typename T, int S>
+__device__ __forceinline__ void lds_rec_swz(const T *base, uint32_t idx, T (&o)[S])
+{
+    if constexpr (kSwizzleRec<T, S>) {
+        const char *rec = reinterpret_cast<const char *>(base) + size_t(idx) * 32;
+        const uint32_t sw = rec_swz(idx);
+        if constexpr (sizeof(T) == 8) {
+            const double2 a = *reinterpret_cast<const double2 *>(rec + sw);
+            const double2 b = *reinterpret_cast<const double2 *>(rec + (16u ^ sw));
+            o[0] = a.x; o[1] = a.y; o[2] = b.x; o[3] = b.y;
+        } else {
+            const float4 a = *reinterpret_cast<const float4 *>(rec + sw);
+            const float4 b = *reinterpret_cast<const float4 *>(rec + (16u ^ sw));
+            o[0] = a.x; o[1] = a.y; o[2] = a.z; o[3] = a.w;
+            o[4] = b.x; o[5] = b.y; o[6] = b.z; o[7] = b.w;
+        }
+    } else {
+        lds_rec<T, S>(base + size_t(idx) * S, o);
+    }
+}
+
 // Stage input of matrix TAG at row j (same values as the gathers of rk4_stage).
 template <typename T, int S, int STAGE, int MAT>
 __device__ __forceinline__ void staged_input(const StageArgs<T> &a, uint32_t key, T (&v)[S])
@@ -213,9 +263,15 @@ __global__ void __launch_bounds__(kGtThreads) rk4_stage_gt(const StageArgs<T> a,
                     const int tag = int(key[q] >> kTagBits);
                     const T *src = (tag == 0 ? a.in_m : (tag == 1 ? a.in_t : a.in_h)) + size_t(key[q] & kColMask) * S;
                     T *d = sx + size_t(uu) * S;
+                    if constexpr (kSwizzleRec<T, S>) {
+                        const uint32_t sw = rec_swz(uint32_t(uu));
+                        cp_async16(reinterpret_cast<char *>(d) + sw, reinterpret_cast<const char *>(src));
+                        cp_async16(reinterpret_cast<char *>(d) + (16u ^ sw), reinterpret_cast<const char *>(src) + 16);
+                    } else {
 #pragma unroll
-                    for (size_t b = 0; b < kRec; b += 16)
-                        cp_async16(reinterpret_cast<char *>(d) + b, reinterpret_cast<const char *>(src) + b);
+                        for (size_t b = 0; b < kRec; b += 16)
+                            cp_async16(reinterpret_cast<char *>(d) + b, reinterpret_cast<const char *>(src) + b);
+                    }
                 }
             }
         }
@@ -234,7 +290,7 @@ __global__ void __launch_bounds__(kGtThreads) rk4_stage_gt(const StageArgs<T> a,
 #pragma unroll
             for (int q = 0; q < Q; ++q) {
                 const int uu = u + q * kGtThreads;
-                if (uu < nu) sts_rec<T, S>(sx + size_t(uu) * S, v[q]);
+                if (uu < nu) sts_rec_swz<T, S>(sx, uint32_t(uu), v[q]);
             }
         }
     }
@@ -263,7 +319,8 @@ __global__ void __launch_bounds__(kGtThreads) rk4_stage_gt(const StageArgs<T> a,
                 const int kk = k + uu * G;
                 if (kk < k3) {
                     T x[S];
-                    lds_rec<T, S>(sx + size_t(s_lidx[kk]) * S, x);
+                    if constexpr (RUNS) lds_rec<T, S>(sx + size_t(s_lidx[kk]) * S, x);   // bulk copies keep the plain layout
+                    else lds_rec_swz<T, S>(sx, s_lidx[kk], x);
                     const T w = s_val[kk];
 #pragma unroll
                     for (int s = 0; s < S; ++s) acc[s] = fmaT(w, x[s], acc[s]);
