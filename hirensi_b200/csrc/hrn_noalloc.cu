@@ -16,6 +16,7 @@
 #include <mutex>
 
 #include "hrn_internal.h"
+#include "hrn_misfit.cuh"
 
 namespace hrn {
 
@@ -35,32 +36,15 @@ __global__ void k_noalloc_terms(int nshot, int nstep, int nstore, int nrec3, int
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= (nstep + 1) * nshot) return;
     const int s = t % nshot, n = t / nshot;
-    double d = 0.0;
-    // uneven shots: nothing past the shot's record length, masked receivers skipped
-    for (int sl = 0; sl < nslot && !(shot_nstep && n > shot_nstep[s]); ++sl) {
-        double r = 0.0;
-        for (int k = ptr[sl]; k < ptr[sl + 1]; ++k) {
-            const int q = qlist[k];
-            if (mask && !mask[size_t(s) * nrec3 + q]) continue;
-            r += double(hist[(size_t(n) * nstore + emap[q]) * nshot + s]) - dis[(size_t(s) * nrec3 + q) * (nstep + 1) + n];
-        }
-        d += r * r;
-    }
-    terms[size_t(s) * (nstep + 1) + n] = d;
+    terms[size_t(s) * (nstep + 1) + n] =
+        misfit_term<T>(nshot, s, n, nstep, nstore, nrec3, nslot, ptr, qlist, emap, hist, dis, shot_nstep, mask);
 }
 
 // cost[0] = total, cost[1 + s] = shot s; the reference's order n = nstep..1
 __global__ void k_noalloc_sum(int nshot, int nstep, double dt, const double *__restrict__ terms, double *__restrict__ cost)
 {
     if (blockIdx.x != 0 || threadIdx.x != 0) return;
-    double total = 0.0;
-    for (int s = 0; s < nshot; ++s) {
-        double c = 0.0;
-        for (int n = nstep; n >= 1; --n) c = c + 0.5 * terms[size_t(s) * (nstep + 1) + n] * dt;
-        cost[1 + s] = c;
-        total += c;
-    }
-    cost[0] = total;
+    misfit_sum(nshot, nstep, dt, terms, cost);
 }
 
 // Device address of the scratch array, looked up once per device with that
