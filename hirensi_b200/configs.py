@@ -116,8 +116,20 @@ def inversion_config(nstep: int = 2000, dt: float = 1.0e-4, fr: float = 15.0, nx
     ft = time_table(nstep, dt, 2, fr)
     rec = surface_grid(mesh, list(receivers))
     eqdis = mesh.equations(rec)
-    return Problem("inversion_16x16x8_pml3", mesh, lam_t, mu_t, lam0, mu0, nstep, dt, src_eq,
+    return Problem(f"inversion_{nx}x{ny}x{nz}_pml{npml}", mesh, lam_t, mu_t, lam0, mu0, nstep, dt, src_eq,
                    np.eye(len(src_eq)), np.stack([ft] * len(src_eq)), eqdis, mesh.store_position(eqdis))
+
+
+def training_config(nstep: int = 2000) -> Problem:
+    """The learned preconditioner's training-mesh workload: the inversion
+    configuration's model distribution on 40 x 40 x 20 hexahedra (100 x 100 x 50 m)
+    plus a 3-element PML (2.08 M equations), 8 vertical Ricker forces on a 3 x 3
+    surface grid without its centre (25 m apart), 7 x 7 surface receivers 12.5 m
+    apart; 15 Hz, dt = 1e-4 s."""
+    g = (-25.0, 0.0, 25.0)
+    shots = tuple((x, y) for y in g for x in g if (x, y) != (0.0, 0.0))
+    return inversion_config(nstep=nstep, nx=40, ny=40, nz=20, shots=shots,
+                            receivers=(-37.5, -25.0, -12.5, 0.0, 12.5, 25.0, 37.5))
 
 
 def forward_config(nstep: int = 2000) -> Problem:

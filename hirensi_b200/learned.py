@@ -443,10 +443,11 @@ def _to_targets(h, targets):
 
 
 def time_to_targets(runner: _Runner, dnet: DeviceNet, seeds, cap: int = 30, targets=(0.5, 0.9), cfg=None,
-                    unit_scale_seeds=()):
+                    unit_scale_seeds=(), on_row=None):
     """Per held-out model: iterations and wall time to each misfit-reduction target for
     plain L-BFGS and for the network's proposals (and the unit-scale ablation on
-    `unit_scale_seeds`), each run stopped at the last target or after `cap` iterations."""
+    `unit_scale_seeds`), each run stopped at the last target or after `cap` iterations.
+    on_row(rows), if given, sees the rows so far after each model."""
     cfg = cfg or study_inversion_config()
     pre = LearnedPreconditioner(dnet, runner.prob.mesh, runner.rho)
     rows = []
@@ -465,6 +466,8 @@ def time_to_targets(runner: _Runner, dnet: DeviceNet, seeds, cap: int = 30, targ
             if p is not None:
                 row[name]["accepted"] = int(sum(1 for x in h[1:] if x.get("learned")))
         rows.append(row)
+        if on_row:
+            on_row(rows)
     return rows
 
 
@@ -527,7 +530,7 @@ def main(argv=None):
     import json
     import time
     import torch
-    from .configs import inversion_config
+    from .configs import inversion_config, training_config
     ap = argparse.ArgumentParser(description="train the learned gradient preconditioner on solver-generated data")
     ap.add_argument("--out", required=True, help="weights file (.npz); a .json summary is written beside it")
     ap.add_argument("--models", type=int, default=48)
@@ -536,7 +539,7 @@ def main(argv=None):
     ap.add_argument("--epochs", type=int, default=60)
     ap.add_argument("--lr", type=float, default=2e-3)
     ap.add_argument("--nstep", type=int, default=2000)
-    ap.add_argument("--fwi-iters", type=int, default=10)
+    ap.add_argument("--fwi-iters", type=int, default=10, help="iterations of the after-training comparison (0: none)")
     ap.add_argument("--eval-only", help="skip training: evaluate these weights")
     ap.add_argument("--inputs", type=int, choices=[4, 6], default=6,
                     help="input channels: 4 = gradients, illumination, Vs; 6 = also the pseudo-Hessian diagonals")
@@ -545,34 +548,44 @@ def main(argv=None):
     ap.add_argument("--study-models", type=int, default=32)
     ap.add_argument("--study-cap", type=int, default=30)
     ap.add_argument("--fac", type=float, default=20.0, help="Fac_Max_Update of the study's inversions")
+    ap.add_argument("--mesh", choices=["16x16x8", "40x40x20"], default="16x16x8",
+                    help="16x16x8: the inversion configuration (4 shots); 40x40x20: the training mesh of the "
+                         "learned-preconditioner configuration (8 shots, configs.training_config)")
+    ap.add_argument("--unit-scale-models", type=int, default=8, help="held-out models that also run the D = 1 ablation")
+    ap.add_argument("--study-out", help="summary file of --study (default: beside the weights, suffix _study)")
     a = ap.parse_args(argv)
     t0 = time.time()
-    prob = inversion_config(nstep=a.nstep)
+    prob = inversion_config(nstep=a.nstep) if a.mesh == "16x16x8" else training_config(nstep=a.nstep)
     runner = _Runner(prob, "fp32")
     if a.study:
         dnet = DeviceNet(Net.load(a.study), runner.lat.shape)
         seeds = list(range(5000, 5000 + a.study_models))
-        rows = time_to_targets(runner, dnet, seeds, cap=a.study_cap, cfg=study_inversion_config(a.fac),
-                               unit_scale_seeds=seeds[:8])
+        out = a.study_out or a.study.replace(".npz", "_study.json")
 
-        def med(key, tgt, field):
-            v = [r[key][tgt][field] for r in rows if r[key].get(tgt)]
-            return (float(np.median(v)) if v else None), len(v)
-        summary = {"models": len(rows), "cap": a.study_cap, "fac_max_update": a.fac, "precision": "fp32",
-                   "mesh": "16x16x8 + PML 3, 4 shots, 2000 steps", "lattice": list(runner.lat.shape)}
-        for key in ("plain", "learned"):
+        def summarize(rows):
+            def med(key, tgt, field):
+                v = [r[key][tgt][field] for r in rows if r[key].get(tgt)]
+                return (float(np.median(v)) if v else None), len(v)
+            summary = {"models": len(rows), "cap": a.study_cap, "fac_max_update": a.fac, "precision": "fp32",
+                       "mesh": f"{prob.name}, {len(prob.src_eq)} shots, {prob.nstep} steps",
+                       "lattice": list(runner.lat.shape)}
+            for key in ("plain", "learned"):
+                for tgt in ("50pct", "90pct"):
+                    (mi, n), (mw, _) = med(key, tgt, "iterations"), med(key, tgt, "wall_s")
+                    summary[f"{key}_{tgt}"] = {"reached": n, "median_iterations": mi, "median_wall_s": mw}
             for tgt in ("50pct", "90pct"):
-                (mi, n), (mw, _) = med(key, tgt, "iterations"), med(key, tgt, "wall_s")
-                summary[f"{key}_{tgt}"] = {"reached": n, "median_iterations": mi, "median_wall_s": mw}
-        both = [r for r in rows if r["plain"].get("90pct") and r["learned"].get("90pct")]
-        summary["median_speedup_to_90pct"] = (float(np.median([r["plain"]["90pct"]["wall_s"] / r["learned"]["90pct"]["wall_s"]
-                                                               for r in both])) if both else None)
-        both50 = [r for r in rows if r["plain"].get("50pct") and r["learned"].get("50pct")]
-        summary["median_speedup_to_50pct"] = (float(np.median([r["plain"]["50pct"]["wall_s"] / r["learned"]["50pct"]["wall_s"]
-                                                               for r in both50])) if both50 else None)
-        summary["rows"] = rows
-        with open(a.study.replace(".npz", "_study.json"), "w") as f:
-            json.dump(summary, f, indent=1)
+                both = [r for r in rows if r["plain"].get(tgt) and r["learned"].get(tgt)]
+                summary[f"median_speedup_to_{tgt}"] = (
+                    float(np.median([r["plain"][tgt]["wall_s"] / r["learned"][tgt]["wall_s"] for r in both]))
+                    if both else None)
+            summary["rows"] = rows
+            with open(out, "w") as f:
+                json.dump(summary, f, indent=1)
+            return summary
+
+        rows = time_to_targets(runner, dnet, seeds, cap=a.study_cap, cfg=study_inversion_config(a.fac),
+                               unit_scale_seeds=seeds[:a.unit_scale_models], on_row=summarize)
+        summary = summarize(rows)
         print(json.dumps({k: v for k, v in summary.items() if k != "rows"}), flush=True)
         return
     if a.eval_only:
@@ -588,11 +601,12 @@ def main(argv=None):
     t_train = time.time() - t0 - t_data
     ev_net, ev_one = evaluate(dnet, eval_s)
     dnet.net.save(a.out)
-    gains = fwi_gain(runner, dnet, range(5000, 5000 + a.eval_models), a.fwi_iters)
+    gains = fwi_gain(runner, dnet, range(5000, 5000 + a.eval_models), a.fwi_iters) if a.fwi_iters > 0 else []
     summary = {"train_samples": len(train_s), "eval_samples": len(eval_s), "epochs": a.epochs,
                "loss_first_epoch": hist[0], "loss_last_epoch": hist[-1], "eval_loss_network": ev_net,
                "eval_loss_unscaled_gradient": ev_one, "fwi": gains, "data_s": t_data, "train_s": t_train,
-               "nstep": a.nstep, "shape": list(runner.lat.shape), "inputs": a.inputs}
+               "nstep": a.nstep, "shape": list(runner.lat.shape), "inputs": a.inputs,
+               "mesh": f"{prob.name}, {len(prob.src_eq)} shots, {prob.nstep} steps"}
     with open(a.out.replace(".npz", ".json"), "w") as f:
         json.dump(summary, f, indent=1)
     print(json.dumps({k: v for k, v in summary.items() if k != "fwi"}), flush=True)

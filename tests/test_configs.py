@@ -32,3 +32,15 @@ def test_inversion_config_inputs():
         assert dof == 2 and p.mesh.xyz[node, 2] == 0.0
     assert len(p.eqdis) == 3 * 25
     assert np.all(p.mesh.xyz[np.unique(np.nonzero(np.isin(p.mesh.ID[:, :3], p.eqdis))[0]), 2] == 0.0)
+
+
+def test_training_config_sizes():
+    """The learned preconditioner's training mesh: 40 x 40 x 20 + PML 3 with the sizes
+    of the configuration table (48,668 elements, 406,503 nodes, 807,003 displacement
+    DOF), 8 surface shots and the 7 x 7 receiver grid."""
+    p = configs.training_config(nstep=20)
+    m = p.mesh
+    assert m.nel == 48668 and m.nj == 406503 and p.dof == 807003
+    assert p.nshot == 8 and len(p.eqdis) == 3 * 49
+    assert p.name == "inversion_40x40x20_pml3"
+    assert np.all(m.xyz[np.unique(np.nonzero(np.isin(m.ID[:, 2], p.src_eq))[0]), 2] == 0.0)
