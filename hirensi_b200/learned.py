@@ -471,11 +471,15 @@ def time_to_targets(runner: _Runner, dnet: DeviceNet, seeds, cap: int = 30, targ
     return rows
 
 
-def generate_samples(runner: _Runner, seeds, iters: int = 3, log=None, inputs: int = 4):
-    """(x, q, dm) of the first `iters` iterations of a plain inversion of each seeded model."""
+def generate_samples(runner: _Runner, seeds, iters: int = 3, log=None, inputs: int = 4, budget_s=None):
+    """(x, q, dm) of the first `iters` iterations of a plain inversion of each seeded model;
+    with budget_s, no further model is started once that many seconds have passed."""
+    import time
     out = []
-    nj = runner.prob.mesh.nj
+    t0 = time.perf_counter()
     for sd in seeds:
+        if budget_s is not None and time.perf_counter() - t0 > budget_s:
+            break
         rng = np.random.default_rng(int(sd))
         lam_t, mu_t = random_true_model(runner.prob, rng)
         runner.set_true(lam_t, mu_t)
@@ -553,6 +557,7 @@ def main(argv=None):
                          "learned-preconditioner configuration (8 shots, configs.training_config)")
     ap.add_argument("--unit-scale-models", type=int, default=8, help="held-out models that also run the D = 1 ablation")
     ap.add_argument("--study-out", help="summary file of --study (default: beside the weights, suffix _study)")
+    ap.add_argument("--data-budget-s", type=float, help="start no further training model after this many seconds")
     a = ap.parse_args(argv)
     t0 = time.time()
     prob = inversion_config(nstep=a.nstep) if a.mesh == "16x16x8" else training_config(nstep=a.nstep)
@@ -593,7 +598,8 @@ def main(argv=None):
         for g in fwi_gain(runner, dnet, range(5000, 5000 + a.eval_models), a.fwi_iters):
             print(g, flush=True)
         return
-    train_s = generate_samples(runner, range(1000, 1000 + a.models), a.iters, inputs=a.inputs)
+    train_s = generate_samples(runner, range(1000, 1000 + a.models), a.iters, inputs=a.inputs,
+                               budget_s=a.data_budget_s, log=lambda m: print(m, flush=True))
     eval_s = generate_samples(runner, range(5000, 5000 + a.eval_models), a.iters, inputs=a.inputs)
     t_data = time.time() - t0
     dnet = DeviceNet(Net(seed=0, inputs=a.inputs), runner.lat.shape)
