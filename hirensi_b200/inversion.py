@@ -39,6 +39,12 @@ class InversionConfig:
     armijo_rho: float = 0.5
     iter_begin: int = 1
     search: str = "LBFGS"             # 'LBFGS' or 'SD'
+    # line search of a preconditioner's proposal (no reference counterpart): 'wolfe' =
+    # Armijo and the weak curvature condition, expanding a too-short step; 'armijo' =
+    # one sufficient-decrease test
+    proposal_search: str = "wolfe"
+    wolfe_c2: float = 0.9
+    wolfe_expansions: int = 2
 
 
 class ArmijoFailure(RuntimeError):
@@ -48,9 +54,22 @@ class ArmijoFailure(RuntimeError):
 class FWI:
     """preconditioner: optional object with ``direction(backend, g_l, g_m, lam, mu)``
     returning a proposed update direction (``hirensi_b200.learned.LearnedPreconditioner``).
-    Each iteration tries it first with one Armijo test on the true misfit.  If the test
-    fails, the model is restored and the iteration takes the reference's L-BFGS path
-    unchanged."""
+    Each iteration tries it first with a line search on the true misfit in FP64
+    (``cfg.proposal_search``):
+
+    * the first trial takes the step that moves no node by more than Fac_Max_Update;
+    * a trial must pass the Armijo test J(m + s) <= J(m) + c1 g.s; if the first does
+      not, the model is restored and the iteration takes the reference's L-BFGS path
+      unchanged;
+    * with 'wolfe', a trial that passes also needs the weak curvature condition
+      g(m + s).s >= c2 g.s, with the gradient at the trial point (the next iteration's
+      gradient, kept for it).  A trial that fails it has stopped short of the
+      curvature, and the step doubles, at most ``wolfe_expansions`` times.  If a
+      doubled step fails the Armijo test, the last trial that passed it stands.
+
+    g is the gradient of the iteration as the reference forms it (sign flip, TV when on,
+    gradient-mass scaling), and the trial's gradient gets the same treatment without the
+    TV term."""
 
     def __init__(self, backend, cfg: InversionConfig, preconditioner=None):
         self.b = backend
@@ -68,6 +87,9 @@ class FWI:
         p_l, p_m = b.zeros(), b.zeros()
         reg_l, reg_m = b.zeros(), b.zeros()
         tmp = b.zeros()
+        raw_l, raw_m = b.zeros(), b.zeros()      # raw gradient of a proposal's trial point
+        keep_l, keep_m = b.zeros(), b.zeros()    # the same, kept while the step doubles
+        have_raw = False
         img, restriction = b.gradient_mass_inverse()
         b.lbfgs_setup(cfg.m_lbfgs, restriction)
         fac_l, fac_m = cfg.fac_max_update_lambda, cfg.fac_max_update_mu
@@ -101,7 +123,12 @@ class FWI:
             J_pre = J
             b.copy(g_l, g_l_pre)
             b.copy(g_m, g_m_pre)
-            b.gradient(g_l, g_m)                 # raw accumulated gradient of the current forward
+            if have_raw:                         # computed by the proposal's line search
+                b.copy(raw_l, g_l)
+                b.copy(raw_m, g_m)
+                have_raw = False
+            else:
+                b.gradient(g_l, g_m)             # raw accumulated gradient of the current forward
             b.axpby(-1.0, g_l, 0.0, None, g_l)   # :412-413
             b.axpby(-1.0, g_m, 0.0, None, g_m)
             cost_rl = cost_rm = 0.0
@@ -154,26 +181,70 @@ class FWI:
             if chk_m and cfg.search == "LBFGS":
                 a_m = a_m_sd
             learned = False
+            search = {}
             if self.pre is not None:
                 q_l, q_m = self.pre.direction(b, g_l, g_m, lam, mu)
                 gq_l, gq_m = b.dot(g_l, q_l), b.dot(g_m, q_m)
                 if gq_l < 0.0 and gq_m < 0.0:
                     al = fac_l / b.norminf(q_l)
                     am = fac_m / b.norminf(q_m)
-                    b.axpby(al, q_l, 1.0, lam_pre, lam)
-                    b.axpby(am, q_m, 1.0, mu_pre, mu)
-                    b.extend(lam)
-                    b.extend(mu)
-                    b.clip(lam, *cfg.bounds_lambda)
-                    b.clip(mu, *cfg.bounds_mu)
-                    J_try = b.forward(lam, mu)
-                    if J_try <= J_pre + cfg.armijo_c * (al * gq_l + am * gq_m):   # sufficient decrease (g.q < 0)
-                        learned, J, a_l, a_m = True, J_try, al, am
+
+                    def place(scale):
+                        b.axpby(scale * al, q_l, 1.0, lam_pre, lam)
+                        b.axpby(scale * am, q_m, 1.0, mu_pre, mu)
+                        b.extend(lam)
+                        b.extend(mu)
+                        b.clip(lam, *cfg.bounds_lambda)
+                        b.clip(mu, *cfg.bounds_mu)
+
+                    wolfe = cfg.proposal_search == "wolfe"
+                    slope0 = al * gq_l + am * gq_m            # g.s of the first trial (< 0)
+                    best = None                               # (scale, J, curvature met)
+                    trials = 0
+                    for k in range(cfg.wolfe_expansions + 1 if wolfe else 1):
+                        scale = float(2 ** k)
+                        place(scale)
+                        J_try = b.forward(lam, mu)
+                        trials += 1
+                        if J_try > J_pre + cfg.armijo_c * scale * slope0:   # sufficient decrease
+                            break
+                        if not wolfe:
+                            best = (scale, J_try, None)
+                            break
+                        b.gradient(raw_l, raw_m)              # the trial point's gradient
+                        b.axpby(-1.0, raw_l, 0.0, None, tmp)
+                        b.mul(tmp, img, tmp)
+                        d_l = b.dot(tmp, q_l)
+                        b.axpby(-1.0, raw_m, 0.0, None, tmp)
+                        b.mul(tmp, img, tmp)
+                        d_m = b.dot(tmp, q_m)
+                        curv = scale * (al * d_l + am * d_m) >= cfg.wolfe_c2 * scale * slope0
+                        best = (scale, J_try, curv)
+                        if curv:
+                            break
+                        b.copy(raw_l, keep_l)
+                        b.copy(raw_m, keep_m)
+                    if best is not None:
+                        scale, J_best, curv = best
+                        if scale != float(2 ** (trials - 1)):
+                            # a doubled step failed the Armijo test: back to the last trial that
+                            # passed it, with its forward state for the next iteration's inputs
+                            place(scale)
+                            J_best = b.forward(lam, mu)
+                            b.copy(keep_l, raw_l)
+                            b.copy(keep_m, raw_m)
+                        learned, J, a_l, a_m = True, J_best, scale * al, scale * am
+                        have_raw = wolfe
+                        search = {"trials": trials, "scale": scale}
+                        if wolfe:
+                            search["curvature"] = bool(curv)
+                    else:
+                        search = {"trials": trials}
             if learned:
                 count = 0
-                rec_extra = {"learned": True}
+                rec_extra = {"learned": True, "search": search}
             else:
-                rec_extra = {"learned": False} if self.pre is not None else {}
+                rec_extra = {"learned": False, "search": search} if self.pre is not None else {}
                 update(a_l, a_m, it)
                 J = b.forward(lam, mu)
             armijo = cfg.armijo_c * abs(a_m) * gp_m + cfg.armijo_c * abs(a_l) * gp_l
