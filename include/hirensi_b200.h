@@ -189,8 +189,8 @@ int hrn_misfit(hrn_ctx *ctx, const double *dis_meas, double *cost);
  * shared by every context and call in the process, so nothing is allocated.
  * Limit: nshot * (nstep + 1) <= 131072, larger problems return HRN_EARG.  The
  * first call on a device looks the array's address up (cudaGetSymbolAddress)
- * with that device current and keeps it; make that first call before any stream
- * capture, and do not use the entry across a cudaDeviceReset.  Calls whose
+ * with that device current and keeps it; do not use the entry across a
+ * cudaDeviceReset.  Calls whose
  * kernels overlap on one GPU (other streams, other contexts, other host threads)
  * race on the scratch: serialize them.  It synchronizes its stream and returns
  * once *cost is ready. */
