@@ -363,15 +363,18 @@ class LearnedPreconditioner:
 
 def random_true_model(prob, rng):
     """A model of the inversion configuration's distribution: three layers with
-    Vs 200 / 300 / 400 m/s (each +-10 %, interfaces +-2 m) and a Gaussian Vs anomaly
-    of +-20..40 % (radius 3..7 m) at a random position in the regular domain."""
+    Vs 200 / 300 / 400 m/s (each +-10 %, interfaces at 7.5 and 15 m +-2 m) and a
+    Gaussian Vs anomaly of +-20..40 % (radius 3..7 m) at a random position in the
+    regular domain.  Lengths are those of the configuration's 20 m deep box and
+    scale with the depth of a deeper one (the training mesh: 50 m, factor 2.5)."""
     from .configs import extend_into_pml, layered_vs, vs_to_lame
     m = prob.mesh
-    vs_l = np.array([200.0, 300.0, 400.0]) * (1.0 + rng.uniform(-0.1, 0.1, 3))
-    vs = layered_vs(m, tuple(vs_l), (-7.5 + rng.uniform(-2, 2), -15.0 + rng.uniform(-2, 2)))
     (x0, x1), (y0, y1), (z0, _) = m.rd_box
+    f = -z0 / 20.0
+    vs_l = np.array([200.0, 300.0, 400.0]) * (1.0 + rng.uniform(-0.1, 0.1, 3))
+    vs = layered_vs(m, tuple(vs_l), (f * (-7.5 + rng.uniform(-2, 2)), f * (-15.0 + rng.uniform(-2, 2))))
     c = np.array([rng.uniform(0.7 * x0, 0.7 * x1), rng.uniform(0.7 * y0, 0.7 * y1), rng.uniform(0.8 * z0, 0.2 * z0)])
-    r = rng.uniform(3.0, 7.0)
+    r = f * rng.uniform(3.0, 7.0)
     amp = rng.choice([-1.0, 1.0]) * rng.uniform(0.2, 0.4)
     d2 = ((m.xyz - c) ** 2).sum(axis=1)
     vs = extend_into_pml(m, vs * (1.0 + amp * np.exp(-d2 / (r * r))))
