@@ -875,7 +875,7 @@ def fwi_leg(precision, prob, dis, local_rank, iters, learned=False, target=None,
            "time_to_50pct_s": t_half, "iterations_to_50pct": it_half,
            "misfit_initial": J0, "misfit_final": J, "misfit_reduction": 1.0 - J / J0,
            "misfit_history": [h["misfit"] for h in hist],
-           "forward_solves": sum(1 + h["armijo"] + (1 if h.get("learned") is False else 0) for h in hist[1:]) + 1,
+           "forward_solves": hist[-1]["forward_solves"], "adjoint_solves": hist[-1]["adjoint_solves"],
            "config": f"L-BFGS memory 5, {'TV regularization' if tv else 'no regularization'}, reference step "
                      f"rules (lambda bias on), Fac_Max_Update {fac}, bounds lambda [10,2000] mu [10,1000]",
            "warmup": "one inversion iteration (tables, buffers, captured time loops) before the timed inversion", **err}
@@ -883,6 +883,9 @@ def fwi_leg(precision, prob, dis, local_rank, iters, learned=False, target=None,
         out["armijo_failure"] = failed
     if learned:
         out["learned_steps_accepted"] = int(sum(1 for h in hist[1:] if h.get("learned")))
+        out["proposal_search"] = {"trials": [h["search"].get("trials", 0) for h in hist[1:]],
+                                  "curvature_met": [h["search"].get("curvature") for h in hist[1:]],
+                                  "rule": "weak Wolfe (Armijo c1 1e-4, curvature c2 0.9, up to two doublings)"}
         out["weights"] = os.path.relpath(PRECOND_WEIGHTS, ROOT)
     if target is not None:
         out["target_reduction"] = target

@@ -81,6 +81,15 @@ class FWI:
         gradient before the direction is chosen."""
         b, cfg = self.b, self.cfg
         n = b.n
+        solves = {"forward": 0, "adjoint": 0}    # forward runs and adjoint runs with the gradient
+
+        def fwd(lam_, mu_):
+            solves["forward"] += 1
+            return b.forward(lam_, mu_)
+
+        def grad(gl_, gm_):
+            solves["adjoint"] += 1
+            b.gradient(gl_, gm_)
         lam, mu = b.vec(lam0), b.vec(mu0)
         lam_pre, mu_pre = b.zeros(), b.zeros()
         g_l, g_m, g_l_pre, g_m_pre = b.zeros(), b.zeros(), b.zeros(), b.zeros()
@@ -94,10 +103,10 @@ class FWI:
         b.lbfgs_setup(cfg.m_lbfgs, restriction)
         fac_l, fac_m = cfg.fac_max_update_lambda, cfg.fac_max_update_mu
         t0 = time.perf_counter()
-        J = b.forward(lam, mu)
+        J = fwd(lam, mu)
         J0 = J
         hist = [dict(iter=0, misfit=J, cost=J, reg_lambda=0.0, reg_mu=0.0, g_lambda=0.0, g_mu=0.0, armijo=0,
-                     wall_s=time.perf_counter() - t0)]
+                     wall_s=time.perf_counter() - t0, forward_solves=1, adjoint_solves=0)]
         self.hist = hist   # kept up to date, also when an ArmijoFailure ends the run
         if log:
             log(hist[-1])
@@ -128,7 +137,7 @@ class FWI:
                 b.copy(raw_m, g_m)
                 have_raw = False
             else:
-                b.gradient(g_l, g_m)             # raw accumulated gradient of the current forward
+                grad(g_l, g_m)             # raw accumulated gradient of the current forward
             b.axpby(-1.0, g_l, 0.0, None, g_l)   # :412-413
             b.axpby(-1.0, g_m, 0.0, None, g_m)
             cost_rl = cost_rm = 0.0
@@ -204,14 +213,14 @@ class FWI:
                     for k in range(cfg.wolfe_expansions + 1 if wolfe else 1):
                         scale = float(2 ** k)
                         place(scale)
-                        J_try = b.forward(lam, mu)
+                        J_try = fwd(lam, mu)
                         trials += 1
                         if J_try > J_pre + cfg.armijo_c * scale * slope0:   # sufficient decrease
                             break
                         if not wolfe:
                             best = (scale, J_try, None)
                             break
-                        b.gradient(raw_l, raw_m)              # the trial point's gradient
+                        grad(raw_l, raw_m)              # the trial point's gradient
                         b.axpby(-1.0, raw_l, 0.0, None, tmp)
                         b.mul(tmp, img, tmp)
                         d_l = b.dot(tmp, q_l)
@@ -230,7 +239,7 @@ class FWI:
                             # a doubled step failed the Armijo test: back to the last trial that
                             # passed it, with its forward state for the next iteration's inputs
                             place(scale)
-                            J_best = b.forward(lam, mu)
+                            J_best = fwd(lam, mu)
                             b.copy(keep_l, raw_l)
                             b.copy(keep_m, raw_m)
                         learned, J, a_l, a_m = True, J_best, scale * al, scale * am
@@ -246,7 +255,7 @@ class FWI:
             else:
                 rec_extra = {"learned": False, "search": search} if self.pre is not None else {}
                 update(a_l, a_m, it)
-                J = b.forward(lam, mu)
+                J = fwd(lam, mu)
             armijo = cfg.armijo_c * abs(a_m) * gp_m + cfg.armijo_c * abs(a_l) * gp_l
             count = 0
             while not learned and J > J_pre + armijo:            # :737-896
@@ -259,13 +268,14 @@ class FWI:
                 if count == 9:
                     a_l, a_m = -a_l, -a_m
                 update(a_l, a_m, it)
-                J = b.forward(lam, mu)
+                J = fwd(lam, mu)
                 armijo = cfg.armijo_c * abs(a_m) * gp_m + cfg.armijo_c * abs(a_l) * gp_l
                 if count == 10:
                     raise ArmijoFailure(f"Armijo condition failure at iteration {it}")
             rec = dict(iter=it, misfit=J, cost=J + cost_rl + cost_rm, reg_lambda=cost_rl, reg_mu=cost_rm,
                        g_lambda=b.norm2(g_l), g_mu=b.norm2(g_m), armijo=count, alpha_lambda=a_l, alpha_mu=a_m,
-                       wall_s=time.perf_counter() - t0, **rec_extra)
+                       wall_s=time.perf_counter() - t0, forward_solves=solves["forward"],
+                       adjoint_solves=solves["adjoint"], **rec_extra)
             hist.append(rec)
             if log:
                 log(rec)

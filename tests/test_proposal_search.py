@@ -82,6 +82,7 @@ def test_short_proposal_doubles_until_the_curvature_condition_holds():
     assert np.allclose(fwi.lam, p.start[0] + 0.16 * (p.lt - p.start[0]), rtol=1e-13, atol=0)
     # one forward for J0 and one per trial; one gradient for iteration 1, one per trial
     assert b.forwards == 1 + 3 and b.gradients == 1 + 3
+    assert (h[-1]["forward_solves"], h[-1]["adjoint_solves"]) == (b.forwards, b.gradients)
 
 
 def test_accepted_proposal_hands_its_gradient_to_the_next_iteration():
