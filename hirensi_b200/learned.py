@@ -263,6 +263,64 @@ class DeviceNet:
         return gws, gbs
 
 
+def conv_bench(shape, reps: int = 20, inputs: int = 6, seed: int = 0) -> dict:
+    """Device time of the network's convolutions on a lattice of `shape` (nz, ny, nx):
+    the four forward layers, then the four backward layers (data and weight
+    gradients), each timed over `reps` back-to-back passes with CUDA events on the
+    network's stream, activations resident on the device.  The calls go through the C
+    ABI, and each one reads its kernels' error flag back (a stream synchronization),
+    so the times include that round trip.  The tensor cores run every
+    layer at 16 input and 16 output channels; `tflops_mma` counts those MMAs,
+    `tflops_useful` only the layers' real channel counts."""
+    import torch
+    net = Net(seed=seed, inputs=inputs)
+    dn = DeviceNet(net, tuple(shape))
+    rng = np.random.default_rng(seed)
+    dn.forward(rng.standard_normal((net.ch[0],) + tuple(shape)))        # activations of a real input
+    nz, ny, nx = shape
+    V = dn.V
+    CH = net.ch
+    t = torch
+    gy = [t.from_numpy(rng.standard_normal(16 * V).astype(np.float32)).to(dn.dev) for _ in range(4)]
+    gx = [t.zeros(16 * V, dtype=t.float32, device=dn.dev) for _ in range(4)]
+    gw = [t.zeros(CH[i + 1] * CH[i] * 27, dtype=t.float32, device=dn.dev) for i in range(4)]
+    gb = [t.zeros(CH[i + 1], dtype=t.float32, device=dn.dev) for i in range(4)]
+    stream = torch.cuda.ExternalStream(dn.stream) if dn.stream else torch.cuda.current_stream(dn.dev)
+
+    def fwd():
+        for i in range(4):
+            dn._ck(dn.L.hrn_cnn_conv3d_forward(CH[i], CH[i + 1], nz, ny, nx, C.c_void_p(dn.act[i].data_ptr()),
+                                               C.c_void_p(dn.wd[i].data_ptr()), C.c_void_p(dn.bd[i].data_ptr()),
+                                               int(i < 3), C.c_void_p(dn.act[i + 1].data_ptr()), C.c_void_p(dn.stream)))
+
+    def bwd():
+        for i in range(3, -1, -1):
+            dn._ck(dn.L.hrn_cnn_conv3d_backward(CH[i], CH[i + 1], nz, ny, nx, C.c_void_p(dn.act[i].data_ptr()),
+                                                C.c_void_p(dn.wd[i].data_ptr()), C.c_void_p(dn.act[i + 1].data_ptr()),
+                                                int(i < 3), C.c_void_p(gy[i].data_ptr()),
+                                                C.c_void_p(gx[i].data_ptr() if i > 0 else 0),
+                                                C.c_void_p(gw[i].data_ptr()), C.c_void_p(gb[i].data_ptr()),
+                                                C.c_void_p(dn.stream)))
+
+    out = {"shape": list(shape), "voxels": V, "channels": list(CH), "reps": reps}
+    for name, fn, passes in (("forward", fwd, [1, 1, 1, 1]), ("backward", bwd, [1, 2, 2, 2])):
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / reps
+        # backward: the weight gradient of every layer, the data gradient of layers 1-3
+        useful = sum(2.0 * V * 27 * CH[i] * CH[i + 1] * passes[i] for i in range(4))
+        mma = sum(2.0 * V * 27 * 16 * 16 * passes[i] for i in range(4))
+        out[name] = {"ms": ms, "tflops_useful": useful / (ms * 1e-3) / 1e12, "tflops_mma": mma / (ms * 1e-3) / 1e12}
+    return out
+
+
 def scale_from_z(z: np.ndarray) -> np.ndarray:
     return np.exp(np.clip(z, -ZCLIP, ZCLIP))
 
@@ -561,8 +619,12 @@ def main(argv=None):
     ap.add_argument("--unit-scale-models", type=int, default=8, help="held-out models that also run the D = 1 ablation")
     ap.add_argument("--study-out", help="summary file of --study (default: beside the weights, suffix _study)")
     ap.add_argument("--data-budget-s", type=float, help="start no further training model after this many seconds")
+    ap.add_argument("--conv-bench", help="only time the convolutions on a lattice NZxNYxNX (e.g. 41x81x81)")
     a = ap.parse_args(argv)
     t0 = time.time()
+    if a.conv_bench:
+        print(json.dumps(conv_bench(tuple(int(v) for v in a.conv_bench.split("x")), inputs=a.inputs)), flush=True)
+        return
     prob = inversion_config(nstep=a.nstep) if a.mesh == "16x16x8" else training_config(nstep=a.nstep)
     runner = _Runner(prob, "fp32")
     if a.study:
