@@ -597,7 +597,7 @@ def main(argv=None):
     import torch
     from .configs import inversion_config, training_config
     ap = argparse.ArgumentParser(description="train the learned gradient preconditioner on solver-generated data")
-    ap.add_argument("--out", required=True, help="weights file (.npz); a .json summary is written beside it")
+    ap.add_argument("--out", help="weights file of a training run (.npz); a .json summary is written beside it")
     ap.add_argument("--models", type=int, default=48)
     ap.add_argument("--eval-models", type=int, default=6)
     ap.add_argument("--iters", type=int, default=3)
@@ -663,6 +663,8 @@ def main(argv=None):
         for g in fwi_gain(runner, dnet, range(5000, 5000 + a.eval_models), a.fwi_iters):
             print(g, flush=True)
         return
+    if not a.out:
+        ap.error("training needs --out")
     train_s = generate_samples(runner, range(1000, 1000 + a.models), a.iters, inputs=a.inputs,
                                budget_s=a.data_budget_s, log=lambda m: print(m, flush=True))
     eval_s = generate_samples(runner, range(5000, 5000 + a.eval_models), a.iters, inputs=a.inputs)
