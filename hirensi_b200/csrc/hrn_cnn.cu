@@ -43,16 +43,6 @@ struct Grid {
     __host__ __device__ int size() const { return nz * ny * nx; }
 };
 
-// voxel index of the neighbour of v at tap k (9 dz + 3 dy + dx, each 0..2), offset
-// multiplied by sign; -1 outside the grid
-__device__ __forceinline__ int neighbour(const Grid &g, int v, int k, int sign)
-{
-    const int x = v % g.nx, y = (v / g.nx) % g.ny, z = v / (g.nx * g.ny);
-    const int zz = z + sign * (k / 9 - 1), yy = y + sign * ((k / 3) % 3 - 1), xx = x + sign * (k % 3 - 1);
-    if (zz < 0 || zz >= g.nz || yy < 0 || yy >= g.ny || xx < 0 || xx >= g.nx) return -1;
-    return (zz * g.ny + yy) * g.nx + xx;
-}
-
 __device__ __forceinline__ uint32_t smem_u32(const void *p) { return uint32_t(__cvta_generic_to_shared(p)); }
 
 // Shared-memory matrix descriptor, no swizzle: start address, leading-dimension
@@ -136,6 +126,15 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&o)[16])
     for (int i = 0; i < 16; ++i) o[i] = __uint_as_float(r[i]);
 }
 
+// 16-byte asynchronous copy global -> shared; valid = false writes 16 zero bytes and
+// reads nothing (source size 0)
+__device__ __forceinline__ void cp_async16_zfill(void *dst, const void *src, bool valid)
+{
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(smem_u32(dst)), "l"(src), "r"(valid ? 16 : 0)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
 __device__ __forceinline__ uint32_t pack2(float a, float b)
 {
     const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
@@ -165,18 +164,41 @@ __device__ __forceinline__ uint4 channels8(const void *src, const __nv_bfloat16 
     }
 }
 
+// B operand of every tap in the canonical layout, written once per call into
+// global memory (27 x 512 bytes) for the tiles to copy: core matrix (n / 8, k / 8)
+// at ((n / 8) * 2 + k / 8) * 128, row n % 8.  Forward: B_tap[n = co][k = ci];
+// data gradient: B_tap[n = ci][k = co].
+template <bool GRAD>
+__global__ void k_conv_pack_b(int cin, int cout, const __nv_bfloat16 *__restrict__ w, unsigned char *__restrict__ bpack)
+{
+    const int nrow = GRAD ? cin : cout, ncol = GRAD ? cout : cin;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < 27 * kC * kC; i += gridDim.x * blockDim.x) {
+        const int tap = i / (kC * kC), n = (i / kC) % kC, k = i % kC;
+        __nv_bfloat16 val = __float2bfloat16_rn(0.f);
+        if (n < nrow && k < ncol) {
+            const int co = GRAD ? k : n, ci = GRAD ? n : k;
+            val = w[(size_t(co) * cin + ci) * 27 + tap];
+        }
+        *reinterpret_cast<__nv_bfloat16 *>(bpack + tap * 512 + ((n >> 3) * 2 + (k >> 3)) * 128 + (n & 7) * 16 + (k & 7) * 2) = val;
+    }
+}
+
 // Forward (GRAD = false) and data gradient (GRAD = true) of one 128-voxel tile.
 //   forward: src = x (BF16 [V][16]), B_tap[n = co][k = ci] = w[co][ci][tap], out = y (BF16 [V][16]);
 //   data gradient: src = gy (FP32 [V][16]) masked by y, B_tap[n = ci][k = co] = w[co][ci][tap],
 //   neighbour offset negated, out = gx (FP32 [V][16]).
-// Shared memory: B for all taps (27 x 512 B), A for the taps of one round (9 x 4 KB).
+// Shared memory: B for all taps (27 x 512 B, copied from the packed operand), A for the
+// taps of one round (9 x 4 KB).  Thread m stages voxel v0 + m for every tap: its grid
+// coordinates are computed once, and a quarter-warp's 16-byte stores fill one
+// contiguous 128-byte core matrix (no bank conflicts).
 template <bool GRAD>
 __global__ void __launch_bounds__(kThreads) k_conv_tc(int cin, int cout, Grid g, const void *__restrict__ src,
                                                       const __nv_bfloat16 *__restrict__ y_act,
-                                                      const __nv_bfloat16 *__restrict__ w,
+                                                      const unsigned char *__restrict__ bpack,
                                                       const float *__restrict__ bias, int relu, void *__restrict__ out,
                                                       int *__restrict__ err)
 {
+    static_assert(kThreads == kM, "one thread per voxel of the tile");
     extern __shared__ __align__(1024) unsigned char smem[];
     unsigned char *Bs = smem;                         // 27 x 512
     unsigned char *As = smem + 27 * 512;              // 9 x 4096
@@ -184,20 +206,22 @@ __global__ void __launch_bounds__(kThreads) k_conv_tc(int cin, int cout, Grid g,
     uint32_t *s_taddr = reinterpret_cast<uint32_t *>(bar + 1);
     const int V = g.size();
     const int v0 = blockIdx.x * kM;
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int nrow = GRAD ? cin : cout, ncol = GRAD ? cout : cin;   // B rows (N) and columns (K)
+    const int warp = threadIdx.x >> 5;
 
-    // B operand of every tap: core matrix (n / 8, k / 8) at ((n / 8) * 2 + k / 8) * 128, row n % 8
-    for (int i = threadIdx.x; i < 27 * kC * kC; i += kThreads) {
-        const int tap = i / (kC * kC), n = (i / kC) % kC, k = i % kC;
-        float val = 0.f;
-        if (n < nrow && k < ncol) {
-            const int co = GRAD ? k : n, ci = GRAD ? n : k;
-            val = __bfloat162float(w[(size_t(co) * cin + ci) * 27 + tap]);
-        }
-        *reinterpret_cast<__nv_bfloat16 *>(Bs + tap * 512 + ((n >> 3) * 2 + (k >> 3)) * 128 + (n & 7) * 16 + (k & 7) * 2) =
-            __float2bfloat16_rn(val);
+    for (int i = threadIdx.x; i < 27 * 512 / 16; i += kThreads)
+        reinterpret_cast<uint4 *>(Bs)[i] = __ldg(reinterpret_cast<const uint4 *>(bpack) + i);
+    // this thread's voxel
+    const int m = threadIdx.x, v = v0 + m;
+    const bool inside = v < V;
+    int vx = 0, vy = 0, vz = 0;
+    if (inside) {
+        vx = v % g.nx;
+        const int q = v / g.nx;
+        vy = q % g.ny;
+        vz = q / g.ny;
     }
+    constexpr int sgn = GRAD ? -1 : 1;
+    unsigned char *arow = As + (m >> 3) * 256 + (m & 7) * 16;   // core (m / 8, h) at ((m / 8) * 2 + h) * 128
     if (threadIdx.x == 0) mbar_init(bar);
     if (warp == 0) tmem_alloc(s_taddr);
     fence_before();
@@ -208,13 +232,42 @@ __global__ void __launch_bounds__(kThreads) k_conv_tc(int cin, int cout, Grid g,
     bool ok = true;
     int issued = 0;
     for (int r = 0; r < 27 / kTapsRound && ok; ++r) {
-        // A operand of the round's taps: voxel m, channels 8h..8h+7 -> core (m / 8, h), row m % 8
-        for (int i = threadIdx.x; i < kTapsRound * kM * 2; i += kThreads) {
-            const int t = i / (kM * 2), m = (i >> 1) % kM, h = i & 1;
-            const int v = v0 + m;
-            const int u = v < V ? neighbour(g, v, r * kTapsRound + t, GRAD ? -1 : 1) : -1;
-            *reinterpret_cast<uint4 *>(As + t * 4096 + ((m >> 3) * 2 + h) * 128 + (m & 7) * 16) =
-                channels8<GRAD>(src, y_act, relu, u, h);
+        // A operand of the round's taps (tap 9 r + t: dz = r - 1, dy = t / 3 - 1, dx = t % 3 - 1,
+        // times sgn): voxel m, channels 8h..8h+7 -> core (m / 8, h), row m % 8
+        static_assert(kTapsRound == 9, "a round is one dz plane of taps");
+        const int zz = vz + sgn * (r - 1);
+        const bool zin = inside && zz >= 0 && zz < g.nz;
+        if constexpr (!GRAD) {
+            // the activations are already BF16: all 18 copies of the thread in flight at once
+#pragma unroll
+            for (int t = 0; t < kTapsRound; ++t) {
+                const int yy = vy + sgn * (t / 3 - 1), xx = vx + sgn * (t % 3 - 1);
+                const bool nb = zin && yy >= 0 && yy < g.ny && xx >= 0 && xx < g.nx;   // neighbour in the grid
+                const uint4 *p = reinterpret_cast<const uint4 *>(static_cast<const __nv_bfloat16 *>(src) +
+                                                                 (nb ? size_t((zz * g.ny + yy) * g.nx + xx) * kC : 0));
+                cp_async16_zfill(arow + t * 4096, p, nb);
+                cp_async16_zfill(arow + t * 4096 + 128, p + 1, nb);
+            }
+            cp_async_wait_all();
+        } else {
+            // gz is formed in registers (mask, BF16 rounding): three taps' loads at a time
+#pragma unroll
+            for (int t0 = 0; t0 < kTapsRound; t0 += 3) {
+                uint4 a[3][2];
+#pragma unroll
+                for (int j = 0; j < 3; ++j) {
+                    const int t = t0 + j;
+                    const int yy = vy + sgn * (t / 3 - 1), xx = vx + sgn * (t % 3 - 1);
+                    const int u = (zin && yy >= 0 && yy < g.ny && xx >= 0 && xx < g.nx) ? (zz * g.ny + yy) * g.nx + xx : -1;
+                    a[j][0] = channels8<GRAD>(src, y_act, relu, u, 0);
+                    a[j][1] = channels8<GRAD>(src, y_act, relu, u, 1);
+                }
+#pragma unroll
+                for (int j = 0; j < 3; ++j) {
+                    *reinterpret_cast<uint4 *>(arow + (t0 + j) * 4096) = a[j][0];
+                    *reinterpret_cast<uint4 *>(arow + (t0 + j) * 4096 + 128) = a[j][1];
+                }
+            }
         }
         fence_async_smem();
         __syncthreads();
@@ -237,9 +290,8 @@ __global__ void __launch_bounds__(kThreads) k_conv_tc(int cin, int cout, Grid g,
     } else {
         fence_after();
         float acc[16];
-        tmem_ld16(taddr + (uint32_t(32 * warp) << 16), acc);
-        const int v = v0 + 32 * warp + lane;
-        if (v < V) {
+        tmem_ld16(taddr + (uint32_t(32 * warp) << 16), acc);   // this thread's TMEM lane is m
+        if (inside) {
             if constexpr (!GRAD) {
                 uint32_t o[8];
 #pragma unroll
@@ -297,20 +349,34 @@ __global__ void __launch_bounds__(kThreads) k_conv_wgrad_tc(Grid g, const __nv_b
     for (int r = 0; r < nround && ok; ++r) {
         const int vr = c0 + r * kRoundVox;
         if (vr >= V) break;
-        // A: 16 M groups (tap, channel half) x 16 voxels per step; B: 2 N groups x 16 voxels
-        for (int i = threadIdx.x; i < kWgSteps * 16 * 16; i += kThreads) {
-            const int s = i / 256, mg = (i / 16) % 16, kv = i % 16;
-            const int v = vr + s * 16 + kv, tap = mt * 8 + (mg >> 1), h = mg & 1;
-            const int u = (v < V && tap < 27) ? neighbour(g, v, tap, 1) : -1;
-            *reinterpret_cast<uint4 *>(As + s * 4096 + (mg * 2 + (kv >> 3)) * 128 + (kv & 7) * 16) =
-                channels8<false>(x, nullptr, 0, u, h);
+        // Thread m stages voxel vr + m (step s = m / 16, voxel kv = m % 16 of the step).
+        // A: 16 M groups (tap, channel half) x 16 voxels per step; B: 2 N groups x 16 voxels.
+        // A quarter-warp's 16-byte stores fill one contiguous 128-byte core matrix.
+        const int m = threadIdx.x, s = m >> 4, kv = m & 15, v = vr + m;
+        const bool inside = v < V;
+        int vx = 0, vy = 0, vz = 0;
+        if (inside) {
+            vx = v % g.nx;
+            const int q = v / g.nx;
+            vy = q % g.ny;
+            vz = q / g.ny;
         }
-        for (int i = threadIdx.x; i < kWgSteps * 2 * 16; i += kThreads) {
-            const int s = i / 32, ng = (i / 16) % 2, kv = i % 16;
-            const int v = vr + s * 16 + kv;
-            *reinterpret_cast<uint4 *>(Bs + s * 512 + (ng * 2 + (kv >> 3)) * 128 + (kv & 7) * 16) =
-                channels8<true>(gy, y_act, relu, v < V ? v : -1, ng);
+        unsigned char *arow = As + s * 4096 + (kv >> 3) * 128 + (kv & 7) * 16;
+#pragma unroll
+        for (int tl = 0; tl < 8; ++tl) {
+            const int tap = mt * 8 + tl;
+            const int zz = vz + tap / 9 - 1, yy = vy + (tap / 3) % 3 - 1, xx = vx + tap % 3 - 1;
+            const bool nb = inside && tap < 27 && zz >= 0 && zz < g.nz && yy >= 0 && yy < g.ny && xx >= 0 && xx < g.nx;
+            const uint4 *p = reinterpret_cast<const uint4 *>(x + (nb ? size_t((zz * g.ny + yy) * g.nx + xx) * kC : 0));
+            cp_async16_zfill(arow + (tl * 2 + 0) * 256, p, nb);
+            cp_async16_zfill(arow + (tl * 2 + 1) * 256, p + 1, nb);
         }
+        unsigned char *brow = Bs + s * 512 + (kv >> 3) * 128 + (kv & 7) * 16;
+        const uint4 b0 = channels8<true>(gy, y_act, relu, inside ? v : -1, 0);
+        const uint4 b1 = channels8<true>(gy, y_act, relu, inside ? v : -1, 1);
+        *reinterpret_cast<uint4 *>(brow) = b0;
+        *reinterpret_cast<uint4 *>(brow + 256) = b1;
+        cp_async_wait_all();
         fence_async_smem();
         __syncthreads();
         if (threadIdx.x == 0) {
@@ -392,10 +458,13 @@ int check(int cin, int cout, int nz, int ny, int nx)
     return HRN_OK;
 }
 
-// Per-device scratch of the layers (the error flag and the weight-gradient partial
-// sums), grown on demand and kept until the process exits.
+// Per-device scratch of the layers (the error flag, the packed B operand and the
+// weight-gradient partial sums), grown on demand and kept until the process exits.
+// Calls that overlap on one device share it, as they share the error flag: the
+// calls synchronize their stream before returning.
 struct Scratch {
     int *err = nullptr;
+    unsigned char *bpack = nullptr;   // 27 x 512 bytes
     float *part = nullptr;
     size_t part_bytes = 0;
 };
@@ -411,6 +480,7 @@ int scratch(int dev, size_t part_bytes, Scratch &out)
         if (cudaMalloc(&s.err, sizeof(int)) != cudaSuccess) return HRN_EOOM;
         if (cudaMemset(s.err, 0, sizeof(int)) != cudaSuccess) return HRN_ECUDA;
     }
+    if (!s.bpack && cudaMalloc(&s.bpack, 27 * 512) != cudaSuccess) return HRN_EOOM;
     if (part_bytes > s.part_bytes) {
         if (s.part) cudaFree(s.part);
         s.part = nullptr;
@@ -460,8 +530,9 @@ extern "C" int hrn_cnn_conv3d_forward(int32_t cin, int32_t cout, int32_t nz, int
     const Grid g{nz, ny, nx};
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     set_smem_once<false>();
-    k_conv_tc<false><<<(g.size() + kM - 1) / kM, kThreads, kConvSmem, st>>>(
-        cin, cout, g, x, nullptr, static_cast<const __nv_bfloat16 *>(w), bias, relu, y, s.err);
+    k_conv_pack_b<false><<<27, 256, 0, st>>>(cin, cout, static_cast<const __nv_bfloat16 *>(w), s.bpack);
+    k_conv_tc<false><<<(g.size() + kM - 1) / kM, kThreads, kConvSmem, st>>>(cin, cout, g, x, nullptr, s.bpack, bias,
+                                                                            relu, y, s.err);
     if (cudaGetLastError() != cudaSuccess) return HRN_ECUDA;
     return check_err(s, st);
 }
@@ -483,8 +554,9 @@ extern "C" int hrn_cnn_conv3d_backward(int32_t cin, int32_t cout, int32_t nz, in
     const __nv_bfloat16 *yb = static_cast<const __nv_bfloat16 *>(y);
     if (gx) {
         set_smem_once<true>();
-        k_conv_tc<true><<<(V + kM - 1) / kM, kThreads, kConvSmem, st>>>(
-            cin, cout, g, gy, yb, static_cast<const __nv_bfloat16 *>(w), nullptr, relu, gx, s.err);
+        k_conv_pack_b<true><<<27, 256, 0, st>>>(cin, cout, static_cast<const __nv_bfloat16 *>(w), s.bpack);
+        k_conv_tc<true><<<(V + kM - 1) / kM, kThreads, kConvSmem, st>>>(cin, cout, g, gy, yb, s.bpack, nullptr, relu,
+                                                                        gx, s.err);
     }
     k_conv_wgrad_tc<<<dim3(4, nchunk), kThreads, kWgSmem, st>>>(g, static_cast<const __nv_bfloat16 *>(x), gy, yb, relu,
                                                                  s.part, s.err);
