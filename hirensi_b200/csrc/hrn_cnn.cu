@@ -13,6 +13,10 @@
 //                D ((8 taps x 16 ci) x 16 co) += A (128 x 16 voxels) B (16 voxels x 16 co),
 //                voxel chunks in parallel, partial sums added in a fixed order.
 // gz = gy masked by the ReLU of y and rounded to BF16 (the tensor-core operand).
+// The forward and data-gradient kernels read a copy of their A source with a
+// one-voxel zero border, where every tap is a shift of the voxel index: a tile
+// copies each of the nine (dz, dy) row bands once and takes the three dx taps as
+// 16-byte shifts of the same band.
 //
 // One elected thread issues tcgen05.mma (kind::f16, M = 128, N = 16, K = 16) on
 // operands staged in shared memory in the canonical no-swizzle core-matrix layout
@@ -23,6 +27,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <algorithm>
 #include <atomic>
 #include <mutex>
 
@@ -32,7 +37,6 @@ namespace {
 
 constexpr int kC = 16;            // channel stride of the activations (and the padded GEMM K and N)
 constexpr int kM = 128;           // voxels per tile (MMA M)
-constexpr int kTapsRound = 9;     // taps staged per round of the forward / data-gradient kernel
 constexpr int kThreads = 128;     // one warpgroup: warp w reads TMEM lanes 32w..32w+31
 constexpr int kTmemCols = 32;     // smallest TMEM allocation; the accumulator uses 16 columns
 constexpr int kWgSteps = 8;       // K steps (16 voxels each) staged per round of the weight-gradient kernel
@@ -183,115 +187,91 @@ __global__ void k_conv_pack_b(int cin, int cout, const __nv_bfloat16 *__restrict
     }
 }
 
-// Forward (GRAD = false) and data gradient (GRAD = true) of one 128-voxel tile.
-//   forward: src = x (BF16 [V][16]), B_tap[n = co][k = ci] = w[co][ci][tap], out = y (BF16 [V][16]);
-//   data gradient: src = gy (FP32 [V][16]) masked by y, B_tap[n = ci][k = co] = w[co][ci][tap],
-//   neighbour offset negated, out = gx (FP32 [V][16]).
-// Shared memory: B for all taps (27 x 512 B, copied from the packed operand), A for the
-// taps of one round (9 x 4 KB).  Thread m stages voxel v0 + m for every tap: its grid
-// coordinates are computed once, and a quarter-warp's 16-byte stores fill one
-// contiguous 128-byte core matrix (no bank conflicts).
+// Forward (GRAD = false) and data gradient (GRAD = true) on the padded grid: the A
+// operand comes from a copy of the input with a one-voxel zero border (k_conv_pad),
+// so that every tap is a pure shift of the padded voxel index
+//   off(tap) = dz Sz + dy Sy + dx,  Sz = (ny + 2)(nx + 2), Sy = nx + 2,
+// negated for the data gradient.  A tile is 128 consecutive padded voxels p0..p0+127.
+// For each (dz, dy) the tile needs the rows p0 + sgn (dz Sz + dy Sy) - 1 .. +128
+// (130 rows, covering the three dx); the CTA copies each such band once into shared
+// memory as two half-planes of 16-byte rows ([h][row][8 channels]), and the A operand
+// of tap (dz, dy, dx) is the band seen from row 1 + sgn dx: in the no-swizzle
+// K-major layout a core matrix is 8 consecutive 16-byte rows, so the shift is only
+// the descriptor's start address (16 bytes per row), with the half-planes one
+// leading-byte offset apart.  The 27 MMAs run in the tap order of the unpadded
+// formulation on the same operand values, so the result is the same.
+//   forward: src = x padded (BF16), B_tap[n = co][k = ci], out = y (BF16 [V][16]);
+//   data gradient: src = gz padded (BF16, k_conv_pad<true>), B_tap[n = ci][k = co],
+//   out = gx (FP32 [V][16]).
+// Output rows of border voxels are not written.
+constexpr int kBandRows = kM + 2;
+constexpr int kBandBytes = 2 * kBandRows * 16;     // two half-planes
+constexpr int kBandLbo = kBandRows * 16;           // between the half-planes (K direction)
+
 template <bool GRAD>
-__global__ void __launch_bounds__(kThreads) k_conv_tc(int cin, int cout, Grid g, const void *__restrict__ src,
-                                                      const __nv_bfloat16 *__restrict__ y_act,
-                                                      const unsigned char *__restrict__ bpack,
-                                                      const float *__restrict__ bias, int relu, void *__restrict__ out,
-                                                      int *__restrict__ err)
+__global__ void __launch_bounds__(kThreads) k_conv_band(int cin, int cout, Grid g, const __nv_bfloat16 *__restrict__ srcp,
+                                                        const unsigned char *__restrict__ bpack,
+                                                        const float *__restrict__ bias, int relu, void *__restrict__ out,
+                                                        int *__restrict__ err)
 {
-    static_assert(kThreads == kM, "one thread per voxel of the tile");
+    static_assert(kThreads == kM, "one thread per voxel of the tile in the epilogue");
     extern __shared__ __align__(1024) unsigned char smem[];
     unsigned char *Bs = smem;                         // 27 x 512
-    unsigned char *As = smem + 27 * 512;              // 9 x 4096
-    uint64_t *bar = reinterpret_cast<uint64_t *>(As + kTapsRound * 4096);
+    unsigned char *As = smem + 27 * 512;              // 9 bands
+    uint64_t *bar = reinterpret_cast<uint64_t *>(As + 9 * kBandBytes);
     uint32_t *s_taddr = reinterpret_cast<uint32_t *>(bar + 1);
-    const int V = g.size();
-    const int v0 = blockIdx.x * kM;
+    const int Sy = g.nx + 2, Sz = (g.ny + 2) * Sy;
+    const int Vp = (g.nz + 2) * Sz;
+    const int p0 = blockIdx.x * kM;
     const int warp = threadIdx.x >> 5;
+    constexpr int sgn = GRAD ? -1 : 1;
 
     for (int i = threadIdx.x; i < 27 * 512 / 16; i += kThreads)
         reinterpret_cast<uint4 *>(Bs)[i] = __ldg(reinterpret_cast<const uint4 *>(bpack) + i);
-    // this thread's voxel
-    const int m = threadIdx.x, v = v0 + m;
-    const bool inside = v < V;
-    int vx = 0, vy = 0, vz = 0;
-    if (inside) {
-        vx = v % g.nx;
-        const int q = v / g.nx;
-        vy = q % g.ny;
-        vz = q / g.ny;
+    // bands: a thread copies one 32-byte row into the two half-planes; consecutive
+    // threads take consecutive rows (contiguous 16-byte stores in each plane); rows
+    // outside the padded grid are zero-filled
+    for (int i = threadIdx.x; i < 9 * kBandRows; i += kThreads) {
+        const int b = i / kBandRows, j = i % kBandRows;
+        const int dz = b / 3 - 1, dy = b % 3 - 1;
+        const int row = p0 + sgn * (dz * Sz + dy * Sy) - 1 + j;
+        const bool in = row >= 0 && row < Vp;
+        const uint4 *q = reinterpret_cast<const uint4 *>(srcp + (in ? size_t(row) * kC : 0));
+        cp_async16_zfill(As + b * kBandBytes + j * 16, q, in);
+        cp_async16_zfill(As + b * kBandBytes + kBandLbo + j * 16, q + 1, in);
     }
-    constexpr int sgn = GRAD ? -1 : 1;
-    unsigned char *arow = As + (m >> 3) * 256 + (m & 7) * 16;   // core (m / 8, h) at ((m / 8) * 2 + h) * 128
+    cp_async_wait_all();
     if (threadIdx.x == 0) mbar_init(bar);
     if (warp == 0) tmem_alloc(s_taddr);
+    fence_async_smem();
     fence_before();
     __syncthreads();
     fence_after();
     const uint32_t taddr = *s_taddr;
     constexpr uint32_t idesc = instr_desc(kM, kC, 0, 0);
-    bool ok = true;
-    int issued = 0;
-    for (int r = 0; r < 27 / kTapsRound && ok; ++r) {
-        // A operand of the round's taps (tap 9 r + t: dz = r - 1, dy = t / 3 - 1, dx = t % 3 - 1,
-        // times sgn): voxel m, channels 8h..8h+7 -> core (m / 8, h), row m % 8
-        static_assert(kTapsRound == 9, "a round is one dz plane of taps");
-        const int zz = vz + sgn * (r - 1);
-        const bool zin = inside && zz >= 0 && zz < g.nz;
-        if constexpr (!GRAD) {
-            // the activations are already BF16: all 18 copies of the thread in flight at once
-#pragma unroll
-            for (int t = 0; t < kTapsRound; ++t) {
-                const int yy = vy + sgn * (t / 3 - 1), xx = vx + sgn * (t % 3 - 1);
-                const bool nb = zin && yy >= 0 && yy < g.ny && xx >= 0 && xx < g.nx;   // neighbour in the grid
-                const uint4 *p = reinterpret_cast<const uint4 *>(static_cast<const __nv_bfloat16 *>(src) +
-                                                                 (nb ? size_t((zz * g.ny + yy) * g.nx + xx) * kC : 0));
-                cp_async16_zfill(arow + t * 4096, p, nb);
-                cp_async16_zfill(arow + t * 4096 + 128, p + 1, nb);
-            }
-            cp_async_wait_all();
-        } else {
-            // gz is formed in registers (mask, BF16 rounding): three taps' loads at a time
-#pragma unroll
-            for (int t0 = 0; t0 < kTapsRound; t0 += 3) {
-                uint4 a[3][2];
-#pragma unroll
-                for (int j = 0; j < 3; ++j) {
-                    const int t = t0 + j;
-                    const int yy = vy + sgn * (t / 3 - 1), xx = vx + sgn * (t % 3 - 1);
-                    const int u = (zin && yy >= 0 && yy < g.ny && xx >= 0 && xx < g.nx) ? (zz * g.ny + yy) * g.nx + xx : -1;
-                    a[j][0] = channels8<GRAD>(src, y_act, relu, u, 0);
-                    a[j][1] = channels8<GRAD>(src, y_act, relu, u, 1);
-                }
-#pragma unroll
-                for (int j = 0; j < 3; ++j) {
-                    *reinterpret_cast<uint4 *>(arow + (t0 + j) * 4096) = a[j][0];
-                    *reinterpret_cast<uint4 *>(arow + (t0 + j) * 4096 + 128) = a[j][1];
-                }
-            }
+    if (threadIdx.x == 0) {
+        for (int tap = 0; tap < 27; ++tap) {
+            const int b = tap / 3, dx = tap % 3 - 1;     // band (dz, dy) = (tap / 9, tap / 3 % 3)
+            mma_bf16(taddr, smem_desc(As + b * kBandBytes + (1 + sgn * dx) * 16, kBandLbo, 128),
+                     smem_desc(Bs + tap * 512, 128, 256), idesc, tap != 0);
         }
-        fence_async_smem();
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            fence_after();
-            for (int t = 0; t < kTapsRound; ++t)
-                mma_bf16(taddr, smem_desc(As + t * 4096, 128, 256), smem_desc(Bs + (r * kTapsRound + t) * 512, 128, 256),
-                         idesc, (r | t) != 0);
-            mma_commit(bar);
-        }
-        ++issued;
-        ok = mbar_wait(bar, uint32_t(r & 1));   // the MMAs read A before the next round overwrites it
-        ok = __syncthreads_and(ok);
+        mma_commit(bar);
     }
+    bool ok = mbar_wait(bar, 0);
+    ok = __syncthreads_and(ok);
     if (!ok) {
         if (threadIdx.x == 0) {
             atomicExch(err, 1);
-            mbar_wait(bar, uint32_t((issued - 1) & 1));
+            mbar_wait(bar, 0);
         }
     } else {
         fence_after();
         float acc[16];
-        tmem_ld16(taddr + (uint32_t(32 * warp) << 16), acc);   // this thread's TMEM lane is m
-        if (inside) {
+        tmem_ld16(taddr + (uint32_t(32 * warp) << 16), acc);   // this thread's TMEM lane is its voxel
+        const int p = p0 + threadIdx.x;
+        const int px = p % Sy, py = (p / Sy) % (g.ny + 2), pz = p / Sz;
+        if (p < Vp && px >= 1 && px <= g.nx && py >= 1 && py <= g.ny && pz >= 1 && pz <= g.nz) {
+            const int v = ((pz - 1) * g.ny + (py - 1)) * g.nx + (px - 1);
             if constexpr (!GRAD) {
                 uint32_t o[8];
 #pragma unroll
@@ -315,6 +295,24 @@ __global__ void __launch_bounds__(kThreads) k_conv_tc(int cin, int cout, Grid g,
     fence_before();
     __syncthreads();
     if (warp == 0) tmem_dealloc(taddr);
+}
+
+// Copy of the A source with a one-voxel zero border, BF16 [Vp][16]: the activations
+// (forward) or gz = gy masked by ReLU(y) and rounded to BF16 (data gradient).  One
+// thread per (padded voxel, channel half).
+template <bool GRAD>
+__global__ void k_conv_pad(Grid g, const void *__restrict__ src, const __nv_bfloat16 *__restrict__ y_act, int relu,
+                           __nv_bfloat16 *__restrict__ dstp)
+{
+    const int Sy = g.nx + 2, Sz = (g.ny + 2) * Sy;
+    const int n = 2 * (g.nz + 2) * Sz;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int p = i >> 1, h = i & 1;
+        const int px = p % Sy, py = (p / Sy) % (g.ny + 2), pz = p / Sz;
+        const bool interior = px >= 1 && px <= g.nx && py >= 1 && py <= g.ny && pz >= 1 && pz <= g.nz;
+        const int u = interior ? ((pz - 1) * g.ny + (py - 1)) * g.nx + (px - 1) : -1;
+        reinterpret_cast<uint4 *>(dstp + size_t(p) * kC)[h] = channels8<GRAD>(src, y_act, relu, u, h);
+    }
 }
 
 // Weight gradient, partial sums of one chunk of voxels for one M tile of 8 taps:
@@ -448,28 +446,32 @@ __global__ void __launch_bounds__(kBThreads) k_conv_bias_grad(Grid g, const floa
     }
 }
 
-constexpr size_t kConvSmem = 27 * 512 + kTapsRound * 4096 + 16;
+constexpr size_t kConvSmem = 27 * 512 + 9 * kBandBytes + 16;
 constexpr size_t kWgSmem = kWgSteps * (4096 + 512) + 16;
 
 int check(int cin, int cout, int nz, int ny, int nx)
 {
     if (cin < 1 || cin > kC || cout < 1 || cout > kC || nz < 1 || ny < 1 || nx < 1) return HRN_EARG;
-    if (int64_t(nz) * ny * nx > (int64_t(1) << 30)) return HRN_EARG;
+    if (int64_t(nz + 2) * (ny + 2) * (nx + 2) > (int64_t(1) << 30)) return HRN_EARG;   // padded grid
     return HRN_OK;
 }
 
-// Per-device scratch of the layers (the error flag, the packed B operand and the
-// weight-gradient partial sums), grown on demand and kept until the process exits.
-// Calls that overlap on one device share it, as they share the error flag: the
-// calls synchronize their stream before returning.
+// Per-device scratch of the layers (the error flag, the packed B operand, the padded
+// copy of the A source and the weight-gradient partial sums), grown on demand and
+// kept until the process exits.  Calls that overlap on one device share it, as they
+// share the error flag: the calls synchronize their stream before returning.
 struct Scratch {
     int *err = nullptr;
     unsigned char *bpack = nullptr;   // 27 x 512 bytes
+    __nv_bfloat16 *pad = nullptr;     // [(nz + 2)(ny + 2)(nx + 2)][16]
+    size_t pad_bytes = 0;
     float *part = nullptr;
     size_t part_bytes = 0;
 };
 
-int scratch(int dev, size_t part_bytes, Scratch &out)
+size_t pad_bytes(const Grid &g) { return size_t(g.nz + 2) * (g.ny + 2) * (g.nx + 2) * kC * sizeof(__nv_bfloat16); }
+
+int scratch(int dev, size_t part_bytes, size_t padded_bytes, Scratch &out)
 {
     static std::mutex mu;
     static Scratch per[64];
@@ -481,6 +483,13 @@ int scratch(int dev, size_t part_bytes, Scratch &out)
         if (cudaMemset(s.err, 0, sizeof(int)) != cudaSuccess) return HRN_ECUDA;
     }
     if (!s.bpack && cudaMalloc(&s.bpack, 27 * 512) != cudaSuccess) return HRN_EOOM;
+    if (padded_bytes > s.pad_bytes) {
+        if (s.pad) cudaFree(s.pad);
+        s.pad = nullptr;
+        s.pad_bytes = 0;
+        if (cudaMalloc(&s.pad, padded_bytes) != cudaSuccess) return HRN_EOOM;
+        s.pad_bytes = padded_bytes;
+    }
     if (part_bytes > s.part_bytes) {
         if (s.part) cudaFree(s.part);
         s.part = nullptr;
@@ -512,7 +521,7 @@ void set_smem_once()
     cudaGetDevice(&dev);
     const uint64_t bit = dev >= 0 && dev < 64 ? (uint64_t(1) << dev) : 0;
     if (bit && (done.load() & bit)) return;
-    cudaFuncSetAttribute(k_conv_tc<GRAD>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kConvSmem));
+    cudaFuncSetAttribute(k_conv_band<GRAD>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kConvSmem));
     done.fetch_or(bit);
 }
 
@@ -525,14 +534,16 @@ extern "C" int hrn_cnn_conv3d_forward(int32_t cin, int32_t cout, int32_t nz, int
     if (!x || !w || !bias || !y) return HRN_EARG;
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return HRN_ECUDA;
-    Scratch s;
-    if (int rc = scratch(dev, 0, s)) return rc;
     const Grid g{nz, ny, nx};
+    Scratch s;
+    if (int rc = scratch(dev, 0, pad_bytes(g), s)) return rc;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const int np = (nz + 2) * (ny + 2) * (nx + 2);
     set_smem_once<false>();
     k_conv_pack_b<false><<<27, 256, 0, st>>>(cin, cout, static_cast<const __nv_bfloat16 *>(w), s.bpack);
-    k_conv_tc<false><<<(g.size() + kM - 1) / kM, kThreads, kConvSmem, st>>>(cin, cout, g, x, nullptr, s.bpack, bias,
-                                                                            relu, y, s.err);
+    k_conv_pad<false><<<std::min((2 * np + 255) / 256, 148 * 16), 256, 0, st>>>(g, x, nullptr, 0, s.pad);
+    k_conv_band<false><<<(np + kM - 1) / kM, kThreads, kConvSmem, st>>>(cin, cout, g, s.pad, s.bpack, bias, relu, y,
+                                                                        s.err);
     if (cudaGetLastError() != cudaSuccess) return HRN_ECUDA;
     return check_err(s, st);
 }
@@ -549,14 +560,16 @@ extern "C" int hrn_cnn_conv3d_backward(int32_t cin, int32_t cout, int32_t nz, in
     const int V = g.size();
     const int nchunk = (V + kWgChunk - 1) / kWgChunk;
     Scratch s;
-    if (int rc = scratch(dev, size_t(nchunk) * 4 * kM * kC * sizeof(float), s)) return rc;
+    if (int rc = scratch(dev, size_t(nchunk) * 4 * kM * kC * sizeof(float), gx ? pad_bytes(g) : 0, s)) return rc;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     const __nv_bfloat16 *yb = static_cast<const __nv_bfloat16 *>(y);
     if (gx) {
+        const int np = (nz + 2) * (ny + 2) * (nx + 2);
         set_smem_once<true>();
         k_conv_pack_b<true><<<27, 256, 0, st>>>(cin, cout, static_cast<const __nv_bfloat16 *>(w), s.bpack);
-        k_conv_tc<true><<<(V + kM - 1) / kM, kThreads, kConvSmem, st>>>(cin, cout, g, gy, yb, s.bpack, nullptr, relu,
-                                                                        gx, s.err);
+        k_conv_pad<true><<<std::min((2 * np + 255) / 256, 148 * 16), 256, 0, st>>>(g, gy, yb, relu, s.pad);
+        k_conv_band<true><<<(np + kM - 1) / kM, kThreads, kConvSmem, st>>>(cin, cout, g, s.pad, s.bpack, nullptr, relu,
+                                                                           gx, s.err);
     }
     k_conv_wgrad_tc<<<dim3(4, nchunk), kThreads, kWgSmem, st>>>(g, static_cast<const __nv_bfloat16 *>(x), gy, yb, relu,
                                                                  s.part, s.err);
