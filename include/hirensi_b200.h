@@ -319,9 +319,12 @@ int hrn_pseudo_hessian(hrn_ctx *ctx, double *d_h_lambda, double *d_h_mu);
  * when relu != 0.  Activations are channels-last with a channel stride of 16:
  * x [nz][ny][nx][16] BF16 with channels >= cin zero, y [nz][ny][nx][16] BF16 with
  * channels >= cout written as zero.  w is [cout][cin][27] BF16 (tap k = 9 dz + 3 dy + dx),
- * bias [cout] FP32.  At most 16 channels in and out.  All pointers are device pointers;
- * stream is a cudaStream_t or NULL.  Returns once the layer has run (the kernels' error
- * flag is read back). */
+ * bias [cout] FP32.  At most 16 channels in and out; (nz + 2)(ny + 2)(nx + 2) at most
+ * 2^30.  All pointers are device pointers; stream is a cudaStream_t or NULL.  Returns
+ * once the layer has run (the kernels' error flag is read back).  The layers keep a
+ * per-device scratch (the packed weights, a copy of the input with a one-voxel zero
+ * border, weight-gradient partial sums), allocated when a larger grid first needs it
+ * and shared by all calls on that device: calls that overlap on one device race on it. */
 int hrn_cnn_conv3d_forward(int32_t cin, int32_t cout, int32_t nz, int32_t ny, int32_t nx, const void *x,
                            const void *w, const float *bias, int32_t relu, void *y, void *stream);
 /* Gradients of that layer from gy = dL/dy (FP32 [nz][ny][nx][16]): gx = dL/dx (FP32
