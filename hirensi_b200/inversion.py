@@ -462,8 +462,9 @@ class BatchedBackend(DeviceBackend):
             order.insert(0, self.resident)
         self.axpby(0.0, g_l, 0.0, None, g_l)
         self.axpby(0.0, g_m, 0.0, None, g_m)
+        first = self.resident
         for i, k in enumerate(order):
-            if i > 0:
+            if not (i == 0 and k == first):      # no misfit evaluation left this batch resident
                 self._use(k)
                 self.s.forward()
             self.s.adjoint_gradient(None, to_host=False)
