@@ -372,7 +372,7 @@ def run_native(args, rank, world, local_rank):
                               "seismogram_rel_l2_vs_fp64": rel(tr32, tr64),
                               "gradient_rel_l2_vs_fp64": rel(g32.cpu().numpy(), g64.cpu().numpy())}
             s32.close()
-        if rank == 0 and not args.no_cpu_baseline:
+        if world == 1 and not args.no_cpu_baseline:      # the host-core baseline is a single-GPU figure
             cb = cpu_sample(prob, nsteps=200)
             cb.pop("seconds", None)
             result["cpu_baseline"] = cb
