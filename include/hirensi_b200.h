@@ -188,12 +188,12 @@ int hrn_misfit(hrn_ctx *ctx, const double *dis_meas, double *cost);
  * HRN_EARG before anything is launched.  The scratch is one static device array
  * shared by every context and call in the process, so nothing is allocated.
  * Limit: nshot * (nstep + 1) <= 131072, larger problems return HRN_EARG.  The
- * first call on a device looks the array's address up (cudaGetSymbolAddress)
- * with that device current and keeps it; do not use the entry across a
- * cudaDeviceReset.  Calls whose
- * kernels overlap on one GPU (other streams, other contexts, other host threads)
- * race on the scratch: serialize them.  It synchronizes its stream and returns
- * once *cost is ready. */
+ * first call on a device does the set-up: it looks the array's address up
+ * (cudaGetSymbolAddress) with that device current and keeps it, so make that first
+ * call before any stream capture begins, and do not use the entry across a
+ * cudaDeviceReset.  Calls whose kernels overlap on one GPU (other streams, other
+ * contexts, other host threads) race on the scratch: serialize them.  It
+ * synchronizes its stream and returns once *cost is ready. */
 int hrn_misfit_noalloc(hrn_ctx *ctx, const double *d_dis_meas, double *cost);
 
 /* Adjoint RK4 (OtD) with the zero-lag gradient fused into each step:
