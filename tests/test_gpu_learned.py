@@ -31,13 +31,15 @@ def _first(a, c, shape):
 
 
 @pytest.mark.parametrize("cin,cout,shape,relu", [(4, 16, (5, 7, 9), 1), (16, 16, (6, 5, 8), 1), (16, 2, (4, 6, 5), 0),
-                                                 (6, 16, (17, 33, 33), 1), (16, 16, (3, 40, 47), 1)])
+                                                 (6, 16, (17, 33, 33), 1), (16, 16, (3, 40, 47), 1),
+                                                 (16, 16, (1, 1, 300), 1), (4, 16, (2, 1, 3), 0), (16, 2, (1, 9, 1), 1)])
 def test_conv3d_kernels_match_oracle(gpu_lib, cin, cout, shape, relu):
     """The tensor-core layers against the numpy oracle: the forward within one BF16
     rounding of the FP64 result; the gradients at FP32-accumulation accuracy against
     the oracle fed the same BF16-rounded masked gy (the tensor-core operand); gb from
-    the FP32 gy.  The shapes include tiles cut by the grid's end and more than one
-    weight-gradient voxel chunk."""
+    the FP32 gy.  The shapes include tiles cut by the grid's end, more than one
+    weight-gradient voxel chunk, and grids one voxel thin along one or two axes (the
+    padded copy's border on both sides of every tap)."""
     import torch
     rng = np.random.default_rng(cin * 100 + cout)
     x = Lr.round_bf16(rng.standard_normal((cin,) + shape))
